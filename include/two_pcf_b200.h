@@ -1,0 +1,146 @@
+/*
+ * two_pcf_b200 — C ABI of the B200 grid-binned pair-counting engine.
+ *
+ * This is the drop-in boundary for the hot path of lstothert/two_pcf: the
+ * reference's GalaxyBoxes + auto_/cross_pair_count_* + JKHists machinery
+ * (src/boxes.h:16-39, src/correlators.h:7-31, src/hist.h:21-107,
+ * src/correlators_invpweight.h:14-42).  Plain pointers and sizes only; every
+ * call returns a status (0 = TPCF_OK) and no exception crosses it.  Host
+ * buffers passed in are borrowed for the duration of the call.
+ *
+ * Threading: one tpcf_ctx per host thread; calls on one context are
+ * serialised on its CUDA stream.
+ */
+#ifndef TWO_PCF_B200_H
+#define TWO_PCF_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TPCF_ABI_VERSION 1
+
+typedef enum {
+    TPCF_OK = 0,
+    TPCF_E_INVALID_ARG = 1,     /* bad pointer, size, NaN coordinate, region index out of range */
+    TPCF_E_OOM = 2,             /* device allocation failed */
+    TPCF_E_CUDA = 3,            /* any other CUDA runtime error */
+    TPCF_E_DEVICE_TIMEOUT = 4,  /* a bounded device wait gave up; results discarded */
+    TPCF_E_OVERFLOW = 5,        /* a fixed-point histogram bin would overflow */
+    TPCF_E_UNSUPPORTED = 6      /* configuration outside the engine's limits */
+} tpcf_status;
+
+typedef enum {
+    TPCF_MONOPOLE = 0, /* Hist on s                        (src/correlators.cpp:127-153) */
+    TPCF_SIGMA_PI = 1, /* Hist2D on (sigma, |pi|)          (src/correlators.cpp:280-307) */
+    TPCF_S_MU = 2,     /* Hist2D on (s, mu), mu in [0, 1]  (src/correlators.cpp:432-459) */
+    TPCF_ANGULAR = 3   /* Hist on 1 - cos(theta)           (src/correlators_invpweight.cpp:985-1033) */
+} tpcf_mode;
+
+typedef enum {
+    TPCF_FP32_GUARD = 0, /* FP32 from cell-relative coordinates, exact re-check near every edge */
+    TPCF_FP64 = 1        /* every candidate evaluated with the reference's exact float/double sequence */
+} tpcf_precision;
+
+typedef struct tpcf_ctx tpcf_ctx;
+typedef struct tpcf_catalog tpcf_catalog;
+typedef struct tpcf_binning tpcf_binning;
+
+/* One histogram axis with the parameter-file meaning (src/io.h:42-66):
+ * log binning when log_base > 1.02 (src/hist.cpp:25). */
+typedef struct {
+    double min;
+    double max;
+    double log_base;
+    int32_t n_bins;
+} tpcf_axis_spec;
+
+typedef struct {
+    uint64_t candidates;       /* pair evaluations enumerated */
+    uint64_t in_range;         /* pairs passing the reference range test (auto pairs once) */
+    uint64_t guard_evals;      /* pairs re-evaluated with the exact sequence */
+    uint64_t overflow_updates; /* jackknife updates that bypassed shared memory */
+    uint64_t work_items;
+    double ms_kernel;          /* device time of the counting kernels */
+    double ms_total;           /* host wall time of the call */
+} tpcf_stats;
+
+int tpcf_abi_version(void);
+const char *tpcf_status_string(int status);
+
+/* Context on one CUDA device.  Replaces the OpenMP set-up of src/main.cpp:29-35. */
+int tpcf_create(int device, tpcf_ctx **out);
+int tpcf_destroy(tpcf_ctx *ctx);
+const char *tpcf_last_error(const tpcf_ctx *ctx);
+/* Run on a caller-owned cudaStream_t (NULL: the context's own stream). */
+int tpcf_set_stream(tpcf_ctx *ctx, void *cuda_stream);
+/* Cells per maximum separation (1..3; 0 = automatic). */
+int tpcf_set_refinement(tpcf_ctx *ctx, int cells_per_rmax);
+int tpcf_synchronize(tpcf_ctx *ctx);
+
+/* A catalogue resident on the device: the Galaxy fields of src/galaxy.h:16-35.
+ *   xyz[3n]         comoving position (Galaxy::x)
+ *   x_norm[3n]      unit vector (Galaxy::x_norm); NULL: x / |x| as the
+ *                   cartesian reader computes it (src/io.cpp:393-399)
+ *   d_comov[n]      NULL: |x|.  Points with d_comov < 0 are dropped by the
+ *                   reference's partition loop (src/boxes.cpp:15-26), which is
+ *                   reproduced exactly, including the points it drops early.
+ *   weight[n]       Galaxy::weight (float); NULL: 1.0
+ *   input_weight[n] Galaxy::input_weight (inverse-p build); NULL: weight
+ *   jk_region[n]    in [0, n_jk_regions); NULL: 0
+ *   bitmask[n * n_mask_ints]  Galaxy::bitmask, object-major; NULL: none
+ * Replaces GalaxyBoxes(...) (src/boxes.h:30); the caller's arrays are not
+ * permuted. */
+int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const double *x_norm, const double *d_comov,
+                        const float *weight, const float *input_weight, const int32_t *jk_region,
+                        int32_t n_jk_regions, const int64_t *bitmask, int32_t n_mask_ints, tpcf_catalog **out);
+int tpcf_catalog_destroy(tpcf_catalog *cat);
+/* Points kept by the d_comov partition (GalaxyBoxes::n_gals). */
+int64_t tpcf_catalog_n_used(const tpcf_catalog *cat);
+
+/* Histogram definition.  ax2 is the pi axis for TPCF_SIGMA_PI and supplies
+ * only n_bins (mu bins on [0, 1]) for TPCF_S_MU; it is ignored otherwise.
+ * Replaces Hist / Hist2D construction (src/hist.cpp:15-36, :64, :393).
+ * Host-only: ctx may be NULL (errors are then reported by status alone). */
+int tpcf_binning_create(tpcf_ctx *ctx, int mode, const tpcf_axis_spec *ax1, const tpcf_axis_spec *ax2,
+                        int32_t n_jk_regions, tpcf_binning **out);
+int tpcf_binning_destroy(tpcf_binning *bin);
+int tpcf_binning_total_bins(const tpcf_binning *bin);
+/* Threshold table of one axis (axis 1 or 2): T[0..n] with bin = #{T <= x} - 1.
+ * Writes min(cap, n + 1) floats; returns n + 1, or a negative status. */
+int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int cap);
+
+/* Raw pair count.  b == NULL: auto count of a (each unordered pair once).
+ *   full_out[nb]            sum of pair weights per bin
+ *   region_out[n_jk * nb]   per region r: sum over pairs with either end in r
+ *                           (JKHists::add_pair, src/hist.cpp:246-260), before
+ *                           invert_jk_hists; may be NULL
+ * Neither is doubled for auto counts. */
+int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+               int precision, double *full_out, double *region_out, tpcf_stats *stats);
+
+/* The reference's counting entry points with its output convention: the
+ * histograms after invert_jk_hists() and, for auto counts, multiply_hists(2.0)
+ * — what auto_pair_count_{monopole,sigma_pi,s_mu}(const GalaxyBoxes*, JKHists*)
+ * and cross_pair_count_*(a, b, hist) leave in hist (src/correlators.cpp:11-430). */
+int tpcf_auto_pair_count(tpcf_ctx *ctx, const tpcf_catalog *cat, const tpcf_binning *bin, int precision,
+                         double *full_hist, double *sub_hist, tpcf_stats *stats);
+int tpcf_cross_pair_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                          int precision, double *full_hist, double *sub_hist, tpcf_stats *stats);
+
+/* JKHists::normalise (src/hist.cpp:290-367) over the kept points of the
+ * catalogue(s), in place on arrays of nb and n_jk * nb doubles. */
+int tpcf_normalise_auto(const tpcf_catalog *cat, int32_t nb, double *full_hist, double *sub_hist);
+int tpcf_normalise_cross(const tpcf_catalog *a, const tpcf_catalog *b, int32_t nb, double *full_hist,
+                         double *sub_hist);
+
+/* ls_estimator (src/io.cpp:643-651). */
+double tpcf_ls_estimator(double dd, double dr, double rr);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TWO_PCF_B200_H */

@@ -1,0 +1,225 @@
+"""two_pcf_b200 — B200-native grid-binned pair counting for the two-point
+correlation function (the hot path of lstothert/two_pcf).
+
+Python mirror of the reference's counting interface, over the C ABI of
+include/two_pcf_b200.h:
+
+===========================================  =====================================
+reference (lstothert/two_pcf)                here
+===========================================  =====================================
+GalaxyBoxes(gals, n, other, n_other, rmax)   Catalog(ctx, xyz, ...)  (src/boxes.h:30)
+Hist / Hist2D(min, max, n, base, ...)        Binning(ctx, mode, ax1, ax2, n_jk)
+auto_pair_count_{monopole,sigma_pi,s_mu}     auto_pair_count(ctx, cat, binning)
+cross_pair_count_{monopole,sigma_pi,s_mu}    cross_pair_count(ctx, a, b, binning)
+JKHists::normalise                           normalise_auto / normalise_cross
+ls_estimator                                 ls_estimator
+===========================================  =====================================
+
+The counting functions return (full_hist, sub_hist) exactly as the reference
+leaves JKHists after invert_jk_hists() and, for auto counts, multiply_hists(2.0)
+(src/correlators.cpp:76-77).  There is no CPU fallback: every count runs the
+CUDA kernels in two_pcf_b200/lib/libtpcf_b200.so.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _capi
+from ._capi import ANGULAR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI, AxisSpec, Stats
+
+__all__ = ["Context", "Catalog", "Binning", "TpcfError", "count", "auto_pair_count", "cross_pair_count",
+           "normalise_auto", "normalise_cross", "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR",
+           "FP32_GUARD", "FP64"]
+
+
+class TpcfError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"[{status}] {msg}")
+        self.status = status
+
+
+def _check(rc: int, ctx=None):
+    if rc != 0:
+        L = _capi.lib()
+        detail = L.tpcf_last_error(ctx._h).decode() if ctx is not None and ctx._h else ""
+        raise TpcfError(rc, f"{L.tpcf_status_string(rc).decode()}: {detail}")
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class Context:
+    """One CUDA device; owns a stream.  Replaces the OpenMP set-up of src/main.cpp:29-35."""
+
+    def __init__(self, device: int = 0, refinement: int = 0):
+        L = _capi.lib()
+        h = C.c_void_p()
+        rc = L.tpcf_create(int(device), C.byref(h))
+        if rc != 0:
+            raise TpcfError(rc, f"tpcf_create(device={device}) failed: {L.tpcf_status_string(rc).decode()}")
+        self._h = h
+        if refinement:
+            _check(L.tpcf_set_refinement(self._h, int(refinement)), self)
+
+    def set_refinement(self, m: int):
+        _check(_capi.lib().tpcf_set_refinement(self._h, int(m)), self)
+
+    def set_stream(self, stream_handle: int | None):
+        _check(_capi.lib().tpcf_set_stream(self._h, C.c_void_p(stream_handle or 0)), self)
+
+    def synchronize(self):
+        _check(_capi.lib().tpcf_synchronize(self._h), self)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().tpcf_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Catalog:
+    """A catalogue resident on the device (Galaxy fields of src/galaxy.h:16-35)."""
+
+    def __init__(self, ctx: Context, xyz, x_norm=None, d_comov=None, weight=None, input_weight=None,
+                 jk_region=None, n_jk_regions: int = 1, bitmask=None):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        n = xyz.shape[0]
+        arrs = {
+            "x_norm": None if x_norm is None else np.ascontiguousarray(x_norm, np.float64).reshape(n, 3),
+            "d_comov": None if d_comov is None else np.ascontiguousarray(d_comov, np.float64).reshape(n),
+            "weight": None if weight is None else np.ascontiguousarray(weight, np.float32).reshape(n),
+            "input_weight": None if input_weight is None else np.ascontiguousarray(input_weight, np.float32).reshape(n),
+            "jk": None if jk_region is None else np.ascontiguousarray(jk_region, np.int32).reshape(n),
+            "mask": None if bitmask is None else np.ascontiguousarray(bitmask, np.int64).reshape(n, -1),
+        }
+        n_mask = 0 if arrs["mask"] is None else arrs["mask"].shape[1]
+        h = C.c_void_p()
+        rc = _capi.lib().tpcf_catalog_create(ctx._h, n, _ptr(xyz), _ptr(arrs["x_norm"]), _ptr(arrs["d_comov"]),
+                                             _ptr(arrs["weight"]), _ptr(arrs["input_weight"]), _ptr(arrs["jk"]),
+                                             int(n_jk_regions), _ptr(arrs["mask"]), n_mask, C.byref(h))
+        _check(rc, ctx)
+        self._h = h
+        self.ctx = ctx
+        self.n = n
+        self.n_jk = int(n_jk_regions)
+
+    @property
+    def n_used(self) -> int:
+        return int(_capi.lib().tpcf_catalog_n_used(self._h))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().tpcf_catalog_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def _axis(spec) -> AxisSpec:
+    if isinstance(spec, AxisSpec):
+        return spec
+    vmin, vmax, base, n = spec
+    return AxisSpec(float(vmin), float(vmax), float(base), int(n))
+
+
+class Binning:
+    """Histogram definition: mode plus (min, max, log_base, n_bins) axes."""
+
+    def __init__(self, ctx: Context | None, mode: int, ax1, ax2=None, n_jk_regions: int = 1):
+        a1 = _axis(ax1)
+        a2 = _axis(ax2) if ax2 is not None else None
+        h = C.c_void_p()
+        rc = _capi.lib().tpcf_binning_create(ctx._h if ctx is not None else None, int(mode), C.byref(a1), C.byref(a2) if a2 is not None else None,
+                                             int(n_jk_regions), C.byref(h))
+        _check(rc, ctx)
+        self._h = h
+        self.ctx = ctx
+        self.mode = mode
+        self.n_jk = int(n_jk_regions)
+        self.nb = int(_capi.lib().tpcf_binning_total_bins(h))
+        self.shape = (a1.n_bins,) if mode in (MONOPOLE, ANGULAR) else (a1.n_bins, a2.n_bins)
+
+    def thresholds(self, axis: int = 1) -> np.ndarray:
+        n = _capi.lib().tpcf_binning_thresholds(self._h, axis, None, 0)
+        out = np.empty(n, np.float32)
+        _capi.lib().tpcf_binning_thresholds(self._h, axis, _ptr(out), n)
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().tpcf_binning_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def count(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, precision: int = FP32_GUARD,
+          with_regions: bool = True):
+    """Raw count: (full[nb], regions[n_jk, nb] or None, stats dict), not inverted nor doubled."""
+    full = np.zeros(binning.nb)
+    reg = np.zeros((binning.n_jk, binning.nb)) if with_regions else None
+    st = Stats()
+    rc = _capi.lib().tpcf_count(ctx._h, a._h, b._h if b is not None else None, binning._h, int(precision),
+                                _ptr(full), _ptr(reg), C.byref(st))
+    _check(rc, ctx)
+    return full, reg, st.as_dict()
+
+
+def auto_pair_count(ctx: Context, cat: Catalog, binning: Binning, precision: int = FP32_GUARD):
+    """auto_pair_count_{monopole,sigma_pi,s_mu} (src/correlators.cpp:11-78, :190-239, :345-393)."""
+    full = np.zeros(binning.nb)
+    sub = np.zeros((binning.n_jk, binning.nb))
+    st = Stats()
+    _check(_capi.lib().tpcf_auto_pair_count(ctx._h, cat._h, binning._h, int(precision), _ptr(full), _ptr(sub),
+                                            C.byref(st)), ctx)
+    return full, sub, st.as_dict()
+
+
+def cross_pair_count(ctx: Context, a: Catalog, b: Catalog, binning: Binning, precision: int = FP32_GUARD):
+    """cross_pair_count_{monopole,sigma_pi,s_mu} (src/correlators.cpp:80-125, :241-278, :395-430)."""
+    full = np.zeros(binning.nb)
+    sub = np.zeros((binning.n_jk, binning.nb))
+    st = Stats()
+    _check(_capi.lib().tpcf_cross_pair_count(ctx._h, a._h, b._h, binning._h, int(precision), _ptr(full), _ptr(sub),
+                                             C.byref(st)), ctx)
+    return full, sub, st.as_dict()
+
+
+def normalise_auto(cat: Catalog, full, sub):
+    """JKHists::normalise(cat, n_gals) (src/hist.cpp:290-321); returns normalised copies."""
+    full = np.array(full, np.float64, copy=True)
+    sub = np.array(sub, np.float64, copy=True)
+    _check(_capi.lib().tpcf_normalise_auto(cat._h, full.size, _ptr(full), _ptr(sub)))
+    return full, sub
+
+
+def normalise_cross(a: Catalog, b: Catalog, full, sub):
+    """JKHists::normalise(cat1, n1, cat2, n2) (src/hist.cpp:323-367); returns normalised copies."""
+    full = np.array(full, np.float64, copy=True)
+    sub = np.array(sub, np.float64, copy=True)
+    _check(_capi.lib().tpcf_normalise_cross(a._h, b._h, full.size, _ptr(full), _ptr(sub)))
+    return full, sub
+
+
+def ls_estimator(dd, dr, rr):
+    """Landy-Szalay estimator (src/io.cpp:643-651), elementwise."""
+    dd, dr, rr = np.broadcast_arrays(np.asarray(dd, float), np.asarray(dr, float), np.asarray(rr, float))
+    f = _capi.lib().tpcf_ls_estimator
+    out = np.array([f(float(x), float(y), float(z)) for x, y, z in zip(dd.ravel(), dr.ravel(), rr.ravel())])
+    return out.reshape(dd.shape)

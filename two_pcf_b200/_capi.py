@@ -1,0 +1,92 @@
+"""ctypes declarations of the C ABI in include/two_pcf_b200.h.
+
+The shared library is built in-tree (two_pcf_b200/build.py ->
+two_pcf_b200/lib/libtpcf_b200.so).  There is no fallback: if the library is
+missing or cannot be loaded, import fails with the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libtpcf_b200.so")
+
+TPCF_OK = 0
+TPCF_E_INVALID_ARG = 1
+TPCF_E_OOM = 2
+TPCF_E_CUDA = 3
+TPCF_E_DEVICE_TIMEOUT = 4
+TPCF_E_OVERFLOW = 5
+TPCF_E_UNSUPPORTED = 6
+
+MONOPOLE, SIGMA_PI, S_MU, ANGULAR = 0, 1, 2, 3
+FP32_GUARD, FP64 = 0, 1
+
+
+class AxisSpec(C.Structure):
+    _fields_ = [("min", C.c_double), ("max", C.c_double), ("log_base", C.c_double), ("n_bins", C.c_int32)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("candidates", C.c_uint64), ("in_range", C.c_uint64), ("guard_evals", C.c_uint64),
+                ("overflow_updates", C.c_uint64), ("work_items", C.c_uint64), ("ms_kernel", C.c_double),
+                ("ms_total", C.c_double)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# Every symbol the header declares, with (restype, argtypes).
+_vp = C.c_void_p
+_PROTOTYPES = {
+    "tpcf_abi_version": (C.c_int, []),
+    "tpcf_status_string": (C.c_char_p, [C.c_int]),
+    "tpcf_create": (C.c_int, [C.c_int, C.POINTER(_vp)]),
+    "tpcf_destroy": (C.c_int, [_vp]),
+    "tpcf_last_error": (C.c_char_p, [_vp]),
+    "tpcf_set_stream": (C.c_int, [_vp, _vp]),
+    "tpcf_set_refinement": (C.c_int, [_vp, C.c_int]),
+    "tpcf_synchronize": (C.c_int, [_vp]),
+    "tpcf_catalog_create": (C.c_int, [_vp, C.c_int64, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, _vp, C.c_int32,
+                                      C.POINTER(_vp)]),
+    "tpcf_catalog_destroy": (C.c_int, [_vp]),
+    "tpcf_catalog_n_used": (C.c_int64, [_vp]),
+    "tpcf_binning_create": (C.c_int, [_vp, C.c_int, C.POINTER(AxisSpec), C.POINTER(AxisSpec), C.c_int32,
+                                      C.POINTER(_vp)]),
+    "tpcf_binning_destroy": (C.c_int, [_vp]),
+    "tpcf_binning_total_bins": (C.c_int, [_vp]),
+    "tpcf_binning_thresholds": (C.c_int, [_vp, C.c_int, _vp, C.c_int]),
+    "tpcf_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),
+    "tpcf_normalise_cross": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
+    "tpcf_ls_estimator": (C.c_double, [C.c_double, C.c_double, C.c_double]),
+}
+
+_LIB = None
+
+
+def header_symbols(header_path: str | None = None) -> list[str]:
+    """Function names declared in include/two_pcf_b200.h."""
+    import re
+    if header_path is None:
+        header_path = os.path.join(os.path.dirname(os.path.dirname(LIB_PATH)), os.pardir, "include",
+                                   "two_pcf_b200.h")
+    src = open(os.path.normpath(header_path)).read()
+    return sorted(set(re.findall(r"\b(tpcf_[a-z0-9_]+)\s*\(", src)))
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python two_pcf_b200/build.py` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOTYPES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _LIB = L
+    return _LIB

@@ -1,0 +1,82 @@
+"""Builds the engine in-tree: two_pcf_b200/lib/libtpcf_b200.so (C ABI of
+include/two_pcf_b200.h) for sm_100a only, plus the command-line driver.
+
+Host C++ is compiled with -ffp-contract=off: the threshold tables and the
+cosmology table must round every float/double operation once, like the
+reference's x86-64 build.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+LIB_DIR = os.path.join(PKG, "lib")
+BUILD_DIR = os.path.join(PKG, "lib", "obj")
+LIB_PATH = os.path.join(LIB_DIR, "libtpcf_b200.so")
+
+CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
+CXX = os.environ.get("TPCF_CXX", "g++")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+CU_SOURCES = ["grid.cu", "pair_count.cu"]
+CPP_SOURCES = ["axis.cpp", "capi.cpp"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    return r.stdout + r.stderr
+
+
+def _stale(obj, srcs):
+    if not os.path.exists(obj):
+        return True
+    t = os.path.getmtime(obj)
+    return any(os.path.getmtime(s) > t for s in srcs)
+
+
+def build(verbose: bool = False, ptxas_info: bool = False) -> str:
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))]
+    headers.append(os.path.join(ROOT, "include", "two_pcf_b200.h"))
+    jobs = []
+    objs = []
+    for f in CU_SOURCES:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD_DIR, f + ".o")
+        objs.append(obj)
+        if _stale(obj, [src] + headers):
+            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+                   "-I", CSRC, "-c", src, "-o", obj]
+            if ptxas_info:
+                cmd.insert(1, "-Xptxas=-v")
+            jobs.append(cmd)
+    for f in CPP_SOURCES:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD_DIR, f + ".o")
+        objs.append(obj)
+        if _stale(obj, [src] + headers):
+            jobs.append([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", CSRC,
+                         "-I", os.path.join(CUDA_HOME, "include"), "-c", src, "-o", obj])
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
+        outs = list(ex.map(_run, jobs))
+    if verbose:
+        for o in outs:
+            sys.stdout.write(o)
+    if jobs or not os.path.exists(LIB_PATH):
+        tmp = LIB_PATH + ".tmp"
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static"])
+        shutil.move(tmp, LIB_PATH)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, ptxas_info="--ptxas" in sys.argv))

@@ -1,0 +1,472 @@
+// C ABI of the engine (include/two_pcf_b200.h).  Validation happens here,
+// on the host, before anything is launched.
+#include "../../include/two_pcf_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "engine.h"
+
+struct tpcf_ctx {
+    tpcf::Ctx c;
+};
+struct tpcf_catalog {
+    tpcf::Catalog c;
+};
+struct tpcf_binning {
+    tpcf::Binning b;
+};
+
+namespace {
+
+int fail(tpcf_ctx *ctx, int status, const std::string &msg) {
+    if (ctx) ctx->c.last_error = msg;
+    return status;
+}
+
+int cuda_fail(tpcf_ctx *ctx, cudaError_t e, const char *where) {
+    int st = (e == cudaErrorMemoryAllocation) ? TPCF_E_OOM : TPCF_E_CUDA;
+    return fail(ctx, st, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+// The d_comov < 0 partition of GalaxyBoxes (src/boxes.cpp:15-26), applied to
+// an index permutation; returns the number of points the reference keeps.
+// The loop condition makes it stop before every point has been examined when
+// points are dropped, so some good points at the end are dropped too.
+int partition_kept(const double *dcom, int n, std::vector<int> &perm) {
+    perm.resize(n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    if (!dcom) return n;
+    int n_gals = 0;
+    for (int ii = 0; ii < n - ii + n_gals; ++ii) {
+        if (dcom[perm[n_gals]] < 0.0) {
+            std::swap(perm[n_gals], perm[n - 1 - ii + n_gals]);
+        } else {
+            ++n_gals;
+        }
+    }
+    return n_gals;
+}
+
+}  // namespace
+
+extern "C" {
+
+int tpcf_abi_version(void) { return TPCF_ABI_VERSION; }
+
+const char *tpcf_status_string(int status) {
+    switch (status) {
+    case TPCF_OK: return "ok";
+    case TPCF_E_INVALID_ARG: return "invalid argument";
+    case TPCF_E_OOM: return "out of device memory";
+    case TPCF_E_CUDA: return "CUDA error";
+    case TPCF_E_DEVICE_TIMEOUT: return "device wait timed out";
+    case TPCF_E_OVERFLOW: return "histogram overflow";
+    case TPCF_E_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown status";
+    }
+}
+
+int tpcf_create(int device, tpcf_ctx **out) {
+    if (!out) return TPCF_E_INVALID_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) return TPCF_E_CUDA;
+    if (device < 0 || device >= ndev) return TPCF_E_INVALID_ARG;
+    tpcf_ctx *ctx = new (std::nothrow) tpcf_ctx();
+    if (!ctx) return TPCF_E_OOM;
+    ctx->c.device = device;
+    e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&ctx->c.num_sms, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    ctx->c.smem_optin = (size_t)optin;
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete ctx;
+        return TPCF_E_CUDA;
+    }
+    ctx->c.own_stream = true;
+    *out = ctx;
+    return TPCF_OK;
+}
+
+int tpcf_destroy(tpcf_ctx *ctx) {
+    if (!ctx) return TPCF_E_INVALID_ARG;
+    cudaSetDevice(ctx->c.device);
+    if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    delete ctx;
+    return TPCF_OK;
+}
+
+const char *tpcf_last_error(const tpcf_ctx *ctx) { return ctx ? ctx->c.last_error.c_str() : "no context"; }
+
+int tpcf_set_stream(tpcf_ctx *ctx, void *stream) {
+    if (!ctx) return TPCF_E_INVALID_ARG;
+    if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
+    ctx->c.own_stream = false;
+    ctx->c.stream = (cudaStream_t)stream;
+    if (!stream) {
+        cudaError_t e = cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "stream");
+        ctx->c.own_stream = true;
+    }
+    return TPCF_OK;
+}
+
+int tpcf_set_refinement(tpcf_ctx *ctx, int m) {
+    if (!ctx || m < 0 || m > 3) return TPCF_E_INVALID_ARG;
+    ctx->c.refinement = m;
+    return TPCF_OK;
+}
+
+int tpcf_synchronize(tpcf_ctx *ctx) {
+    if (!ctx) return TPCF_E_INVALID_ARG;
+    cudaError_t e = cudaStreamSynchronize(ctx->c.stream);
+    return e == cudaSuccess ? TPCF_OK : cuda_fail(ctx, e, "synchronize");
+}
+
+int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const double *x_norm, const double *d_comov,
+                        const float *weight, const float *input_weight, const int32_t *jk_region,
+                        int32_t n_jk_regions, const int64_t *bitmask, int32_t n_mask_ints, tpcf_catalog **out) {
+    if (!ctx || !out) return TPCF_E_INVALID_ARG;
+    *out = nullptr;
+    if (n < 0 || n > 0x7fffffff - 1) return fail(ctx, TPCF_E_INVALID_ARG, "catalogue size out of range");
+    if (n > 0 && !xyz) return fail(ctx, TPCF_E_INVALID_ARG, "xyz is NULL");
+    if (n_jk_regions < 1 || n_jk_regions > tpcf::kMaxRegions)
+        return fail(ctx, TPCF_E_INVALID_ARG, "n_jk_regions must be in [1, 4096]");
+    if (n_mask_ints < 0 || n_mask_ints > tpcf::kMaxMaskInts || (n_mask_ints > 0 && !bitmask && n > 0))
+        return fail(ctx, TPCF_E_INVALID_ARG, "bad bitmask arguments");
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+
+    const int N = (int)n;
+    std::unique_ptr<tpcf_catalog> cat(new (std::nothrow) tpcf_catalog());
+    if (!cat) return TPCF_E_OOM;
+    tpcf::Catalog &c = cat->c;
+    c.ctx = &ctx->c;
+    c.n_all = n;
+    c.n_jk = n_jk_regions;
+    c.n_mask = bitmask ? n_mask_ints : 0;
+
+    std::vector<double> unit;
+    std::vector<double> dcom_v;
+    for (int i = 0; i < N; ++i)
+        for (int m = 0; m < 3; ++m)
+            if (!std::isfinite(xyz[3 * (size_t)i + m]))
+                return fail(ctx, TPCF_E_INVALID_ARG, "non-finite coordinate at index " + std::to_string(i));
+    if (!x_norm) {
+        // src/io.cpp:393-399: d_comov = sqrt(x.x), x_norm = x / d_comov.
+        unit.resize(3 * (size_t)N);
+        for (int i = 0; i < N; ++i) {
+            const double *p = xyz + 3 * (size_t)i;
+            double d = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
+            for (int m = 0; m < 3; ++m) unit[3 * (size_t)i + m] = p[m] / d;
+        }
+        x_norm = unit.data();
+    }
+    c.h_jk.assign(N, 0);
+    if (jk_region)
+        for (int i = 0; i < N; ++i) {
+            if (jk_region[i] < 0 || jk_region[i] >= n_jk_regions)
+                return fail(ctx, TPCF_E_INVALID_ARG, "jk_region out of range at index " + std::to_string(i));
+            c.h_jk[i] = jk_region[i];
+        }
+    c.h_w.assign(N, 1.0f);
+    c.unit_weights = true;
+    c.w_max = 0;
+    c.w_min = 0;
+    if (weight) {
+        for (int i = 0; i < N; ++i) {
+            if (!std::isfinite(weight[i])) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite weight");
+            c.h_w[i] = weight[i];
+            if (weight[i] != 1.0f) c.unit_weights = false;
+        }
+    }
+    c.n_kept = partition_kept(d_comov, N, c.h_kept);
+    for (int m = 0; m < 3; ++m) {
+        c.lo_kept[m] = c.lo_all[m] = 1e300;
+        c.hi_kept[m] = c.hi_all[m] = -1e300;
+    }
+    std::vector<char> is_kept(N, 0);
+    for (int k = 0; k < c.n_kept; ++k) is_kept[c.h_kept[k]] = 1;
+    for (int i = 0; i < N; ++i) {
+        const float a = std::fabs(c.h_w[i]);
+        if (is_kept[i]) c.w_max = std::max(c.w_max, a);
+        for (int m = 0; m < 3; ++m) {
+            const double v = xyz[3 * (size_t)i + m];
+            c.lo_all[m] = std::min(c.lo_all[m], v);
+            c.hi_all[m] = std::max(c.hi_all[m], v);
+            if (is_kept[i]) {
+                c.lo_kept[m] = std::min(c.lo_kept[m], v);
+                c.hi_kept[m] = std::max(c.hi_kept[m], v);
+            }
+        }
+    }
+    c.iw_max = c.w_max;
+    if (input_weight)
+        for (int i = 0; i < N; ++i) c.iw_max = std::max(c.iw_max, std::fabs(input_weight[i]));
+
+    cudaStream_t st = ctx->c.stream;
+#define CAT_TRY(expr)                                            \
+    do {                                                         \
+        cudaError_t _e = (expr);                                 \
+        if (_e != cudaSuccess) return cuda_fail(ctx, _e, "catalogue upload"); \
+    } while (0)
+    CAT_TRY(c.xyz.alloc(3 * (size_t)N));
+    CAT_TRY(c.unit.alloc(3 * (size_t)N));
+    CAT_TRY(c.w.alloc(N));
+    CAT_TRY(c.jk.alloc(N));
+    CAT_TRY(c.kept.alloc(c.n_kept));
+    if (N > 0) {
+        CAT_TRY(cudaMemcpyAsync(c.xyz.p, xyz, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+        CAT_TRY(cudaMemcpyAsync(c.unit.p, x_norm, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
+        CAT_TRY(cudaMemcpyAsync(c.w.p, c.h_w.data(), sizeof(float) * N, cudaMemcpyHostToDevice, st));
+        CAT_TRY(cudaMemcpyAsync(c.jk.p, c.h_jk.data(), sizeof(int) * N, cudaMemcpyHostToDevice, st));
+    }
+    if (c.n_kept > 0)
+        CAT_TRY(cudaMemcpyAsync(c.kept.p, c.h_kept.data(), sizeof(int) * c.n_kept, cudaMemcpyHostToDevice, st));
+    if (input_weight) {
+        CAT_TRY(c.iw.alloc(N));
+        if (N > 0) CAT_TRY(cudaMemcpyAsync(c.iw.p, input_weight, sizeof(float) * N, cudaMemcpyHostToDevice, st));
+    }
+    if (c.n_mask > 0) {
+        CAT_TRY(c.masks.alloc((size_t)N * c.n_mask));
+        if (N > 0)
+            CAT_TRY(cudaMemcpyAsync(c.masks.p, bitmask, sizeof(long long) * (size_t)N * c.n_mask,
+                                    cudaMemcpyHostToDevice, st));
+    }
+    CAT_TRY(cudaStreamSynchronize(st));
+#undef CAT_TRY
+    *out = cat.release();
+    return TPCF_OK;
+}
+
+int tpcf_catalog_destroy(tpcf_catalog *cat) {
+    if (!cat) return TPCF_E_INVALID_ARG;
+    delete cat;
+    return TPCF_OK;
+}
+
+int64_t tpcf_catalog_n_used(const tpcf_catalog *cat) { return cat ? cat->c.n_kept : -1; }
+
+int tpcf_binning_create(tpcf_ctx *ctx, int mode, const tpcf_axis_spec *ax1, const tpcf_axis_spec *ax2,
+                        int32_t n_jk_regions, tpcf_binning **out) {
+    if (!out || !ax1) return TPCF_E_INVALID_ARG;
+    *out = nullptr;
+    if (mode < TPCF_MONOPOLE || mode > TPCF_ANGULAR) return fail(ctx, TPCF_E_INVALID_ARG, "bad mode");
+    if ((mode == TPCF_SIGMA_PI || mode == TPCF_S_MU) && !ax2) return fail(ctx, TPCF_E_INVALID_ARG, "ax2 required");
+    if (n_jk_regions < 1 || n_jk_regions > tpcf::kMaxRegions) return fail(ctx, TPCF_E_INVALID_ARG, "bad n_jk");
+    auto bad_axis = [](const tpcf_axis_spec *a) {
+        return a->n_bins < 1 || a->n_bins > tpcf::kMaxBins1D || !std::isfinite(a->min) || !std::isfinite(a->max) ||
+               !(a->max > a->min);
+    };
+    if (bad_axis(ax1)) return fail(ctx, TPCF_E_INVALID_ARG, "bad axis 1");
+    std::unique_ptr<tpcf_binning> b(new (std::nothrow) tpcf_binning());
+    if (!b) return TPCF_E_OOM;
+    tpcf::Binning &B = b->b;
+    B.mode = mode;
+    B.n_jk = n_jk_regions;
+    B.ax1 = tpcf::make_axis(ax1->min, ax1->max, ax1->n_bins, ax1->log_base);
+    B.nb1 = ax1->n_bins;
+    B.nb2 = 1;
+    using tpcf::ValueSpace;
+    if (mode == TPCF_MONOPOLE) {
+        // src/correlators.cpp:13-14
+        B.max_r_sq = B.ax1.max * B.ax1.max;
+        B.min_r_sq = B.ax1.min * B.ax1.min;
+        B.vs1 = ValueSpace::Sqrt;
+    } else if (mode == TPCF_SIGMA_PI) {
+        if (bad_axis(ax2)) return fail(ctx, TPCF_E_INVALID_ARG, "bad axis 2");
+        B.ax2 = tpcf::make_axis(ax2->min, ax2->max, ax2->n_bins, ax2->log_base);
+        B.nb2 = ax2->n_bins;
+        // src/correlators.cpp:192-195
+        B.max_r_sq = B.ax1.max * B.ax1.max + B.ax2.max * B.ax2.max;
+        B.min_r_sq = B.ax1.min * B.ax1.min;
+        if (B.ax1.min > B.ax2.min) B.min_r_sq = B.ax2.min * B.ax2.min;
+        B.vs1 = ValueSpace::Sqrt;  // sigma = sqrtf(s^2 - pi^2)
+        B.vs2 = ValueSpace::Direct;
+    } else if (mode == TPCF_S_MU) {
+        if (ax2->n_bins < 1 || ax2->n_bins > tpcf::kMaxBins1D) return fail(ctx, TPCF_E_INVALID_ARG, "bad mu bins");
+        // src/correlators.cpp:436-437: Hist2D(s..., 0.0, 1.0, mu_n_bins, 0)
+        B.ax2 = tpcf::make_axis(0.0, 1.0, ax2->n_bins, 0.0);
+        B.nb2 = ax2->n_bins;
+        B.max_r_sq = B.ax1.max * B.ax1.max;
+        B.min_r_sq = B.ax1.min * B.ax1.min;
+        B.vs1 = ValueSpace::Sqrt;
+        B.vs2 = ValueSpace::Direct;
+    } else {
+        B.vs1 = ValueSpace::Direct;  // binned on (float)(1 - cos theta)
+        B.max_r_sq = B.ax1.max;
+        B.min_r_sq = 0;
+    }
+    B.nb = B.nb1 * B.nb2;
+    if (B.nb > tpcf::kMaxBinsTotal) return fail(ctx, TPCF_E_UNSUPPORTED, "more than 8192 bins");
+    // Threshold domains: the values a binned pair can present.  s^2 and
+    // sigma^2 = s^2 - pi^2 lie in [0, max_r_sq); |pi| <= s (up to rounding);
+    // mu = |pi| / s lies in [0, ~1]; 1 - cos(theta) in [-2, 2] (tiny negative
+    // values occur and land in bin 0 in the reference).
+    const float sq = B.max_r_sq;
+    const float rmax_f = (float)(std::sqrt((double)sq) * 1.01 + 1.0);
+    if (mode == TPCF_ANGULAR) {
+        B.t1 = tpcf::build_thresholds(B.ax1, B.vs1, -2.0f, 2.0f);
+    } else {
+        B.t1 = tpcf::build_thresholds(B.ax1, B.vs1, 0.0f, sq);
+    }
+    if (mode == TPCF_SIGMA_PI) B.t2 = tpcf::build_thresholds(B.ax2, B.vs2, 0.0f, rmax_f);
+    else if (mode == TPCF_S_MU) B.t2 = tpcf::build_thresholds(B.ax2, B.vs2, 0.0f, 2.0f);
+    else B.t2.assign(1, 0.0f);
+    // Every in-range pair has |x1_m - x2_m| below sqrt(max_r_sq) up to a few
+    // float roundings.
+    B.rmax_bound = std::sqrt((double)B.max_r_sq) * (1.0 + 1e-6) + 1e-30;
+    *out = b.release();
+    return TPCF_OK;
+}
+
+int tpcf_binning_destroy(tpcf_binning *bin) {
+    if (!bin) return TPCF_E_INVALID_ARG;
+    delete bin;
+    return TPCF_OK;
+}
+
+int tpcf_binning_total_bins(const tpcf_binning *bin) { return bin ? bin->b.nb : -TPCF_E_INVALID_ARG; }
+
+int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int cap) {
+    if (!bin || (axis != 1 && axis != 2) || (cap > 0 && !out)) return -TPCF_E_INVALID_ARG;
+    const std::vector<float> &t = axis == 1 ? bin->b.t1 : bin->b.t2;
+    for (int k = 0; k < (int)t.size() && k < cap; ++k) out[k] = t[k];
+    return (int)t.size();
+}
+
+int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+               int precision, double *full_out, double *region_out, tpcf_stats *stats) {
+    if (!ctx || !a || !bin || !full_out) return TPCF_E_INVALID_ARG;
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
+    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "angular binning: use the angular counter");
+    if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
+        return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    auto t0 = std::chrono::steady_clock::now();
+    tpcf::CountRequest req;
+    req.a = &a->c;
+    req.b = b ? &b->c : nullptr;
+    req.bin = &bin->b;
+    req.exact_fp64 = precision == TPCF_FP64;
+    tpcf::Stats st;
+    tpcf::Error err{0, ""};
+    const int nb = bin->b.nb;
+    if ((b ? b->c.n_kept : 0) == 0 && b) {
+        std::memset(full_out, 0, sizeof(double) * nb);
+        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
+        return TPCF_OK;
+    }
+    if (a->c.n_kept == 0) {
+        std::memset(full_out, 0, sizeof(double) * nb);
+        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
+        return TPCF_OK;
+    }
+    int rc = tpcf::run_count(&ctx->c, req, full_out, region_out, &st, &err);
+    if (rc) return fail(ctx, rc, err.msg);
+    if (stats) {
+        stats->candidates = st.candidates;
+        stats->in_range = st.in_range;
+        stats->guard_evals = st.guard;
+        stats->overflow_updates = st.overflow;
+        stats->work_items = st.items;
+        stats->ms_kernel = st.ms_kernel;
+        stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return TPCF_OK;
+}
+
+static int reference_form(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                          int precision, double *full, double *sub, tpcf_stats *stats) {
+    if (!sub) return fail(ctx, TPCF_E_INVALID_ARG, "sub_hist is NULL");
+    int rc = tpcf_count(ctx, a, b, bin, precision, full, sub, stats);
+    if (rc) return rc;
+    const int nb = bin->b.nb, nj = bin->b.n_jk;
+    // invert_jk_hists (src/hist.cpp:270-277, :464-471)
+    for (int r = 0; r < nj; ++r)
+        for (int k = 0; k < nb; ++k) sub[(size_t)r * nb + k] = full[k] - sub[(size_t)r * nb + k];
+    if (!b) {
+        // multiply_hists(2.0) (src/hist.cpp:279-288, :473-482)
+        for (int k = 0; k < nb; ++k) full[k] *= 2.0;
+        for (size_t k = 0; k < (size_t)nb * nj; ++k) sub[k] *= 2.0;
+    }
+    return TPCF_OK;
+}
+
+int tpcf_auto_pair_count(tpcf_ctx *ctx, const tpcf_catalog *cat, const tpcf_binning *bin, int precision,
+                         double *full_hist, double *sub_hist, tpcf_stats *stats) {
+    return reference_form(ctx, cat, nullptr, bin, precision, full_hist, sub_hist, stats);
+}
+
+int tpcf_cross_pair_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                          int precision, double *full_hist, double *sub_hist, tpcf_stats *stats) {
+    if (!b) return TPCF_E_INVALID_ARG;
+    return reference_form(ctx, a, b, bin, precision, full_hist, sub_hist, stats);
+}
+
+int tpcf_normalise_auto(const tpcf_catalog *cat, int32_t nb, double *full, double *sub) {
+    if (!cat || !full || !sub || nb < 1) return TPCF_E_INVALID_ARG;
+    const tpcf::Catalog &c = cat->c;
+    const int nj = c.n_jk;
+    const int n = c.n_kept;
+    // src/hist.cpp:290-321
+    double sw = 0.0;
+    std::vector<double> swj(nj, 0.0);
+    std::vector<int> nj_cnt(nj, 0);
+    for (int k = 0; k < n; ++k) {
+        const int i = c.h_kept[k];
+        sw += c.h_w[i];
+        swj[c.h_jk[i]] += c.h_w[i];
+        ++nj_cnt[c.h_jk[i]];
+    }
+    for (int r = 0; r < nj; ++r) swj[r] = sw - swj[r];
+    sw = sw * sw * (1.0 - 1.0 / (double)n);
+    for (int r = 0; r < nj; ++r) swj[r] = swj[r] * swj[r] * (1.0 - 1.0 / nj_cnt[r]);
+    for (int k = 0; k < nb; ++k) full[k] /= sw;
+    for (int r = 0; r < nj; ++r)
+        for (int k = 0; k < nb; ++k) sub[(size_t)r * nb + k] /= swj[r];
+    return TPCF_OK;
+}
+
+int tpcf_normalise_cross(const tpcf_catalog *a, const tpcf_catalog *b, int32_t nb, double *full, double *sub) {
+    if (!a || !b || !full || !sub || nb < 1 || a->c.n_jk != b->c.n_jk) return TPCF_E_INVALID_ARG;
+    const int nj = a->c.n_jk;
+    // src/hist.cpp:323-367
+    auto sums = [nj](const tpcf::Catalog &c, double &s, std::vector<double> &sj) {
+        s = 0.0;
+        sj.assign(nj, 0.0);
+        for (int k = 0; k < c.n_kept; ++k) {
+            const int i = c.h_kept[k];
+            s += c.h_w[i];
+            sj[c.h_jk[i]] += c.h_w[i];
+        }
+        for (int r = 0; r < nj; ++r) sj[r] = s - sj[r];
+    };
+    double s1, s2;
+    std::vector<double> j1, j2;
+    sums(a->c, s1, j1);
+    sums(b->c, s2, j2);
+    s1 *= s2;
+    for (int r = 0; r < nj; ++r) j1[r] *= j2[r];
+    for (int k = 0; k < nb; ++k) full[k] /= s1;
+    for (int r = 0; r < nj; ++r)
+        for (int k = 0; k < nb; ++k) sub[(size_t)r * nb + k] /= j1[r];
+    return TPCF_OK;
+}
+
+double tpcf_ls_estimator(double dd, double dr, double rr) {
+    if (rr == 0) return 0;
+    return dd / rr - 2.0 * dr / rr + 1.0;
+}
+
+}  // extern "C"

@@ -1,0 +1,135 @@
+// Internal engine objects behind the C ABI (include/two_pcf_b200.h).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "axis.h"
+#include "tpcf_common.h"
+
+namespace tpcf {
+
+// Device buffer with RAII ownership.
+template <typename T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc((void **)&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
+
+struct Error {
+    int status;
+    std::string msg;
+};
+
+// The points of one catalogue sorted into cubic cells of side `side` on the
+// lattice x = k * side (k integer), with points inside a cell ordered by
+// jackknife region.  Replaces GalaxyBoxes (src/boxes.cpp:10-163).
+struct Grid {
+    double side = 0;
+    int kmin[3] = {0, 0, 0};
+    int dim[3] = {1, 1, 1};
+    bool morton = false;  // dense cell id = Morton code of the local cell coords
+    int ncell = 0;        // size of the dense cell table
+    int n = 0;            // points in the grid
+    bool subset_kept = true;
+    DevBuf<float4> pos;   // (x - kx*side, y - ky*side, z - kz*side, weight), float
+    DevBuf<float4> aux;   // (x_norm as float, jk as int bits)
+    DevBuf<int> idx;      // original catalogue index
+    DevBuf<double4> xyz_s;   // sorted double coordinates (exact path, FP64 path)
+    DevBuf<double4> unit_s;  // sorted double unit vectors
+    DevBuf<int> cell_start;  // ncell + 1
+    DevBuf<int3> cell_coord; // local coords of each dense cell id (for offsets)
+    DevBuf<int> region_start;  // ncell + 1, CSR of distinct jk regions per cell
+    DevBuf<int> regions;
+    std::vector<int> h_cell_start;  // host copy for the work-list build
+    std::vector<int> h_region_start;
+    std::vector<int> h_regions;
+    bool has_fp64 = false;
+};
+
+struct Ctx;
+
+struct Catalog {
+    Ctx *ctx = nullptr;
+    int64_t n_all = 0;
+    int n_kept = 0;
+    int n_mask = 0;
+    int n_jk = 1;
+    bool unit_weights = true;  // every weight == 1.0f
+    float w_min = 1, w_max = 1, iw_min = 1, iw_max = 1;
+    double lo_kept[3], hi_kept[3], lo_all[3], hi_all[3];
+    DevBuf<double> xyz, unit;
+    DevBuf<float> w, iw;
+    DevBuf<int> jk;
+    DevBuf<long long> masks;
+    DevBuf<int> kept;             // indices kept by the d_comov partition
+    std::vector<float> h_w;       // host copies used by normalisation
+    std::vector<int> h_jk;
+    std::vector<int> h_kept;
+    std::map<std::string, std::unique_ptr<Grid>> grids;  // cached by geometry
+};
+
+struct Binning {
+    int mode = 0;
+    int n_jk = 1;
+    AxisParams ax1, ax2;
+    int nb1 = 0, nb2 = 1, nb = 0;
+    float min_r_sq = 0, max_r_sq = 0;  // float range test of the reference
+    double rmax_bound = 0;             // every in-range pair is closer than this on each axis
+    std::vector<float> t1, t2;         // threshold tables (see axis.h)
+    ValueSpace vs1 = ValueSpace::Direct, vs2 = ValueSpace::Direct;
+};
+
+struct Stats {
+    unsigned long long candidates = 0, in_range = 0, guard = 0, overflow = 0, items = 0;
+    double ms_kernel = 0, ms_total = 0;
+};
+
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    int refinement = 0;  // 0 = automatic
+    DevBuf<unsigned long long> counters;
+    DevBuf<int> err_flag;
+};
+
+// grid.cu
+int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_fp64, Grid **out, Error *err);
+
+// pair_count.cu
+struct CountRequest {
+    const Catalog *a = nullptr;
+    const Catalog *b = nullptr;  // nullptr: auto count of a
+    const Binning *bin = nullptr;
+    bool exact_fp64 = false;     // plain FP64 path for every candidate
+    int weight_kind = W_PLAIN;
+    int refinement = 0;
+};
+int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);
+
+}  // namespace tpcf

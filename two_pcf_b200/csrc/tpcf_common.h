@@ -1,0 +1,48 @@
+// Shared host/device definitions of the pair-counting engine.
+#pragma once
+#include <cstdint>
+
+#ifdef __CUDACC__
+#define TPCF_HD __host__ __device__
+#else
+#define TPCF_HD
+#endif
+
+namespace tpcf {
+
+enum Mode { MODE_MONOPOLE = 0, MODE_SIGMA_PI = 1, MODE_S_MU = 2, MODE_ANGULAR = 3 };
+
+// How a pair's weight is formed (src/correlators.cpp:40 for PLAIN;
+// src/correlators_invpweight.cpp:51-77 for INVP_DD, :184-189 for INVP_DR,
+// :743-764 / :853 / :901 / :968 for the angular kinds).
+enum WeightKind {
+    W_UNIT = 0,       // every weight is 1.0: integer counts
+    W_PLAIN = 1,      // w1 * w2 (float product)
+    W_INVP_DD = 2,    // iw1 * iw2 * (float)(interp(1-cos) * n_runs / popc)
+    W_INVP_DR = 3,    // (float)((w1 * w2) * interp(1-cos))
+    W_ANG_INPUT = 4,  // iw1 * iw2 (angular DD/DR: input weights)
+    W_ANG_INVP = 5,   // iw1 * iw2 * (n_runs / popc)  (angular DD inverse-p)
+};
+
+// Histogram bins are decided by comparing a float value with a float
+// threshold table: bin(v) = #{k : T[k] <= v} - 1, valid when 0 <= bin < n.
+// The tables come from the host (axis.cpp), which evaluates the reference's
+// own Axis::bin_num on the host's libm.
+constexpr int kMaxBins1D = 256;      // per axis
+constexpr int kMaxBinsTotal = 8192;  // per histogram
+constexpr int kMaxMaskInts = 32;     // 64-bit masks per object for inverse-p weights
+constexpr int kMaxRegions = 4096;    // jackknife regions
+
+// One unit of device work: a chunk of cell A against all of cell B.
+struct WorkItem {
+    int a_start;  // first point of the A chunk (sorted order, grid A)
+    int a_len;
+    int b_start;  // first point of cell B (sorted order, grid B)
+    int b_len;
+    int a_cell;   // dense cell index in grid A
+    int b_cell;   // dense cell index in grid B
+    int self;     // 1 when A and B are the same cell of the same catalogue (auto count)
+    int a_cell_start;  // first point of the whole A cell (for the self-pair ordering)
+};
+
+}  // namespace tpcf
