@@ -1,0 +1,403 @@
+#!/usr/bin/env python
+"""Benchmark of the grid-binned pair-counting hot path on B200.
+
+Workload (one "step"): the equatorial survey-slab configuration — 1M
+clustered data objects and 5M randoms (ra in [0, 60] deg, dec in
+[-10, 10] deg, z ~ N(0.3, 0.08) on [0.1, 0.5], flat LCDM Omega_m = 0.25),
+lognormal(0, 0.2) weights, 100 jackknife regions on a 10 x 10 ra/dec grid —
+counted as the reference's driver does it (src/main.cpp:63-70): sigma-pi
+(50 x 50 linear bins over 0-50 Mpc/h) DD, DR and RR, then s-mu (40 log bins,
+base 1.3, 0-100 Mpc/h, x 50 mu bins) DD, DR and RR.  Each step rebuilds the
+cell grids (the GalaxyBoxes stage) from the resident catalogues.
+
+Metric: in-range pairs per second (pairs passing the reference's float range
+test, auto pairs counted once) on the FP32+guard path, with the plain FP64
+path run on the same step for comparison and bit-exactness of the two
+paths' histograms checked.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--scale f]
+
+Under torchrun each rank runs its own seeded copy of the workload (weak
+scaling, no data-path collective); the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "in-range pairs/sec, FP32+guard vs FP64 GPU path at bit-exact counts"
+UNIT = "pairs/s"
+SIGMA_PI_AXES = ((0.0, 50.0, 1.0, 50), (0.0, 50.0, 1.0, 50))
+S_MU_AXES = ((0.0, 100.0, 1.3, 40), (0.0, 1.0, 0.0, 50))
+F_MODE = {1: 16, 2: 13, 0: 0}   # FP32 flops per in-range pair beyond the 8 of s^2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    p.add_argument("--scale", type=float, default=1.0, help="fraction of the catalogue sizes (quick runs)")
+    p.add_argument("--no-fp64", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        import datetime
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
+    return ws, rank, local
+
+
+def dist_max(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier(ws: int):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def make_workload(seed: int, scale: float):
+    from two_pcf_b200 import synthetic
+    w = synthetic.survey_catalogue(seed=seed, n_data=max(1000, int(1_000_000 * scale)),
+                                   n_rand=max(5000, int(5_000_000 * scale)))
+    return w
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        os.makedirs(os.path.dirname(self.path), exist_ok=True)
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.fh,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def count_step(tp, ctx, D, R, bins, precision, release=True):
+    """One pass: grids rebuilt, then DD, DR, RR for each binning.
+    Returns (in_range, candidates, kernel_ms, flops, hists)."""
+    if release:
+        for c in (D, R):
+            tp._capi.lib().tpcf_catalog_release_cache(c._h)
+    in_range = cand = 0
+    kms = 0.0
+    flops = 0.0
+    hists = []
+    for mode, b in bins:
+        for a, bb in ((D, None), (D, R), (R, None)):
+            full, reg, st = tp.count(ctx, a, bb, b, precision)
+            in_range += st["in_range"]
+            cand += st["candidates"]
+            kms += st["ms_kernel"]
+            flops += 8.0 * st["candidates"] + F_MODE[mode] * st["in_range"]
+            hists.append((full, reg))
+    return in_range, cand, kms, flops, hists
+
+
+def cpu_reference_sample(w, target_s: float = 12.0, ctx=None):
+    """Time the reference's own OpenMP code (oracle/_ref, built from the
+    reference sources) on a random subsample of the same workload.  The
+    in-range pair count of the sample comes from the engine on the identical
+    sample.  Returns a cpu_baseline dict."""
+    from oracle import refl
+    import two_pcf_b200 as tp
+    n_threads = os.cpu_count() or 1
+    rng = np.random.default_rng(7)
+
+    def run(frac):
+        d, r = w["data"], w["rand"]
+        nd = max(200, int(d["xyz"].shape[0] * frac))
+        nr = max(1000, int(r["xyz"].shape[0] * frac))
+        di = np.sort(rng.choice(d["xyz"].shape[0], nd, replace=False))
+        ri = np.sort(rng.choice(r["xyz"].shape[0], nr, replace=False))
+
+        def cat(c, idx):
+            return {"xyz": c["xyz"][idx], "unit": c["x_norm"][idx], "dcom": c["d_comov"][idx],
+                    "w": c["weight"][idx], "jk": c["jk"][idx]}
+
+        cd, cr = cat(d, di), cat(r, ri)
+        t0 = time.perf_counter()
+        for ax, mode in ((SIGMA_PI_AXES, refl.SIGMA_PI), (S_MU_AXES, refl.S_MU)):
+            axes = (*ax[0][:3], ax[0][3], *ax[1][:3], ax[1][3])
+            refl.count_3d(mode, cd, cr, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
+            refl.count_3d(mode, cd, cr, is_auto=False, n_jk=100, axes=axes, n_threads=n_threads)
+            refl.count_3d(mode, cr, cd, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
+        dt = time.perf_counter() - t0
+        pairs = None
+        if ctx is not None:
+            D = tp.Catalog(ctx, cd["xyz"], cd["unit"], cd["dcom"], cd["w"], None, cd["jk"], 100)
+            R = tp.Catalog(ctx, cr["xyz"], cr["unit"], cr["dcom"], cr["w"], None, cr["jk"], 100)
+            bins = [(1, tp.Binning(ctx, tp.SIGMA_PI, *SIGMA_PI_AXES, 100)),
+                    (2, tp.Binning(ctx, tp.S_MU, *S_MU_AXES, 100))]
+            pairs = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)[0]
+        return dt, pairs, nd, nr
+
+    frac = 0.01
+    dt, pairs, nd, nr = run(frac)
+    if dt < target_s / 8:
+        frac = min(1.0, frac * np.sqrt(target_s / max(dt, 1e-3)))
+        dt, pairs, nd, nr = run(frac)
+    return {"value": (pairs / dt) if pairs else None, "unit": UNIT, "cores": n_threads, "kind": "reference",
+            "seconds": dt, "in_range_pairs": pairs,
+            "sample": f"random {frac:.3f} subsample of the workload: {nd} data, {nr} randoms; sigma-pi and s-mu "
+                      f"DD+DR+RR through the reference's auto_/cross_pair_count_* built from its sources "
+                      f"(g++ -O3 -fopenmp), {n_threads} OpenMP threads"}
+
+
+def run_reference_arm(args, ws, rank):
+    """--impl reference: the reference's CPU implementation on the host cores."""
+    if rank != 0:
+        return
+    from oracle import refl
+    ctx = None
+    try:
+        import torch
+        if torch.cuda.is_available():
+            import two_pcf_b200 as tp
+            ctx = tp.Context(0)
+    except Exception:
+        ctx = None
+    if not refl.available("plain"):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtwopcf_ref_plain.so not built "
+                          "(oracle/build_ref.sh needs the reference sources)"}))
+        return
+    w = make_workload(2, args.scale)
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    vals, secs, base = [], [], None
+    for s in range(args.steps):
+        base = cpu_reference_sample(w, target_s=8.0, ctx=ctx)
+        if base["value"] is None:
+            # no GPU for the pair tally: count in-range pairs with the oracle restatement is too slow here
+            print(json.dumps({"impl": "reference", "unavailable": "needs a GPU to tally in-range pairs"}))
+            return
+        vals.append(base["value"])
+        secs.append(base["seconds"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+            "data": "synthetic", "config": {"workload": "survey slab 1M data / 5M randoms, sigma-pi 50x50 + "
+                                                        "s-mu 40x50, 100 jackknife regions, weighted",
+                                            "sample": base["sample"]},
+            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup()
+    if args.impl == "reference":
+        run_reference_arm(args, ws, rank)
+        return
+    import torch
+    import two_pcf_b200 as tp
+    torch.cuda.set_device(local)
+    ctx = tp.Context(local)
+    stream = torch.cuda.Stream(device=local)
+    ctx.set_stream(stream.cuda_stream)
+
+    w = make_workload(2 + rank, args.scale)
+    n_jk = w["n_jk"]
+    d, r = w["data"], w["rand"]
+    D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], n_jk)
+    R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], n_jk)
+    bins = [(1, tp.Binning(ctx, tp.SIGMA_PI, *SIGMA_PI_AXES, n_jk)),
+            (2, tp.Binning(ctx, tp.S_MU, *S_MU_AXES, n_jk))]
+    fp32_tflops, atom_rate = 0.0, 0.0
+    import ctypes as C
+    a1, a2 = C.c_double(), C.c_double()
+    if tp._capi.lib().tpcf_measure_peaks(ctx._h, C.byref(a1), C.byref(a2)) == 0:
+        fp32_tflops, atom_rate = a1.value, a2.value
+    flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
+
+    for _ in range(max(3, args.warmup)):
+        count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)
+    torch.cuda.synchronize()
+
+    launches0 = tp._capi.lib().tpcf_kernel_launches(ctx._h)
+    tot_in = tot_cand = 0
+    tot_kms = tot_flops = 0.0
+    step_ms = []
+    with ClockSampler(local) as clk:
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        for _ in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.random_(0, 255)   # evict the L2 between steps
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            n_in, n_c, kms, fl, hists = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)
+            e1.record(stream)
+            e1.synchronize()
+            step_ms.append(e0.elapsed_time(e1))
+            tot_in += n_in
+            tot_cand += n_c
+            tot_kms += kms
+            tot_flops += fl
+        torch.cuda.synchronize()
+        dist_barrier(ws)
+    launches = tp._capi.lib().tpcf_kernel_launches(ctx._h) - launches0
+    total_ms = dist_max(sum(step_ms), ws)
+    value = tot_in * ws / (total_ms * 1e-3)   # every rank processes the same-sized workload
+    clocks = clk.summary()
+
+    # plain FP64 path on one step, and bit-exactness of the two paths
+    fp64 = None
+    if not args.no_fp64:
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        n64, _, kms64, _, h64 = count_step(tp, ctx, D, R, bins, tp.FP64)
+        e1.record(stream)
+        e1.synchronize()
+        ms64 = e0.elapsed_time(e1)
+        exact = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(hists, h64))
+        fp64 = {"value": n64 / (ms64 * 1e-3), "ms_per_step": ms64, "kernel_ms": kms64,
+                "speedup_fp32_guard": (ms64 / (sum(step_ms) / len(step_ms))),
+                "bit_exact_histograms": bool(exact), "in_range_equal": int(n64) == int(tot_in // args.steps)}
+
+    # end to end through the C ABI: pinned host catalogues in, histograms out
+    e2e = None
+    if not args.no_e2e:
+        pin = {}
+        for name, c in (("d", d), ("r", r)):
+            pin[name] = {k: torch.from_numpy(np.ascontiguousarray(c[k])).pin_memory().numpy()
+                         for k in ("xyz", "x_norm", "d_comov", "weight", "jk")}
+        h2d = sum(pin[n][k].nbytes for n in pin for k in ("xyz", "x_norm", "weight", "jk"))
+        d2h = sum(b.nb * (1 + n_jk) * 8 * 3 for _, b in bins)
+        e_ms = []
+        e_in = 0
+        for s in range(args.steps + 1):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            Dp = tp.Catalog(ctx, pin["d"]["xyz"], pin["d"]["x_norm"], pin["d"]["d_comov"], pin["d"]["weight"], None,
+                            pin["d"]["jk"], n_jk)
+            Rp = tp.Catalog(ctx, pin["r"]["xyz"], pin["r"]["x_norm"], pin["r"]["d_comov"], pin["r"]["weight"], None,
+                            pin["r"]["jk"], n_jk)
+            n_in = count_step(tp, ctx, Dp, Rp, bins, tp.FP32_GUARD, release=False)[0]
+            torch.cuda.synchronize()
+            dt = time.perf_counter() - t0
+            Dp.close()
+            Rp.close()
+            if s > 0:   # first pass warms the allocator
+                e_ms.append(dt * 1e3)
+                e_in += n_in
+        e_total = dist_max(sum(e_ms), ws)
+        e2e = {"value": e_in * ws / (e_total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": e_total / len(e_ms)}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            from oracle import refl
+            if refl.available("plain"):
+                cpu = cpu_reference_sample(w, ctx=ctx)
+        except Exception as ex:  # report, do not fail the bench
+            cpu = {"value": None, "error": str(ex)}
+
+    achieved = tot_flops / (tot_kms * 1e-3) / 1e12 if tot_kms > 0 else 0.0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "survey slab: 1M clustered data + 5M randoms, weights lognormal(0,0.2), 100 jk "
+                               "regions; sigma-pi 50x50 linear 0-50 + s-mu 40 log(1.3) 0-100 x 50 mu; "
+                               "DD+DR+RR each; grids rebuilt every step",
+                   "scale": args.scale, "n_data": int(d["xyz"].shape[0]), "n_rand": int(r["xyz"].shape[0]),
+                   "l2": "inputs larger than L2 (sorted tiles 192 MB + catalogues) and a 256 MB L2 flush "
+                         "between steps",
+                   "parallelism": f"replicas{ws}" if ws > 1 else "single"},
+        "in_range_pairs_per_step": tot_in // args.steps, "candidates_per_step": tot_cand // args.steps,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_tflops if fp32_tflops else None, "traffic": None,
+                     "peak_source": "FP32 FMA probe kernel run live on this GPU (tpcf_measure_peaks); "
+                                    "MEASURED_PEAKS.json has no FP32 figure",
+                     "flops_model": "8 per candidate pair + 16 (sigma-pi) / 13 (s-mu) per in-range pair",
+                     "kernel_ms_per_step": tot_kms / args.steps,
+                     "smem_atomic_peak_per_s": atom_rate},
+        "fp64_path": fp64, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line))
+    ctx.close()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -99,6 +99,8 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
 int tpcf_catalog_destroy(tpcf_catalog *cat);
 /* Points kept by the d_comov partition (GalaxyBoxes::n_gals). */
 int64_t tpcf_catalog_n_used(const tpcf_catalog *cat);
+/* Drop the cell grids cached on the catalogue; the next count rebuilds them. */
+int tpcf_catalog_release_cache(tpcf_catalog *cat);
 
 /* Histogram definition.  ax2 is the pi axis for TPCF_SIGMA_PI and supplies
  * only n_bins (mu bins on [0, 1]) for TPCF_S_MU; it is ignored otherwise.
@@ -138,6 +140,13 @@ int tpcf_normalise_cross(const tpcf_catalog *a, const tpcf_catalog *b, int32_t n
 
 /* ls_estimator (src/io.cpp:643-651). */
 double tpcf_ls_estimator(double dd, double dr, double rr);
+
+/* Diagnostics (no counterpart in the reference): kernels launched by this
+ * context so far, and the device's FP32 FMA rate (TFLOP/s) and returning
+ * 32-bit shared-memory atomic rate (per second) measured with short probe
+ * kernels — the two pipes that bound the pair-count kernels. */
+uint64_t tpcf_kernel_launches(const tpcf_ctx *ctx);
+int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s);
 
 #ifdef __cplusplus
 }

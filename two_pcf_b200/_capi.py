@@ -51,6 +51,7 @@ _PROTOTYPES = {
                                       C.POINTER(_vp)]),
     "tpcf_catalog_destroy": (C.c_int, [_vp]),
     "tpcf_catalog_n_used": (C.c_int64, [_vp]),
+    "tpcf_catalog_release_cache": (C.c_int, [_vp]),
     "tpcf_binning_create": (C.c_int, [_vp, C.c_int, C.POINTER(AxisSpec), C.POINTER(AxisSpec), C.c_int32,
                                       C.POINTER(_vp)]),
     "tpcf_binning_destroy": (C.c_int, [_vp]),
@@ -62,6 +63,8 @@ _PROTOTYPES = {
     "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),
     "tpcf_normalise_cross": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
     "tpcf_ls_estimator": (C.c_double, [C.c_double, C.c_double, C.c_double]),
+    "tpcf_kernel_launches": (C.c_uint64, [_vp]),
+    "tpcf_measure_peaks": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
 _LIB = None

@@ -25,7 +25,7 @@ NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
 CXX = os.environ.get("TPCF_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_SOURCES = ["grid.cu", "pair_count.cu"]
+CU_SOURCES = ["grid.cu", "pair_count.cu", "diag.cu"]
 CPP_SOURCES = ["axis.cpp", "capi.cpp"]
 
 

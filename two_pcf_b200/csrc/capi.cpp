@@ -256,6 +256,12 @@ int tpcf_catalog_destroy(tpcf_catalog *cat) {
 
 int64_t tpcf_catalog_n_used(const tpcf_catalog *cat) { return cat ? cat->c.n_kept : -1; }
 
+int tpcf_catalog_release_cache(tpcf_catalog *cat) {
+    if (!cat) return TPCF_E_INVALID_ARG;
+    cat->c.grids.clear();
+    return TPCF_OK;
+}
+
 int tpcf_binning_create(tpcf_ctx *ctx, int mode, const tpcf_axis_spec *ax1, const tpcf_axis_spec *ax2,
                         int32_t n_jk_regions, tpcf_binning **out) {
     if (!out || !ax1) return TPCF_E_INVALID_ARG;
@@ -467,6 +473,19 @@ int tpcf_normalise_cross(const tpcf_catalog *a, const tpcf_catalog *b, int32_t n
 double tpcf_ls_estimator(double dd, double dr, double rr) {
     if (rr == 0) return 0;
     return dd / rr - 2.0 * dr / rr + 1.0;
+}
+
+uint64_t tpcf_kernel_launches(const tpcf_ctx *ctx) { return ctx ? ctx->c.launches : 0; }
+
+int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s) {
+    if (!ctx || !fp32_tflops || !smem_atomics_per_s) return TPCF_E_INVALID_ARG;
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    tpcf::Error err{0, ""};
+    int rc = tpcf::measure_peaks(&ctx->c, fp32_tflops, smem_atomics_per_s, &err);
+    if (rc) return fail(ctx, rc, err.msg);
+    ctx->c.launches += 5;
+    return TPCF_OK;
 }
 
 }  // extern "C"

@@ -61,10 +61,12 @@ struct Grid {
     DevBuf<int> cell_start;  // ncell + 1
     DevBuf<int3> cell_coord; // local coords of each dense cell id (for offsets)
     DevBuf<int> region_start;  // ncell + 1, CSR of distinct jk regions per cell
-    DevBuf<int> regions;
-    std::vector<int> h_cell_start;  // host copy for the work-list build
+    DevBuf<int> regions;       // region of each run
+    DevBuf<int> run_start;     // first point of each run
+    std::vector<int> h_cell_start;  // host copies for the work-list build
     std::vector<int> h_region_start;
     std::vector<int> h_regions;
+    std::vector<int> h_run_start;
     bool has_fp64 = false;
 };
 
@@ -114,8 +116,7 @@ struct Ctx {
     bool own_stream = false;
     std::string last_error;
     int refinement = 0;  // 0 = automatic
-    DevBuf<unsigned long long> counters;
-    DevBuf<int> err_flag;
+    unsigned long long launches = 0;  // kernels launched by this context
 };
 
 // grid.cu
@@ -131,5 +132,8 @@ struct CountRequest {
     int refinement = 0;
 };
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);
+
+// diag.cu
+int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err);
 
 }  // namespace tpcf

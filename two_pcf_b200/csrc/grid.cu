@@ -73,20 +73,23 @@ __global__ void scan_add_kernel(int *__restrict__ out, const int *__restrict__ o
 }
 
 // Exclusive scan of n ints (in may equal out).  Totals must fit in int.
-cudaError_t exclusive_scan(const int *in, int *out, long long n, cudaStream_t st) {
+cudaError_t exclusive_scan(const int *in, int *out, long long n, cudaStream_t st, unsigned long long *launches) {
     if (n <= 0) return cudaSuccess;
     long long tiles = (n + kScanTile - 1) / kScanTile;
     if (tiles == 1) {
         scan_tile_kernel<<<1, kScanThreads, 0, st>>>(in, out, nullptr, n);
+        ++*launches;
         return cudaGetLastError();
     }
     int *sums = nullptr;
     cudaError_t e = cudaMallocAsync((void **)&sums, sizeof(int) * tiles, st);
     if (e != cudaSuccess) return e;
     scan_tile_kernel<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, sums, n);
-    e = exclusive_scan(sums, sums, tiles, st);
+    ++*launches;
+    e = exclusive_scan(sums, sums, tiles, st, launches);
     if (e == cudaSuccess) {
         scan_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, sums, n);
+        ++*launches;
         e = cudaGetLastError();
     }
     cudaFreeAsync(sums, st);
@@ -202,14 +205,20 @@ __global__ void cells_kernel(GeomDev g, int ncell, int npts, const int *__restri
     nreg[c] = k;
 }
 
+// Runs of one region inside one cell, in sorted order: region id and first
+// point of each run (CSR by cell).
 __global__ void regions_kernel(GeomDev g, int ncell, const int *__restrict__ bstart, const int *__restrict__ rstart,
-                               int *__restrict__ regions) {
+                               int *__restrict__ regions, int *__restrict__ run_start) {
     int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c >= ncell) return;
     int k = rstart[c];
     for (int r = 0; r < g.n_jk; ++r) {
         size_t b = (size_t)c * g.n_jk + r;
-        if (bstart[b + 1] > bstart[b]) regions[k++] = r;
+        if (bstart[b + 1] > bstart[b]) {
+            regions[k] = r;
+            run_start[k] = bstart[b];
+            ++k;
+        }
     }
 }
 
@@ -290,10 +299,11 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
     const int *jk = cat->n_jk > 1 ? cat->jk.p : nullptr;
     if (n > 0) {
         assign_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, cat->xyz.p, jk, subset, n, bucket.p, counts.p);
+        ++ctx->launches;
         TPCF_CUDA_TRY(cudaGetLastError());
     }
     // counts -> bucket starts (exclusive); the extra element becomes n.
-    TPCF_CUDA_TRY(exclusive_scan(counts.p, counts.p, nbucket + 1, st));
+    TPCF_CUDA_TRY(exclusive_scan(counts.p, counts.p, nbucket + 1, st, &ctx->launches));
     DevBuf<int> fill;
     TPCF_CUDA_TRY(fill.alloc(nbucket));
     TPCF_CUDA_TRY(cudaMemsetAsync(fill.p, 0, sizeof(int) * nbucket, st));
@@ -302,6 +312,7 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
                                                         jk, subset, n, bucket.p, counts.p, fill.p, g->pos.p,
                                                         g->aux.p, g->idx.p, want_fp64 ? g->xyz_s.p : nullptr,
                                                         want_fp64 ? g->unit_s.p : nullptr);
+        ++ctx->launches;
         TPCF_CUDA_TRY(cudaGetLastError());
     }
     DevBuf<int> nreg;
@@ -309,8 +320,9 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
     TPCF_CUDA_TRY(cudaMemsetAsync(nreg.p, 0, sizeof(int) * (ncell + 1), st));
     cells_kernel<<<(unsigned)((ncell + 1 + 255) / 256), 256, 0, st>>>(gd, (int)ncell, n, counts.p, g->cell_start.p,
                                                                      g->cell_coord.p, nreg.p);
+    ++ctx->launches;
     TPCF_CUDA_TRY(cudaGetLastError());
-    TPCF_CUDA_TRY(exclusive_scan(nreg.p, g->region_start.p, ncell + 1, st));
+    TPCF_CUDA_TRY(exclusive_scan(nreg.p, g->region_start.p, ncell + 1, st, &ctx->launches));
     g->h_region_start.resize(ncell + 1);
     TPCF_CUDA_TRY(cudaMemcpyAsync(g->h_region_start.data(), g->region_start.p, sizeof(int) * (ncell + 1),
                                   cudaMemcpyDeviceToHost, st));
@@ -320,13 +332,19 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
     int nregions = g->h_region_start[ncell];
     TPCF_CUDA_TRY(g->regions.alloc(nregions));
+    TPCF_CUDA_TRY(g->run_start.alloc(nregions));
     regions_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(gd, (int)ncell, counts.p, g->region_start.p,
-                                                                   g->regions.p);
+                                                                   g->regions.p, g->run_start.p);
+    ++ctx->launches;
     TPCF_CUDA_TRY(cudaGetLastError());
     g->h_regions.resize(nregions);
-    if (nregions > 0)
+    g->h_run_start.resize(nregions);
+    if (nregions > 0) {
         TPCF_CUDA_TRY(cudaMemcpyAsync(g->h_regions.data(), g->regions.p, sizeof(int) * nregions,
                                       cudaMemcpyDeviceToHost, st));
+        TPCF_CUDA_TRY(cudaMemcpyAsync(g->h_run_start.data(), g->run_start.p, sizeof(int) * nregions,
+                                      cudaMemcpyDeviceToHost, st));
+    }
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
     *out = g.get();
     cat->grids[key] = std::move(g);

@@ -2,22 +2,30 @@
 // for auto_/cross_pair_count_{monopole,sigma_pi,s_mu}
 // (src/correlators.cpp:11-125, :156-278, :309-430).
 //
-// One persistent CTA per SM pulls work items (a chunk of cell A against all
-// of cell B) from a device queue.  Each thread holds R points of A in
-// registers; B is streamed through shared memory in tiles by one-dimensional
-// bulk copies (cp.async.bulk, completion on an mbarrier, double buffered).
-// Separations are evaluated in FP32 from cell-relative coordinates; a pair
-// whose FP32 value lies within the proven error bound of the range limits or
-// of a bin threshold is re-evaluated with the reference's exact float/double
-// operation sequence (exact_pair below).  Pairs are binned into privatised
-// shared-memory histograms — one slice for the full histogram and a set of
-// slots for jackknife regions, assigned per work item — holding 64-bit fixed
-// point sums, and merged into global 64-bit integers.
+// Persistent CTAs pull work items — a chunk of one (cell, jackknife region)
+// run of catalogue A against one run of catalogue B — from a device queue.
+// Each thread holds R points of A in registers; B streams through shared
+// memory in tiles staged by one-dimensional bulk copies (cp.async.bulk with
+// mbarrier completion, double buffered).
+//
+// Producer/consumer inside every warp: the candidate loop evaluates s^2 in
+// FP32 from cell-relative coordinates and pushes the pairs that pass the
+// (guard-widened) range test into a per-warp queue with a ballot; whenever 32
+// are queued the whole warp bins them together, so the binning path never
+// runs divergent.  Binning uses host-built lookup tables over the float value
+// (s^2, sigma^2) or a linear bucket index (mu, |pi|); buckets within the
+// proven FP32 error bound of a bin edge are marked ambiguous and resolved by
+// threshold search, and a pair that is still within the bound is re-evaluated
+// with the reference's exact float/double sequence (exact_pair).  Counts go to
+// one privatised 64-bit fixed-point histogram per CTA (two 32-bit shared
+// words with carry), added to the global full histogram and to both regions'
+// rows at the end of each item.
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <vector>
 
 #include "engine.h"
@@ -27,11 +35,19 @@ namespace tpcf {
 namespace {
 
 constexpr int NT = 256;        // threads per CTA
+constexpr int NWARP = NT / 32;
 constexpr int R = 4;           // A points per thread
 constexpr int TA = NT * R;     // A chunk
 constexpr int TB = 256;        // B points per staged tile
-constexpr int kMaxSlots = 32;  // jackknife slots per CTA
+constexpr int QCAP = 32 + 32 * R;  // queue entries per warp: a partial round plus one step's pushes
+constexpr int LUT1_BITS = 8;   // buckets per octave of the float-indexed table
+constexpr int LUT1_OCTAVES = 24;
+constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
+constexpr int LUT2_N = 4096;
+constexpr unsigned char LUT_INV = 254;  // every value of the bucket is dropped
+constexpr unsigned char LUT_AMB = 255;  // bucket within the guard of an edge
 constexpr uint32_t kWaitLimit = 1u << 22;
+constexpr long long kItemMaxB = 16384;  // B points per work item (load balance)
 
 struct GridK {
     const float4 *pos;
@@ -40,8 +56,6 @@ struct GridK {
     const double4 *xyz_s;
     const double4 *unit_s;
     const int3 *coord;
-    const int *rstart;
-    const int *regions;
     int kmin0, kmin1, kmin2;
     const double *xyz;   // original catalogue arrays (exact path)
     const double *unit;
@@ -50,64 +64,63 @@ struct GridK {
 struct KParams {
     GridK a, b;
     const WorkItem *items;
+    const Segment *segs;
     int n_items;
     int *head;
     double side;
     int n1, n2, nb;
     float min_r_sq, max_r_sq, lo_cut, hi_cut;
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
+    float s2_lut_min;   // below this s^2 the mu table's guard does not hold
     const float *t1g, *t2g;
-    int ax1_log, ax2_log;
-    float ax1_min, ax1_inv_step, ax1_ilb, ax1_ils;
-    float ax2_min, ax2_inv_step, ax2_ilb, ax2_ils;
+    const unsigned char *lut1g, *lut2g;
+    unsigned lut1_base;  // (bits of the lowest bucket) >> (23 - LUT1_BITS)
+    float lut2_scale;    // bucket = (int)(value * lut2_scale)
     unsigned long long *g_full, *g_sub;
-    int n_jk, ns;
+    int n_jk;
     float wscale;
-    unsigned long long *counters;  // candidates, in_range, guard, overflow
+    unsigned long long *counters;  // candidates, in_range, guard, flushes
     int *err;
 };
 
-struct Misc {
-    int item;
-    int stop;
-    int n_evict;
-    int slot_region[kMaxSlots];
-    int slot_stamp[kMaxSlots];
-    int evict_slot[kMaxSlots];
-    int evict_region[kMaxSlots];
-};
-
 struct SmemLayout {
-    size_t lo, hi, t1, t2, slotmap, misc, tile0, tile1, bar, total;
+    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, tile0, tile1, misc, total;
 };
 
 __host__ __device__ inline size_t tile_bytes(bool exact) { return (size_t)TB * (exact ? 64 : 32); }
 
-__host__ __device__ inline SmemLayout smem_layout(int nb, int ns, int n1, int n2, int n_jk_map, bool exact) {
+// lo/hi: the histogram pairs are added to (per segment region when there
+// are jackknife regions); alo/ahi: the item's A-side total (jackknife only).
+__host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk) {
     SmemLayout L;
     size_t o = 0;
     L.lo = o;
-    o += 4 * (size_t)(ns + 1) * nb;
+    o += 4 * (size_t)nb;
     L.hi = o;
-    o += 4 * (size_t)(ns + 1) * nb;
+    o += 4 * (size_t)nb;
+    L.alo = o;
+    if (jk) o += 4 * (size_t)nb;
+    L.ahi = o;
+    if (jk) o += 4 * (size_t)nb;
     L.t1 = o;
     o += 4 * (size_t)(n1 + 1);
     L.t2 = o;
     o += 4 * (size_t)(n2 + 1);
-    o = (o + 3) / 4 * 4;
-    L.slotmap = o;
-    o += 2 * (size_t)n_jk_map;
+    L.lut1 = o;
+    o += LUT1_N;
+    L.lut2 = o;
+    o += LUT2_N;
     o = (o + 15) / 16 * 16;
-    L.misc = o;
-    o += sizeof(Misc);
+    L.queue = o;
+    o += (size_t)NWARP * QCAP * 16;
     o = (o + 127) / 128 * 128;
     L.tile0 = o;
     o += tile_bytes(exact);
     L.tile1 = o;
     o += tile_bytes(exact);
-    o = (o + 7) / 8 * 8;
-    L.bar = o;
-    o += 16;
+    o = (o + 15) / 16 * 16;
+    L.misc = o;
+    o += 64;
     L.total = o;
     return L;
 }
@@ -117,8 +130,6 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int ns, int n1, int n2
 // _ANGULAR_PI_DEFN; :185 sigma; :338-340 s and mu; src/hist.cpp:484-502
 // binning), bins looked up in the threshold tables.  Returns the flat bin or
 // -1; *in_range receives the range-test result.
-// Parameters of the exact evaluation, passed by value so that the
-// non-inlined guard path needs no copy of the kernel parameter block.
 struct ExactArgs {
     const double *a_xyz, *a_unit, *b_xyz, *b_unit;
     float min_r_sq, max_r_sq;
@@ -178,37 +189,204 @@ __device__ __noinline__ int exact_pair(const ExactArgs E, const float *t1, const
     return exact_bin<MODE>(E, t1, t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, in_range);
 }
 
+// Parameters of the threshold-search path (passed by value to the
+// non-inlined function).
+struct PreciseArgs {
+    int n1, n2;
+    float min_r_sq, max_r_sq, g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
+};
+
+// Threshold search with the FP32 error bounds; falls back to exact_pair when
+// a value lies within its bound of an edge.  Used for table buckets marked
+// ambiguous.
+template <int MODE>
+__device__ __noinline__ int precise_bin(const PreciseArgs P, const ExactArgs E, const float *t1, const float *t2,
+                                        float s2, float pi, int ia, int jb, bool *in_range, bool *guarded) {
+    *guarded = false;
+    const dev::AxisK ax1{t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
+    const dev::AxisK ax2{t2, P.n2, 0, 0.f, 0.f, 0.f, 0.f};
+    bool ex = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
+    int bin = -1;
+    bool inr = false;
+    if (!ex) {
+        inr = (s2 < P.max_r_sq) && (s2 > P.min_r_sq);
+        if (inr) {
+            if (MODE == MODE_MONOPOLE) {
+                const int b1 = dev::locate_exact(t1, P.n1, s2);
+                ex = dev::near_edge(ax1, s2, b1, P.g_s2);
+                bin = (b1 >= 0 && b1 < P.n1) ? b1 : -1;
+            } else if (MODE == MODE_S_MU) {
+                const float inv_s = rsqrtf(s2);
+                const int b1 = dev::locate_exact(t1, P.n1, s2);
+                const float mu = fabsf(pi) * inv_s;
+                const int b2 = dev::locate_exact(t2, P.n2, mu);
+                const float gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
+                ex = dev::near_edge(ax1, s2, b1, P.g_s2) || dev::near_edge(ax2, mu, b2, gmu);
+                bin = (b1 >= 0 && b1 < P.n1 && b2 >= 0 && b2 < P.n2) ? b1 * P.n2 + b2 : -1;
+            } else {
+                const float a = fmaf(-pi, pi, s2);
+                const float api = fabsf(pi);
+                const int b2 = dev::locate_exact(t2, P.n2, api);
+                ex = dev::near_edge(ax2, api, b2, P.g_pi);
+                int b1 = -1;
+                if (a <= P.g_a) {
+                    ex = ex || (a >= -P.g_a);  // near zero: sqrtf of a value of unknown sign
+                } else {
+                    b1 = dev::locate_exact(t1, P.n1, a);
+                    ex = ex || dev::near_edge(ax1, a, b1, P.g_a);
+                }
+                bin = (b1 >= 0 && b1 < P.n1 && b2 >= 0 && b2 < P.n2) ? b1 * P.n2 + b2 : -1;
+            }
+        }
+    }
+    if (ex) {
+        *guarded = true;
+        bin = exact_pair<MODE>(E, t1, t2, ia, jb, &inr);
+    }
+    *in_range = inr;
+    return bin;
+}
+
+__device__ __forceinline__ int lut1_index(unsigned base, float x) {
+    const int i = (int)((__float_as_uint(x) >> (23 - LUT1_BITS)) - base);
+    return min(max(i, 0), LUT1_N - 1);
+}
+
+__device__ __forceinline__ int lut2_index(float scale, float x) {
+    const int i = (int)(x * scale);
+    return min(max(i, 0), LUT2_N - 1);
+}
+
+struct Counters {
+    unsigned long long in_range = 0, guard = 0;
+};
+
+// Bin one pair that passed the guard-widened range test, from its FP32 s^2,
+// pi and weight.  ia/jb are the pair's positions in the sorted grids (the
+// exact path follows them back to the original arrays).
+template <int MODE, bool UNITW>
+__device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
+                                         const float *s_t1, const float *s_t2, const unsigned char *s_l1,
+                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi, float s2,
+                                         float pi, float w, int ia, int jb, Counters &cnt) {
+    int bin;
+    bool amb;
+    if (MODE == MODE_SIGMA_PI) {
+        if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return;  // certainly out of range
+        amb = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
+        const float a = fmaf(-pi, pi, s2);
+        unsigned c1 = (a <= P.g_a) ? LUT_AMB : s_l1[lut1_index(P.lut1_base, a)];
+        if (a < -P.g_a) c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
+        const unsigned c2 = s_l2[lut2_index(P.lut2_scale, fabsf(pi))];
+        if (!amb && (c1 == LUT_INV || c2 == LUT_INV)) {
+            cnt.in_range += 1;
+            return;
+        }
+        amb = amb || c1 >= LUT_INV || c2 >= LUT_INV;
+        if (!amb) cnt.in_range += 1;
+        bin = (int)(c1 * P.n2 + c2);
+    } else {
+        const unsigned c1 = s_l1[lut1_index(P.lut1_base, s2)];
+        if (c1 == LUT_INV) {
+            // certainly outside the range or the bins; the range status is
+            // the same for every value of the widened bucket
+            cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
+            return;
+        }
+        amb = (c1 == LUT_AMB);
+        unsigned c2 = 0;
+        if (MODE == MODE_S_MU) {
+            const float mu = fabsf(pi) * rsqrtf(s2);
+            c2 = s_l2[lut2_index(P.lut2_scale, mu)];
+            if (c2 == LUT_INV && !amb && s2 >= P.s2_lut_min) {
+                cnt.in_range += 1;
+                return;
+            }
+            amb = amb || c2 >= LUT_INV || s2 < P.s2_lut_min;
+        }
+        if (!amb) cnt.in_range += 1;
+        bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
+    }
+    if (amb) {
+        bool inr, guarded;
+        bin = precise_bin<MODE>(PA, E, s_t1, s_t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
+        cnt.in_range += inr ? 1 : 0;
+        cnt.guard += guarded ? 1 : 0;
+        if (bin < 0) return;
+    }
+    const long long q = UNITW ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
+    dev::acc_add(s_lo, s_hi, bin, q);
+}
+
+// Bin one pair of the plain FP64 path from its exact separation (d0, d1,
+// d2); ia/jb are its positions in the sorted grids.
+template <int MODE, bool UNITW>
+__device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, const float *s_t1, const float *s_t2,
+                                          uint32_t *s_lo, uint32_t *s_hi, float d0, float d1, float d2, int ia,
+                                          int jb, Counters &cnt) {
+    double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
+    if (MODE != MODE_MONOPOLE) {
+        const double4 u1 = P.a.unit_s[ia];
+        const double4 u2 = P.b.unit_s[jb];
+        n1x = u1.x;
+        n1y = u1.y;
+        n1z = u1.z;
+        n2x = u2.x;
+        n2y = u2.y;
+        n2z = u2.z;
+    }
+    bool inr;
+    const int bin = exact_bin<MODE>(E, s_t1, s_t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
+    cnt.in_range += inr ? 1 : 0;
+    if (bin < 0) return;
+    const long long q =
+        UNITW ? 1LL
+              : __float2ll_rn(__fmul_rn(__fmul_rn((float)P.a.xyz_s[ia].w, (float)P.b.xyz_s[jb].w), P.wscale));
+    dev::acc_add(s_lo, s_hi, bin, q);
+}
+
+// Add a 64-bit value held as two 32-bit words into another such pair (the
+// caller owns the bin: no atomics).
+__device__ __forceinline__ void add64_owned(uint32_t *lo, uint32_t *hi, int i, unsigned long long v) {
+    const uint32_t vl = (uint32_t)v, vh = (uint32_t)(v >> 32);
+    const uint32_t old = lo[i];
+    lo[i] = old + vl;
+    hi[i] = hi[i] + vh + ((old + vl) < old ? 1u : 0u);
+}
+
 template <int MODE, bool UNITW, bool JK, bool EXACT>
-__global__ void __launch_bounds__(NT, 1) pair_count_kernel(const KParams P) {
+__global__ void __launch_bounds__(NT, 2) pair_count_kernel(const KParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr bool kNeedAux = (MODE != MODE_MONOPOLE) || JK;
-    const SmemLayout L = smem_layout(P.nb, P.ns, P.n1, P.n2, JK ? P.n_jk : 0, EXACT);
+    constexpr bool kNeedAux = (MODE != MODE_MONOPOLE);
+    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
+    uint32_t *s_alo = (uint32_t *)(smem + L.alo);
+    uint32_t *s_ahi = (uint32_t *)(smem + L.ahi);
     float *s_t1 = (float *)(smem + L.t1);
     float *s_t2 = (float *)(smem + L.t2);
-    short *s_slot = (short *)(smem + L.slotmap);
-    Misc *s_misc = (Misc *)(smem + L.misc);
+    unsigned char *s_l1 = smem + L.lut1;
+    unsigned char *s_l2 = smem + L.lut2;
     unsigned char *tiles[2] = {smem + L.tile0, smem + L.tile1};
-    uint64_t *bar = (uint64_t *)(smem + L.bar);
-    const int tid = threadIdx.x;
-    const int nslices = P.ns + 1;  // slice P.ns is the full histogram
-    const int full_base = P.ns * P.nb;
+    int *s_item = (int *)(smem + L.misc);
+    uint64_t *bar = (uint64_t *)(smem + L.misc + 16);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    float4 *s_q = (float4 *)(smem + L.queue) + warp * QCAP;
+    const unsigned lt_mask = (1u << lane) - 1u;
 
-    for (int i = tid; i < nslices * P.nb; i += NT) {
+    for (int i = tid; i < P.nb; i += NT) {
         s_lo[i] = 0;
         s_hi[i] = 0;
+        if (JK) {
+            s_alo[i] = 0;
+            s_ahi[i] = 0;
+        }
     }
     for (int i = tid; i <= P.n1; i += NT) s_t1[i] = P.t1g[i];
     for (int i = tid; i <= P.n2; i += NT) s_t2[i] = P.t2g[i];
-    if (JK)
-        for (int i = tid; i < P.n_jk; i += NT) s_slot[i] = -1;
+    for (int i = tid; i < LUT1_N; i += NT) s_l1[i] = P.lut1g[i];
+    for (int i = tid; i < LUT2_N; i += NT) s_l2[i] = P.lut2g[i];
     if (tid == 0) {
-        for (int s = 0; s < kMaxSlots; ++s) {
-            s_misc->slot_region[s] = -1;
-            s_misc->slot_stamp[s] = -1;
-        }
-        s_misc->stop = 0;
         dev::mbar_init(&bar[0], 1);
         dev::mbar_init(&bar[1], 1);
         dev::mbar_init_fence();
@@ -216,331 +394,287 @@ __global__ void __launch_bounds__(NT, 1) pair_count_kernel(const KParams P) {
     __syncthreads();
 
     const ExactArgs EA{P.a.xyz, P.a.unit, P.b.xyz, P.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2};
-    const dev::AxisK ax1{s_t1, P.n1, P.ax1_log, P.ax1_min, P.ax1_inv_step, P.ax1_ilb, P.ax1_ils};
-    const dev::AxisK ax2{s_t2, P.n2, P.ax2_log, P.ax2_min, P.ax2_inv_step, P.ax2_ilb, P.ax2_ils};
-
-    unsigned long long n_in = 0, n_guard = 0, n_over = 0, n_cand = 0;
+    const PreciseArgs PA{P.n1, P.n2, P.min_r_sq, P.max_r_sq, P.g_s2, P.g_pi, P.g_a, P.c1_mu, P.c2_mu, P.g_mu0};
+    Counters cnt;
+    unsigned long long n_cand = 0, n_flush = 0;
     unsigned tcount = 0;  // tiles staged so far by this CTA (selects buffer and phase)
-    int stamp = 0;
+
+    auto issue = [&](unsigned tc, int start, int len) {
+        unsigned char *dst = tiles[tc & 1];
+        dev::fence_proxy_async();
+        if (EXACT) {
+            const uint32_t by = (uint32_t)len * 32u;
+            dev::mbar_expect_tx(&bar[tc & 1], by);
+            dev::bulk_g2s(dst, P.b.xyz_s + start, by, &bar[tc & 1]);
+        } else {
+            const uint32_t by = (uint32_t)len * 16u;
+            dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
+            dev::bulk_g2s(dst, P.b.pos + start, by, &bar[tc & 1]);
+            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TB * 16, P.b.aux + start, by, &bar[tc & 1]);
+        }
+    };
 
     for (;;) {
         if (tid == 0) {
             int item = atomicAdd(P.head, 1);
             if (*(volatile int *)P.err != 0) item = P.n_items;
-            s_misc->item = item;
+            s_item[0] = item;
         }
         __syncthreads();
-        const int item = s_misc->item;
+        const int item = s_item[0];
         if (item >= P.n_items) break;
         const WorkItem it = P.items[item];
-        ++stamp;
-        if (tid == 0) {
-            long long al = it.a_len, bl = it.b_len;
-            n_cand += it.self ? (unsigned long long)(al * bl - al * (al + 1) / 2) : (unsigned long long)(al * bl);
-        }
 
-        // ---- jackknife slot assignment for the regions of cells A and B
-        if (JK) {
-            if (tid == 0) {
-                s_misc->n_evict = 0;
-                const int *la = P.a.regions + P.a.rstart[it.a_cell];
-                const int na = P.a.rstart[it.a_cell + 1] - P.a.rstart[it.a_cell];
-                const int *lb = P.b.regions + P.b.rstart[it.b_cell];
-                const int nbr = P.b.rstart[it.b_cell + 1] - P.b.rstart[it.b_cell];
-                // pass 1: regions that already hold a slot keep it
-                for (int pass = 0; pass < 2; ++pass) {
-                    for (int k = 0; k < na + nbr; ++k) {
-                        const int r = k < na ? la[k] : lb[k - na];
-                        const int s = s_slot[r];
-                        if (pass == 0) {
-                            if (s >= 0) s_misc->slot_stamp[s] = stamp;
-                            continue;
-                        }
-                        if (s >= 0) continue;
-                        int pick = -1;
-                        for (int q = 0; q < P.ns; ++q)
-                            if (s_misc->slot_region[q] < 0) {
-                                pick = q;
-                                break;
-                            }
-                        if (pick < 0)
-                            for (int q = 0; q < P.ns; ++q)
-                                if (s_misc->slot_stamp[q] != stamp) {
-                                    pick = q;
-                                    break;
-                                }
-                        if (pick < 0) continue;  // no slot left: this region goes to global memory
-                        const int old = s_misc->slot_region[pick];
-                        if (old >= 0) {
-                            const int e = s_misc->n_evict++;
-                            s_misc->evict_slot[e] = pick;
-                            s_misc->evict_region[e] = old;
-                            s_slot[old] = -1;
-                        }
-                        s_misc->slot_region[pick] = r;
-                        s_misc->slot_stamp[pick] = stamp;
-                        s_slot[r] = (short)pick;
-                    }
-                }
-            }
-            __syncthreads();
-            const int ne = s_misc->n_evict;
-            for (int e = 0; e < ne; ++e) {
-                const int s = s_misc->evict_slot[e], r = s_misc->evict_region[e];
-                for (int b = tid; b < P.nb; b += NT) {
-                    const int i = s * P.nb + b;
-                    const unsigned long long v = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
-                    if (v) {
-                        atomicAdd(&P.g_sub[(size_t)r * P.nb + b], v);
-                        s_lo[i] = 0;
-                        s_hi[i] = 0;
-                    }
-                }
-            }
-            if (ne) __syncthreads();
-        }
+        // ---- phase mapping: Pn groups of G threads; each group holds the
+        // whole A chunk (G * R slots) and takes every Pn-th B point, so short
+        // runs still occupy every thread
+        int Pn = min(32, max(1, TA / max(it.a_len, 1)));
+        while (Pn > 1 && (NT / Pn) * R < it.a_len) --Pn;
+        const int G = NT / Pn;
+        const int grp = tid / G, loc = tid - grp * G;
+        const bool thr_on = grp < Pn;
 
-        // ---- A points into registers, shifted into B's cell frame
-        const int3 ca = P.a.coord[it.a_cell], cb = P.b.coord[it.b_cell];
-        const double offx = (double)((P.a.kmin0 + ca.x) - (P.b.kmin0 + cb.x)) * P.side;
-        const double offy = (double)((P.a.kmin1 + ca.y) - (P.b.kmin1 + cb.y)) * P.side;
-        const double offz = (double)((P.a.kmin2 + ca.z) - (P.b.kmin2 + cb.z)) * P.side;
-        float ax[R], ay[R], az[R], aw[R], anx[R], any_[R], anz[R];
-        int ai[R], ajk[R], aslot[R];
+        // ---- A points: validity and indices; FP32 coordinates are
+        // (re)loaded per segment in that segment's cell frame
+        const int3 ca = P.a.coord[it.a_cell];
         double dax[R], day[R], daz[R];
-        (void)dax; (void)day; (void)daz;
+        int ai[R], apack[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int k = tid + r * NT;
-            const bool valid = k < it.a_len;
+            const int k = loc + r * G;
+            const bool valid = thr_on && k < it.a_len;
             const int gi = it.a_start + k;
+            apack[r] = k << 8;  // queue entry: A chunk index << 8 | tile index
             ai[r] = valid ? gi : 0x7fffffff;
-            ax[r] = ay[r] = az[r] = 1e30f;
-            aw[r] = 0.0f;
-            anx[r] = any_[r] = anz[r] = 0.0f;
-            ajk[r] = 0;
-            aslot[r] = -1;
-            if (EXACT) {
-                dax[r] = day[r] = daz[r] = 1e300;
-                if (valid) {
-                    const double4 p = P.a.xyz_s[gi];
-                    dax[r] = p.x;
-                    day[r] = p.y;
-                    daz[r] = p.z;
-                    aw[r] = (float)p.w;
-                    if (JK) ajk[r] = (int)P.a.unit_s[gi].w;
-                }
-            } else if (valid) {
-                const float4 p = P.a.pos[gi];
-                ax[r] = p.x + (float)offx;
-                ay[r] = p.y + (float)offy;
-                az[r] = p.z + (float)offz;
-                aw[r] = p.w;
-                if (kNeedAux) {
-                    const float4 q = P.a.aux[gi];
-                    anx[r] = q.x;
-                    any_[r] = q.y;
-                    anz[r] = q.z;
-                    ajk[r] = __float_as_int(q.w);
-                }
+            dax[r] = day[r] = daz[r] = 1e300;
+            if (EXACT && valid) {
+                const double4 p = P.a.xyz_s[gi];
+                dax[r] = p.x;
+                day[r] = p.y;
+                daz[r] = p.z;
             }
-            if (JK && valid) aslot[r] = s_slot[ajk[r]];
         }
 
-        // ---- stream B through shared memory
-        const int ntiles = (it.b_len + TB - 1) / TB;
-        auto issue = [&](unsigned tc, int start, int len) {
-            unsigned char *dst = tiles[tc & 1];
-            dev::fence_proxy_async();
-            if (EXACT) {
-                const uint32_t by = (uint32_t)len * 32u;
-                dev::mbar_expect_tx(&bar[tc & 1], (MODE != MODE_MONOPOLE || JK) ? 2 * by : by);
-                dev::bulk_g2s(dst, P.b.xyz_s + start, by, &bar[tc & 1]);
-                if (MODE != MODE_MONOPOLE || JK) dev::bulk_g2s(dst + (size_t)TB * 32, P.b.unit_s + start, by, &bar[tc & 1]);
-            } else {
-                const uint32_t by = (uint32_t)len * 16u;
-                dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
-                dev::bulk_g2s(dst, P.b.pos + start, by, &bar[tc & 1]);
-                if (kNeedAux) dev::bulk_g2s(dst + (size_t)TB * 16, P.b.aux + start, by, &bar[tc & 1]);
+        if (tid == 0) {
+            const Segment s0 = P.segs[it.seg_begin];
+            issue(tcount, s0.b_start, min(TB, s0.b_len));
+        }
+        for (int si = it.seg_begin; si < it.seg_end; ++si) {
+            const Segment sg = P.segs[si];
+            const int rb = sg.meta & 0xffff;
+            const bool self = (sg.meta >> 16) != 0;
+            if (tid == 0) {
+                const long long al = it.a_len, bl = sg.b_len;
+                n_cand += self ? (unsigned long long)(al * bl - al * (al + 1) / 2) : (unsigned long long)(al * bl);
             }
-        };
-        if (tid == 0 && ntiles > 0) issue(tcount, it.b_start, min(TB, it.b_len));
-
-        for (int t = 0; t < ntiles; ++t) {
-            const int tstart = t * TB;
-            const int tlen = min(TB, it.b_len - tstart);
-            if (tid == 0 && t + 1 < ntiles)
-                issue(tcount + 1, it.b_start + tstart + TB, min(TB, it.b_len - tstart - TB));
-            if (!dev::mbar_wait_bounded(&bar[tcount & 1], (tcount >> 1) & 1u, kWaitLimit)) {
-                atomicExch(P.err, 4);  // device timeout: results are discarded by the host
-            }
-            const int jbase = it.b_start + tstart;
-            if (EXACT) {
-                const double4 *s_xyz = (const double4 *)tiles[tcount & 1];
-                const double4 *s_unit = (const double4 *)(tiles[tcount & 1] + (size_t)TB * 32);
-                for (int jj = 0; jj < tlen; ++jj) {
-                    const double4 pb = s_xyz[jj];
-                    const int jg = jbase + jj;
+            // A coordinates in the frame of this segment's cell
+            const int3 cb = P.b.coord[sg.b_cell];
+            const float offx = (float)((double)((P.a.kmin0 + ca.x) - (P.b.kmin0 + cb.x)) * P.side);
+            const float offy = (float)((double)((P.a.kmin1 + ca.y) - (P.b.kmin1 + cb.y)) * P.side);
+            const float offz = (float)((double)((P.a.kmin2 + ca.z) - (P.b.kmin2 + cb.z)) * P.side);
+            float ax[R], ay[R], az[R], aw[R], anx[R], any_[R], anz[R];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float d0 = __double2float_rn(__dsub_rn(dax[r], pb.x));
-                        const float d1 = __double2float_rn(__dsub_rn(day[r], pb.y));
-                        const float d2 = __double2float_rn(__dsub_rn(daz[r], pb.z));
-                        const float s2 = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
-                        bool hit = (s2 < P.max_r_sq) && (s2 > P.min_r_sq);
-                        if (it.self) hit = hit && (jg > ai[r]);
-                        if (hit) {
-                            ++n_in;
-                            int bin;
-                            double4 ub = make_double4(0, 0, 0, 0);
-                            if (MODE != MODE_MONOPOLE || JK) ub = s_unit[jj];
-                            if (MODE == MODE_MONOPOLE) {
-                                bin = dev::locate_exact(s_t1, P.n1, s2);
-                                if (bin >= P.n1) bin = -1;
-                            } else {
-                                const double4 ua = P.a.unit_s[ai[r]];
-                                bool inr;
-                                bin = exact_bin<MODE>(EA, s_t1, s_t2, d0, d1, d2, ua.x, ua.y, ua.z, ub.x, ub.y, ub.z,
-                                                      &inr);
-                            }
-                            if (bin >= 0) {
-                                const float w = UNITW ? 1.0f : __fmul_rn(aw[r], (float)pb.w);
-                                const long long q = UNITW ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
-                                dev::acc_add(s_lo, s_hi, full_base + bin, q);
-                                if (JK) {
-                                    const int ja = ajk[r], jb = (int)ub.w;
-                                    const int sa = aslot[r];
-                                    if (sa >= 0) dev::acc_add(s_lo, s_hi, sa * P.nb + bin, q);
-                                    else { dev::acc_add_global(P.g_sub, (size_t)ja * P.nb + bin, q); ++n_over; }
-                                    if (jb != ja) {
-                                        const int sb = s_slot[jb];
-                                        if (sb >= 0) dev::acc_add(s_lo, s_hi, sb * P.nb + bin, q);
-                                        else { dev::acc_add_global(P.g_sub, (size_t)jb * P.nb + bin, q); ++n_over; }
-                                    }
-                                }
-                            }
-                        }
+            for (int r = 0; r < R; ++r) {
+                ax[r] = ay[r] = az[r] = 1e30f;
+                aw[r] = 0.0f;
+                anx[r] = any_[r] = anz[r] = 0.0f;
+                if (!EXACT && ai[r] != 0x7fffffff) {
+                    const float4 p = P.a.pos[ai[r]];
+                    ax[r] = p.x + offx;
+                    ay[r] = p.y + offy;
+                    az[r] = p.z + offz;
+                    aw[r] = p.w;
+                    if (kNeedAux) {
+                        const float4 q = P.a.aux[ai[r]];
+                        anx[r] = q.x;
+                        any_[r] = q.y;
+                        anz[r] = q.z;
                     }
                 }
-            } else {
-                const float4 *s_pos = (const float4 *)tiles[tcount & 1];
-                const float4 *s_aux = (const float4 *)(tiles[tcount & 1] + (size_t)TB * 16);
-                for (int jj = 0; jj < tlen; ++jj) {
-                    const float4 pb = s_pos[jj];
-                    const int jg = jbase + jj;
+            }
+            const int ntiles = (sg.b_len + TB - 1) / TB;
+            for (int t = 0; t < ntiles; ++t) {
+                const int tstart = t * TB;
+                const int tlen = min(TB, sg.b_len - tstart);
+                if (tid == 0) {
+                    if (t + 1 < ntiles) {
+                        issue(tcount + 1, sg.b_start + tstart + TB, min(TB, sg.b_len - tstart - TB));
+                    } else if (si + 1 < it.seg_end) {
+                        const Segment nx = P.segs[si + 1];
+                        issue(tcount + 1, nx.b_start, min(TB, nx.b_len));
+                    }
+                }
+                if (!dev::mbar_wait_bounded(&bar[tcount & 1], (tcount >> 1) & 1u, kWaitLimit)) {
+                    atomicExch(P.err, 4);  // device timeout: results are discarded by the host
+                }
+                const int jbase = sg.b_start + tstart;
+                const int nsteps = (tlen + Pn - 1) / Pn;
+                // Candidates that pass the (guard-widened) range test are
+                // pushed into the warp's queue with a ballot; each time 32 are
+                // queued the whole warp bins them (no divergent binning).
+                int qn = 0;  // queued entries of this warp (warp-uniform)
+                if (EXACT) {
+                    const double4 *s_xyz = (const double4 *)tiles[tcount & 1];
+                    for (int m = 0; m < nsteps; ++m) {
+                        const int jj = grp + m * Pn;
+                        const bool jv = thr_on && jj < tlen;
+                        const double4 pb = s_xyz[min(jj, tlen - 1)];
+                        const int jg = jbase + jj;
+                        float d0[R], d1[R], d2[R];
+                        bool hit[R];
 #pragma unroll
-                    for (int r = 0; r < R; ++r) {
-                        const float dx = ax[r] - pb.x, dy = ay[r] - pb.y, dz = az[r] - pb.z;
-                        const float s2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));
-                        bool hit = (s2 < P.hi_cut) && (s2 > P.lo_cut);
-                        if (it.self) hit = hit && (jg > ai[r]);
-                        if (!hit) continue;
+                        for (int r = 0; r < R; ++r) {
+                            d0[r] = __double2float_rn(__dsub_rn(dax[r], pb.x));
+                            d1[r] = __double2float_rn(__dsub_rn(day[r], pb.y));
+                            d2[r] = __double2float_rn(__dsub_rn(daz[r], pb.z));
+                            const float s2 = __fadd_rn(__fadd_rn(__fmul_rn(d0[r], d0[r]), __fmul_rn(d1[r], d1[r])),
+                                                       __fmul_rn(d2[r], d2[r]));
+                            hit[r] = jv && (s2 < P.max_r_sq) && (s2 > P.min_r_sq) && (!self || jg > ai[r]);
+                        }
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+                            if (hit[r])
+                                s_q[qn + __popc(bal & lt_mask)] =
+                                    make_float4(d0[r], d1[r], d2[r], __int_as_float(apack[r] | jj));
+                            qn += __popc(bal);
+                        }
+                        while (qn >= 32) {
+                            __syncwarp();
+                            const float4 e = s_q[qn - 32 + lane];
+                            const int pk = __float_as_int(e.w);
+                            bin_exact<MODE, UNITW>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
+                                                   it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            __syncwarp();
+                            qn -= 32;
+                        }
+                    }
+                    if (qn > 0) {
+                        __syncwarp();
+                        if (lane < qn) {
+                            const float4 e = s_q[lane];
+                            const int pk = __float_as_int(e.w);
+                            bin_exact<MODE, UNITW>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
+                                                   it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                        }
+                        __syncwarp();
+                    }
+                } else {
+                    const float4 *s_pos = (const float4 *)tiles[tcount & 1];
+                    const float4 *s_aux = (const float4 *)(tiles[tcount & 1] + (size_t)TB * 16);
+                    for (int m = 0; m < nsteps; ++m) {
+                        const int jj = grp + m * Pn;
+                        const int jc = min(jj, tlen - 1);
+                        const bool jv = thr_on && jj < tlen;
+                        const float4 pb = s_pos[jc];
+                        const int jg = jbase + jj;
+                        float s2[R], dx[R], dy[R], dz[R];
+                        bool hit[R];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            dx[r] = ax[r] - pb.x;
+                            dy[r] = ay[r] - pb.y;
+                            dz[r] = az[r] - pb.z;
+                            s2[r] = fmaf(dz[r], dz[r], fmaf(dy[r], dy[r], dx[r] * dx[r]));
+                            hit[r] = jv && (s2[r] < P.hi_cut) && (s2[r] > P.lo_cut) && (!self || jg > ai[r]);
+                        }
                         float4 ab = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (kNeedAux) ab = s_aux[jj];
-                        bool ex = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
-                        bool inr = false;
-                        int bin = -1;
-                        if (!ex) {
-                            inr = (s2 < P.max_r_sq) && (s2 > P.min_r_sq);
-                            if (inr) {
-                                const float inv_s = rsqrtf(s2);
-                                if (MODE == MODE_MONOPOLE) {
-                                    const int b1 = dev::locate(ax1, s2, dev::approx_bin(ax1, s2 * inv_s));
-                                    ex = dev::near_edge(ax1, s2, b1, P.g_s2);
-                                    bin = (b1 >= 0 && b1 < P.n1) ? b1 : -1;
-                                } else {
-                                    const float pi = 0.5f * fmaf(dz, anz[r] + ab.z,
-                                                                 fmaf(dy, any_[r] + ab.y, dx * (anx[r] + ab.x)));
-                                    if (MODE == MODE_S_MU) {
-                                        const int b1 = dev::locate(ax1, s2, dev::approx_bin(ax1, s2 * inv_s));
-                                        const float mu = fabsf(pi) * inv_s;
-                                        const int b2 = dev::locate(ax2, mu, dev::approx_bin(ax2, mu));
-                                        const float gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
-                                        ex = dev::near_edge(ax1, s2, b1, P.g_s2) || dev::near_edge(ax2, mu, b2, gmu);
-                                        bin = (b1 >= 0 && b1 < P.n1 && b2 >= 0 && b2 < P.n2) ? b1 * P.n2 + b2 : -1;
-                                    } else {
-                                        const float a = fmaf(-pi, pi, s2);
-                                        const float api = fabsf(pi);
-                                        const int b2 = dev::locate(ax2, api, dev::approx_bin(ax2, api));
-                                        ex = dev::near_edge(ax2, api, b2, P.g_pi);
-                                        int b1 = -1;
-                                        if (a <= P.g_a) {
-                                            ex = ex || (a >= -P.g_a);  // near zero: sqrt of a value of unknown sign
-                                        } else {
-                                            b1 = dev::locate(ax1, a, dev::approx_bin(ax1, a * rsqrtf(a)));
-                                            ex = ex || dev::near_edge(ax1, a, b1, P.g_a);
-                                        }
-                                        bin = (b1 >= 0 && b1 < P.n1 && b2 >= 0 && b2 < P.n2) ? b1 * P.n2 + b2 : -1;
-                                    }
-                                }
+                        if (kNeedAux) ab = s_aux[jc];
+#pragma unroll
+                        for (int r = 0; r < R; ++r) {
+                            const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+                            if (hit[r]) {
+                                float pi = 0.f;
+                                if (kNeedAux)
+                                    pi = 0.5f * fmaf(dz[r], anz[r] + ab.z,
+                                                     fmaf(dy[r], any_[r] + ab.y, dx[r] * (anx[r] + ab.x)));
+                                const float w = UNITW ? 1.0f : __fmul_rn(aw[r], pb.w);
+                                s_q[qn + __popc(bal & lt_mask)] =
+                                    make_float4(s2[r], pi, w, __int_as_float(apack[r] | jj));
                             }
+                            qn += __popc(bal);
                         }
-                        if (ex) {
-                            ++n_guard;
-                            bin = exact_pair<MODE>(EA, s_t1, s_t2, P.a.idx[ai[r]], P.b.idx[jg], &inr);
-                        }
-                        if (inr) ++n_in;
-                        if (bin < 0) continue;
-                        const float w = UNITW ? 1.0f : __fmul_rn(aw[r], pb.w);
-                        const long long q = UNITW ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
-                        dev::acc_add(s_lo, s_hi, full_base + bin, q);
-                        if (JK) {
-                            const int ja = ajk[r], jb = __float_as_int(ab.w);
-                            const int sa = aslot[r];
-                            if (sa >= 0) dev::acc_add(s_lo, s_hi, sa * P.nb + bin, q);
-                            else { dev::acc_add_global(P.g_sub, (size_t)ja * P.nb + bin, q); ++n_over; }
-                            if (jb != ja) {
-                                const int sb = s_slot[jb];
-                                if (sb >= 0) dev::acc_add(s_lo, s_hi, sb * P.nb + bin, q);
-                                else { dev::acc_add_global(P.g_sub, (size_t)jb * P.nb + bin, q); ++n_over; }
-                            }
+                        while (qn >= 32) {
+                            __syncwarp();
+                            const float4 e = s_q[qn - 32 + lane];
+                            const int pk = __float_as_int(e.w);
+                            bin_fast<MODE, UNITW>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y, e.z,
+                                                  it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            __syncwarp();
+                            qn -= 32;
                         }
                     }
+                    // drain: the queued entries refer to this tile's positions
+                    if (qn > 0) {
+                        __syncwarp();
+                        if (lane < qn) {
+                            const float4 e = s_q[lane];
+                            const int pk = __float_as_int(e.w);
+                            bin_fast<MODE, UNITW>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y, e.z,
+                                                  it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                        }
+                        __syncwarp();
+                    }
+                }
+                __syncthreads();  // everyone is done with this buffer before it is refilled
+                ++tcount;
+            }
+            // ---- jackknife: a region's pairs (JKHists::add_pair,
+            // src/hist.cpp:246-260) go to its row once per run of equal
+            // regions, and into the item's A-side total
+            if (JK) {
+                const bool last = (si + 1 == it.seg_end) || ((P.segs[si + 1].meta & 0xffff) != rb);
+                if (last) {
+                    for (int b = tid; b < P.nb; b += NT) {
+                        const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
+                        if (!v) continue;
+                        add64_owned(s_alo, s_ahi, b, v);
+                        if (rb != it.a_region) atomicAdd(&P.g_sub[(size_t)rb * P.nb + b], v);
+                        s_lo[b] = 0;
+                        s_hi[b] = 0;
+                    }
+                    ++n_flush;
+                    __syncthreads();
                 }
             }
-            __syncthreads();  // everyone is done with this buffer before it is refilled
-            ++tcount;
+        }
+        // ---- jackknife: the item's total goes to the full histogram and to
+        // the A region's row
+        if (JK) {
+            for (int b = tid; b < P.nb; b += NT) {
+                const unsigned long long v = ((unsigned long long)s_ahi[b] << 32) | s_alo[b];
+                if (!v) continue;
+                atomicAdd(&P.g_full[b], v);
+                atomicAdd(&P.g_sub[(size_t)it.a_region * P.nb + b], v);
+                s_alo[b] = 0;
+                s_ahi[b] = 0;
+            }
+            __syncthreads();
         }
     }
 
-    // ---- merge the privatised histograms
+    // ---- merge the privatised histogram
     __syncthreads();
-    for (int i = tid; i < nslices * P.nb; i += NT) {
-        const unsigned long long v = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
-        if (!v) continue;
-        const int slice = i / P.nb, b = i - slice * P.nb;
-        if (slice == P.ns) atomicAdd(&P.g_full[b], v);
-        else {
-            const int r = s_misc->slot_region[slice];
-            if (r >= 0) atomicAdd(&P.g_sub[(size_t)r * P.nb + b], v);
+    if (!JK) {
+        for (int b = tid; b < P.nb; b += NT) {
+            const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
+            if (v) atomicAdd(&P.g_full[b], v);
         }
     }
     // ---- counters
-    __shared__ unsigned long long red[3][NT / 32];
-    unsigned long long v0 = n_in, v1 = n_guard, v2 = n_over;
+    unsigned long long v0 = cnt.in_range, v1 = cnt.guard;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         v0 += __shfl_down_sync(0xffffffffu, v0, o);
         v1 += __shfl_down_sync(0xffffffffu, v1, o);
-        v2 += __shfl_down_sync(0xffffffffu, v2, o);
     }
     if ((tid & 31) == 0) {
-        red[0][tid >> 5] = v0;
-        red[1][tid >> 5] = v1;
-        red[2][tid >> 5] = v2;
+        atomicAdd(&P.counters[1], v0);
+        atomicAdd(&P.counters[2], v1);
     }
-    __syncthreads();
     if (tid == 0) {
-        unsigned long long s0 = 0, s1 = 0, s2 = 0;
-        for (int w = 0; w < NT / 32; ++w) {
-            s0 += red[0][w];
-            s1 += red[1][w];
-            s2 += red[2][w];
-        }
         atomicAdd(&P.counters[0], n_cand);
-        atomicAdd(&P.counters[1], s0);
-        atomicAdd(&P.counters[2], s1);
-        atomicAdd(&P.counters[3], s2);
+        atomicAdd(&P.counters[3], n_flush);
     }
 }
 
@@ -600,13 +734,55 @@ int encode_cell(const Grid &g, const int c[3]) {
     return (c[0] * g.dim[1] + c[1]) * g.dim[2] + c[2];
 }
 
+inline float f_from_bits(uint32_t u) {
+    float f;
+    std::memcpy(&f, &u, 4);
+    return f;
+}
+inline uint32_t bits_of(float f) {
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    return u;
+}
+
+// Category of a value: bin index, or -1 when the pair is dropped.
+struct Category {
+    const std::vector<float> *t;
+    int n;
+    bool range;  // also apply the s^2 range test (min, max)
+    float rmin, rmax;
+    int operator()(double x) const {
+        const float xf = (float)x;
+        if (range && !(xf < rmax && xf > rmin)) return -1;
+        int c = 0;
+        for (int k = 0; k <= n; ++k)
+            if ((*t)[k] <= xf) c = k + 1;
+        const int b = c - 1;
+        return (b >= 0 && b < n) ? b : -1;
+    }
+};
+
+// Table entry for values in [v0, v1]: the category when every value within
+// g of the interval shares it, else ambiguous.
+unsigned char lut_entry(const Category &cat, const std::vector<double> &edges, double v0, double v1, double g) {
+    const double lo = v0 - g, hi = v1 + g;
+    for (double e : edges)
+        if (e > lo && e <= hi) return LUT_AMB;
+    const int c = cat(0.5 * (v0 + v1));
+    if (c != cat(lo) || c != cat(hi)) return LUT_AMB;
+    return c < 0 ? LUT_INV : (unsigned char)c;
+}
+
 }  // namespace
 
-// Work list: every (chunk of A cell, B cell) pair whose cell boxes are closer
-// than the maximum separation.  For an auto count a cell pair is visited
-// once (B after A in cell order) and a cell with itself keeps only j > i.
+// Work list.  For every (cell, region) run of A, the segments are the runs
+// of B in the cells whose boxes are closer than the maximum separation,
+// sorted by region; long A runs are split into chunks of TA points.  For an
+// auto count every unordered pair of points is visited once: a B run is a
+// segment of an A run when it starts after it in the sorted order, and the A
+// run's own segment starts at the chunk and keeps only j > i.
 void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, double side, double rb,
-                      std::vector<WorkItem> &items) {
+                      std::vector<WorkItem> &items, std::vector<Segment> &segs) {
     std::vector<int> offs;
     for (int ox = -m; ox <= m; ++ox)
         for (int oy = -m; oy <= m; ++oy)
@@ -623,43 +799,84 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
                 }
             }
     items.clear();
+    segs.clear();
+    std::vector<Segment> cand;
+    std::vector<std::pair<long long, int>> cost;  // (cost, item)
     for (int ca = 0; ca < ga.ncell; ++ca) {
         const int a0 = ga.h_cell_start[ca], a1 = ga.h_cell_start[ca + 1];
         if (a1 == a0) continue;
         int c[3];
         decode_cell(ga, ca, c);
-        for (size_t k = 0; k < offs.size(); k += 3) {
-            int cbv[3];
-            for (int mm = 0; mm < 3; ++mm) cbv[mm] = ga.kmin[mm] + c[mm] + offs[k + mm] - gb.kmin[mm];
-            const int cb = encode_cell(gb, cbv);
-            if (cb < 0) continue;
-            const int b0 = gb.h_cell_start[cb], b1 = gb.h_cell_start[cb + 1];
-            if (b1 == b0) continue;
-            if (is_auto && cb < ca) continue;
-            const bool self = is_auto && cb == ca;
-            for (int s = a0; s < a1; s += TA) {
-                WorkItem w;
-                w.a_start = s;
-                w.a_len = std::min(TA, a1 - s);
-                w.a_cell = ca;
-                w.b_cell = cb;
-                w.self = self ? 1 : 0;
-                w.a_cell_start = a0;
-                if (self) {
-                    // j > i: B starts at this chunk; later chunks' points follow.
-                    w.b_start = s;
-                    w.b_len = b1 - s;
-                } else {
-                    w.b_start = b0;
-                    w.b_len = b1 - b0;
+        const int ra0 = ga.h_region_start[ca], ra1 = ga.h_region_start[ca + 1];
+        for (int ra = ra0; ra < ra1; ++ra) {
+            const int s0 = ga.h_run_start[ra];
+            const int s1 = (ra + 1 < ra1) ? ga.h_run_start[ra + 1] : a1;
+            cand.clear();
+            for (size_t k = 0; k < offs.size(); k += 3) {
+                int cbv[3];
+                for (int mm = 0; mm < 3; ++mm) cbv[mm] = ga.kmin[mm] + c[mm] + offs[k + mm] - gb.kmin[mm];
+                const int cb = encode_cell(gb, cbv);
+                if (cb < 0) continue;
+                const int b0 = gb.h_cell_start[cb], b1 = gb.h_cell_start[cb + 1];
+                if (b1 == b0) continue;
+                if (is_auto && cb < ca) continue;
+                const int rb0 = gb.h_region_start[cb], rb1 = gb.h_region_start[cb + 1];
+                for (int rbk = rb0; rbk < rb1; ++rbk) {
+                    const int t0 = gb.h_run_start[rbk];
+                    const int t1 = (rbk + 1 < rb1) ? gb.h_run_start[rbk + 1] : b1;
+                    if (is_auto && t0 < s0) continue;
+                    Segment sg;
+                    sg.b_start = t0;
+                    sg.b_len = t1 - t0;
+                    sg.b_cell = cb;
+                    sg.meta = gb.h_regions[rbk] | ((is_auto && t0 == s0) ? (1 << 16) : 0);
+                    cand.push_back(sg);
                 }
+            }
+            if (cand.empty()) continue;
+            std::stable_sort(cand.begin(), cand.end(),
+                             [](const Segment &x, const Segment &y) { return (x.meta & 0xffff) < (y.meta & 0xffff); });
+            for (int s = s0; s < s1; s += TA) {
+                WorkItem w;
+                std::memset(&w, 0, sizeof(w));
+                w.a_start = s;
+                w.a_len = std::min(TA, s1 - s);
+                w.a_cell = ca;
+                w.a_region = ga.h_regions[ra];
+                w.seg_begin = (int)segs.size();
+                long long bl = 0;
+                for (Segment sg : cand) {
+                    if (sg.meta >> 16) {
+                        // the A run itself: j > i, starting at this chunk
+                        sg.b_len = sg.b_start + sg.b_len - s;
+                        sg.b_start = s;
+                    }
+                    // Close the item when it holds enough B points, so that a
+                    // count always splits into many more items than CTAs.
+                    if (bl > 0 && bl + sg.b_len > kItemMaxB) {
+                        w.seg_end = (int)segs.size();
+                        cost.push_back({(long long)w.a_len * bl, (int)items.size()});
+                        items.push_back(w);
+                        w.seg_begin = (int)segs.size();
+                        bl = 0;
+                    }
+                    bl += sg.b_len;
+                    segs.push_back(sg);
+                }
+                w.seg_end = (int)segs.size();
+                cost.push_back({(long long)w.a_len * bl, (int)items.size()});
                 items.push_back(w);
             }
         }
     }
-    std::stable_sort(items.begin(), items.end(), [](const WorkItem &x, const WorkItem &y) {
-        return (long long)x.a_len * x.b_len > (long long)y.a_len * y.b_len;
-    });
+    // Largest items first, so the dynamic queue ends balanced.
+    std::stable_sort(cost.begin(), cost.end(),
+                     [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
+                         return x.first > y.first;
+                     });
+    std::vector<WorkItem> sorted(items.size());
+    for (size_t k = 0; k < cost.size(); ++k) sorted[k] = items[cost[k].second];
+    items.swap(sorted);
 }
 
 #define TPCF_TRY(expr)                                                                        \
@@ -672,8 +889,13 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
         }                                                                                     \
     } while (0)
 
-// Error bounds of the FP32 path against the reference sequence (see the
-// derivation in the design notes): delta bounds |dx_fast - dx_ref| per axis.
+// Error bounds of the FP32 path against the reference sequence.  delta bounds
+// |dx_fast - dx_ref| per axis for cells of side `side` with offsets up to m
+// cells: the cell-relative coordinates, the cell offset, the shifted A
+// coordinate and the final difference each round once in float (relative
+// 2^-24), and the reference's own float rounding of the difference adds one
+// more.  The other bounds follow by first-order propagation through s^2, pi,
+// sigma^2 = s^2 - pi^2 and mu = |pi| / s, each doubled for safety.
 struct Guards {
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
 };
@@ -692,6 +914,75 @@ Guards compute_guards(double side, int m, double rb) {
     g.c2_mu = (float)(3.0 * delta * delta);
     g.g_mu0 = (float)(28.0 * u);
     return g;
+}
+
+// Host-built binning tables for one binning and one set of guards.
+struct Luts {
+    std::vector<unsigned char> l1, l2;
+    unsigned base1 = 0;
+    float scale2 = 0;
+    float s2_lut_min = 0;
+};
+
+Luts build_luts(const Binning &bin, const Guards &g) {
+    Luts L;
+    L.l1.assign(LUT1_N, LUT_AMB);
+    L.l2.assign(LUT2_N, LUT_AMB);
+    // Table 1 over the float bits of s^2 (monopole, s-mu; the range test is
+    // folded in) or of sigma^2 (sigma-pi).
+    const bool s_axis = bin.mode != MODE_SIGMA_PI;
+    Category c1{&bin.t1, bin.nb1, s_axis, bin.min_r_sq, bin.max_r_sq};
+    std::vector<double> e1(bin.t1.begin(), bin.t1.end());
+    if (s_axis) {
+        e1.push_back(bin.min_r_sq);
+        e1.push_back(std::nextafter(bin.min_r_sq, INFINITY));
+        e1.push_back(bin.max_r_sq);
+    }
+    const double xmax1 = std::max((double)bin.max_r_sq, 1e-30) * 2.0;
+    const int ehi = (int)std::ceil(std::log2(xmax1)) + 1;
+    const int elo = ehi - LUT1_OCTAVES;
+    const uint32_t sh = 23 - LUT1_BITS;
+    L.base1 = bits_of(std::ldexp(1.0f, elo)) >> sh;
+    const double g1 = s_axis ? g.g_s2 : g.g_a;
+    for (int i = 1; i < LUT1_N - 1; ++i) {
+        const double v0 = f_from_bits((L.base1 + i) << sh);
+        const double v1 = f_from_bits((L.base1 + i + 1) << sh);
+        L.l1[i] = lut_entry(c1, e1, v0, v1, g1);
+    }
+    // Bucket 0 holds everything below the table (ambiguous); the last bucket
+    // holds everything above it.
+    {
+        const double v0 = f_from_bits((L.base1 + LUT1_N - 1) << sh);
+        if (s_axis && v0 - g1 > bin.max_r_sq) L.l1[LUT1_N - 1] = LUT_INV;
+        if (!s_axis && std::isfinite(bin.t1[bin.nb1]) && v0 - g1 > bin.t1[bin.nb1]) L.l1[LUT1_N - 1] = LUT_INV;
+    }
+    if (bin.mode != MODE_MONOPOLE) {
+        // Table 2, linear buckets: mu on [0, 1.25) or |pi| on [0, 1.25 rmax).
+        const double xmax2 = bin.mode == MODE_S_MU ? 1.25 : 1.25 * std::sqrt((double)bin.max_r_sq);
+        L.scale2 = (float)(LUT2_N / xmax2);
+        Category c2{&bin.t2, bin.nb2, false, 0, 0};
+        std::vector<double> e2(bin.t2.begin(), bin.t2.end());
+        double g2;
+        if (bin.mode == MODE_S_MU) {
+            // The mu guard grows as 1/s; the table holds for s^2 >= s2_lut_min.
+            const double gt = 0.5 / L.scale2;
+            const double a = gt - g.g_mu0;
+            const double s = (g.c1_mu + std::sqrt((double)g.c1_mu * g.c1_mu + 4.0 * a * g.c2_mu)) / (2.0 * a);
+            L.s2_lut_min = (float)(s * s * 1.0001);
+            g2 = gt;
+        } else {
+            g2 = g.g_pi;
+        }
+        const double w = 1.0 / L.scale2;
+        for (int i = 0; i < LUT2_N - 1; ++i) {
+            const double v0 = i * w, v1 = (i + 1) * w;
+            const double slack = 4.0 * std::ldexp(1.0, -23) * v1;  // bucket-edge rounding of (int)(x * scale)
+            L.l2[i] = lut_entry(c2, e2, v0, v1, g2 + slack);
+        }
+        const double vlast = (LUT2_N - 1) * w;
+        if (c2(vlast - g2) < 0 && vlast - g2 > bin.t2[bin.nb2]) L.l2[LUT2_N - 1] = LUT_INV;
+    }
+    return L;
 }
 
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
@@ -721,42 +1012,37 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     else if (build_grid(ctx, B, side, true, req.exact_fp64, &gb, err)) return err->status;
 
     std::vector<WorkItem> items;
-    build_work_items(*ga, *gb, is_auto, m, side, rb, items);
+    std::vector<Segment> segs;
+    build_work_items(*ga, *gb, is_auto, m, side, rb, items, segs);
 
     // Fixed-point scale: the largest pair weight stays below 2^31.
-    bool unitw = A->unit_weights && B->unit_weights;
+    const bool unitw = A->unit_weights && B->unit_weights;
     float wscale = 1.0f;
     if (!unitw) {
         const double wmax = (double)A->w_max * (double)B->w_max * (1.0 + 1e-6);
-        const double wmin_abs = 0;
-        (void)wmin_abs;
         int S = (int)std::floor(30.0 - std::log2(std::max(wmax, 1e-30)));
         S = std::min(S, 100);
-        wscale = (float)std::ldexp(1.0, S);
-        if (!std::isfinite(wscale)) wscale = std::ldexp(1.0f, 100);
+        wscale = std::ldexp(1.0f, S);
     }
 
-    // Shared-memory budget: as many jackknife slots as fit.
-    const SmemLayout l0 = smem_layout(nb, 0, bin->nb1, bin->nb2, jk ? n_jk : 0, req.exact_fp64);
-    const size_t budget = ctx->smem_optin > 2048 ? ctx->smem_optin - 2048 : 0;  // static shared memory headroom
-    if (l0.total > budget) {
+    const SmemLayout L = smem_layout(nb, bin->nb1, bin->nb2, req.exact_fp64, jk);
+    if (L.total + 1024 > ctx->smem_optin) {
         err->status = 6;
         err->msg = "histogram does not fit in shared memory";
         return err->status;
     }
-    int ns = 0;
-    if (jk) {
-        const size_t per_slot = 8 * (size_t)nb;
-        ns = (int)std::min<size_t>((budget - l0.total) / per_slot, kMaxSlots);
-    }
-    const SmemLayout L = smem_layout(nb, ns, bin->nb1, bin->nb2, jk ? n_jk : 0, req.exact_fp64);
+    const Guards g = compute_guards(side, m, rb);
+    const Luts luts = build_luts(*bin, g);
 
     DevBuf<WorkItem> d_items;
+    DevBuf<Segment> d_segs;
     DevBuf<unsigned long long> d_full, d_sub, d_cnt;
     DevBuf<int> d_head, d_err;
     DevBuf<float> d_t1, d_t2;
+    DevBuf<unsigned char> d_l1, d_l2;
     cudaStream_t stm = ctx->stream;
     TPCF_TRY(d_items.alloc(items.size()));
+    TPCF_TRY(d_segs.alloc(segs.size()));
     TPCF_TRY(d_full.alloc(nb));
     TPCF_TRY(d_sub.alloc((size_t)nb * n_jk));
     TPCF_TRY(d_cnt.alloc(4));
@@ -764,11 +1050,17 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     TPCF_TRY(d_err.alloc(1));
     TPCF_TRY(d_t1.alloc(bin->t1.size()));
     TPCF_TRY(d_t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
-    if (!items.empty())
+    TPCF_TRY(d_l1.alloc(LUT1_N));
+    TPCF_TRY(d_l2.alloc(LUT2_N));
+    if (!items.empty()) {
         TPCF_TRY(cudaMemcpyAsync(d_items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemcpyAsync(d_segs.p, segs.data(), sizeof(Segment) * segs.size(), cudaMemcpyHostToDevice, stm));
+    }
     TPCF_TRY(cudaMemcpyAsync(d_t1.p, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
     if (!bin->t2.empty())
         TPCF_TRY(cudaMemcpyAsync(d_t2.p, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(d_l1.p, luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(d_l2.p, luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
     TPCF_TRY(cudaMemsetAsync(d_full.p, 0, sizeof(unsigned long long) * nb, stm));
     TPCF_TRY(cudaMemsetAsync(d_sub.p, 0, sizeof(unsigned long long) * nb * n_jk, stm));
     TPCF_TRY(cudaMemsetAsync(d_cnt.p, 0, sizeof(unsigned long long) * 4, stm));
@@ -777,24 +1069,23 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
 
     KParams P;
     std::memset(&P, 0, sizeof(P));
-    auto fill = [&](GridK &k, const Grid &g, const Catalog &c) {
-        k.pos = g.pos.p;
-        k.aux = g.aux.p;
-        k.idx = g.idx.p;
-        k.xyz_s = g.xyz_s.p;
-        k.unit_s = g.unit_s.p;
-        k.coord = g.cell_coord.p;
-        k.rstart = g.region_start.p;
-        k.regions = g.regions.p;
-        k.kmin0 = g.kmin[0];
-        k.kmin1 = g.kmin[1];
-        k.kmin2 = g.kmin[2];
+    auto fill = [&](GridK &k, const Grid &gr, const Catalog &c) {
+        k.pos = gr.pos.p;
+        k.aux = gr.aux.p;
+        k.idx = gr.idx.p;
+        k.xyz_s = gr.xyz_s.p;
+        k.unit_s = gr.unit_s.p;
+        k.coord = gr.cell_coord.p;
+        k.kmin0 = gr.kmin[0];
+        k.kmin1 = gr.kmin[1];
+        k.kmin2 = gr.kmin[2];
         k.xyz = c.xyz.p;
         k.unit = c.unit.p;
     };
     fill(P.a, *ga, *A);
     fill(P.b, *gb, *B);
     P.items = d_items.p;
+    P.segs = d_segs.p;
     P.n_items = (int)items.size();
     P.head = d_head.p;
     P.side = side;
@@ -803,44 +1094,41 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     P.nb = nb;
     P.min_r_sq = bin->min_r_sq;
     P.max_r_sq = bin->max_r_sq;
-    const Guards g = compute_guards(side, m, rb);
     P.g_s2 = g.g_s2;
     P.g_pi = g.g_pi;
     P.g_a = g.g_a;
     P.c1_mu = g.c1_mu;
     P.c2_mu = g.c2_mu;
     P.g_mu0 = g.g_mu0;
+    P.s2_lut_min = luts.s2_lut_min;
     P.lo_cut = bin->min_r_sq - g.g_s2;
     P.hi_cut = bin->max_r_sq + g.g_s2;
     P.t1g = d_t1.p;
     P.t2g = d_t2.p;
-    P.ax1_log = bin->ax1.log_binning;
-    P.ax1_min = bin->ax1.min;
-    P.ax1_inv_step = bin->ax1.inv_step;
-    P.ax1_ilb = bin->ax1.inv_log_of_base;
-    P.ax1_ils = bin->ax1.inv_log_step;
-    P.ax2_log = bin->ax2.log_binning;
-    P.ax2_min = bin->ax2.min;
-    P.ax2_inv_step = bin->ax2.inv_step;
-    P.ax2_ilb = bin->ax2.inv_log_of_base;
-    P.ax2_ils = bin->ax2.inv_log_step;
+    P.lut1g = d_l1.p;
+    P.lut2g = d_l2.p;
+    P.lut1_base = luts.base1;
+    P.lut2_scale = luts.scale2;
     P.g_full = d_full.p;
     P.g_sub = d_sub.p;
     P.n_jk = n_jk;
-    P.ns = ns;
     P.wscale = wscale;
     P.counters = d_cnt.p;
     P.err = d_err.p;
 
     KernelFn fn = pick(bin->mode, unitw, jk, req.exact_fp64);
     TPCF_TRY(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    int per_sm = 1;
+    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, L.total));
+    per_sm = std::max(per_sm, 1);
     cudaEvent_t e0, e1;
     TPCF_TRY(cudaEventCreate(&e0));
     TPCF_TRY(cudaEventCreate(&e1));
     TPCF_TRY(cudaEventRecord(e0, stm));
     if (!items.empty()) {
-        const int grid = std::min<int>(ctx->num_sms, (int)items.size());
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)items.size());
         fn<<<grid, NT, L.total, stm>>>(P);
+        ++ctx->launches;
         TPCF_TRY(cudaGetLastError());
     }
     TPCF_TRY(cudaEventRecord(e1, stm));

@@ -33,16 +33,27 @@ constexpr int kMaxBinsTotal = 8192;  // per histogram
 constexpr int kMaxMaskInts = 32;     // 64-bit masks per object for inverse-p weights
 constexpr int kMaxRegions = 4096;    // jackknife regions
 
-// One unit of device work: a chunk of cell A against all of cell B.
+// One unit of device work: a chunk of one (cell, jackknife region) run of
+// catalogue A against a list of runs of catalogue B (its segments) from the
+// neighbouring cells, sorted by region.  All A points of an item share one
+// region and all points of a segment share one region, so each segment's
+// pair histogram is added once to the row of its region and the item's total
+// once to the full histogram and to the row of the A region.
 struct WorkItem {
-    int a_start;  // first point of the A chunk (sorted order, grid A)
+    int a_start;    // first point of the A chunk (sorted order, grid A)
     int a_len;
-    int b_start;  // first point of cell B (sorted order, grid B)
+    int a_cell;     // dense cell index in grid A
+    int a_region;   // jackknife region of every A point of the item
+    int seg_begin;  // segments [seg_begin, seg_end) in the segment array
+    int seg_end;
+    int pad[2];
+};
+
+struct Segment {
+    int b_start;  // first point of the B run (sorted order, grid B)
     int b_len;
-    int a_cell;   // dense cell index in grid A
     int b_cell;   // dense cell index in grid B
-    int self;     // 1 when A and B are the same cell of the same catalogue (auto count)
-    int a_cell_start;  // first point of the whole A cell (for the self-pair ordering)
+    int meta;     // region of the run | (1 << 16) when it is the A run itself (auto count: only j > i)
 };
 
 }  // namespace tpcf
