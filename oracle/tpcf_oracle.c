@@ -547,3 +547,33 @@ double orc_ls(double dd, double dr, double rr) {
     if (rr == 0) return 0;
     return dd / rr - 2.0 * dr / rr + 1.0;
 }
+
+/* ------------------------------------------------ binning monotonicity --- */
+
+/* Exhaustive check that the reference binning is non-decreasing over every
+ * float in [lo, hi] (non-negative lo): the engine's threshold tables rely on
+ * it.  sqrt_space applies sqrtf first (s from s^2, sigma from s^2 - pi^2).
+ * Returns the first offending float's bit pattern, or 0xffffffff. */
+unsigned orc_axis_check_monotone(const orc_axis *ax, int sqrt_space, float lo, float hi) {
+    unsigned ulo, uhi;
+    memcpy(&ulo, &lo, 4);
+    memcpy(&uhi, &hi, 4);
+    unsigned bad = 0xffffffffu;
+    const unsigned chunk = 1u << 20;
+#pragma omp parallel for schedule(dynamic) reduction(min : bad)
+    for (long long c = ulo; c <= (long long)uhi; c += chunk) {
+        unsigned end = (unsigned)((c + chunk - 1 < (long long)uhi) ? c + chunk - 1 : uhi);
+        float x;
+        unsigned u = (unsigned)c;
+        memcpy(&x, &u, 4);
+        int prev = orc_to_int(orc_axis_bin_num(ax, sqrt_space ? sqrtf(x) : x));
+        for (unsigned v = u + 1; v <= end && v > u - 1; ++v) {
+            memcpy(&x, &v, 4);
+            int cur = orc_to_int(orc_axis_bin_num(ax, sqrt_space ? sqrtf(x) : x));
+            if (cur < prev && v < bad) bad = v;
+            prev = cur;
+            if (v == 0xffffffffu) break;
+        }
+    }
+    return bad;
+}

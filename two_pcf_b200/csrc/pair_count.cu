@@ -170,7 +170,7 @@ __device__ __forceinline__ int exact_bin(const ExactArgs &E, const float *t1, co
 
 // Guard-band re-evaluation from the original double arrays.
 template <int MODE>
-__device__ __noinline__ int exact_pair(const ExactArgs E, const float *t1, const float *t2, int ia, int jb,
+__device__ __forceinline__ int exact_pair(const ExactArgs E, const float *t1, const float *t2, int ia, int jb,
                                        bool *in_range) {
     const double *x1 = E.a_xyz + 3 * (size_t)ia, *x2 = E.b_xyz + 3 * (size_t)jb;
     float d0 = __double2float_rn(__dsub_rn(x1[0], x2[0]));
@@ -200,7 +200,7 @@ struct PreciseArgs {
 // a value lies within its bound of an edge.  Used for table buckets marked
 // ambiguous.
 template <int MODE>
-__device__ __noinline__ int precise_bin(const PreciseArgs P, const ExactArgs E, const float *t1, const float *t2,
+__device__ __forceinline__ int precise_bin(const PreciseArgs P, const ExactArgs E, const float *t1, const float *t2,
                                         float s2, float pi, int ia, int jb, bool *in_range, bool *guarded) {
     *guarded = false;
     const dev::AxisK ax1{t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
@@ -258,7 +258,7 @@ __device__ __forceinline__ int lut2_index(float scale, float x) {
 }
 
 struct Counters {
-    unsigned long long in_range = 0, guard = 0;
+    unsigned in_range = 0, guard = 0;  // per thread, folded into 64-bit totals per item
 };
 
 // Bin one pair that passed the guard-widened range test, from its FP32 s^2,
@@ -355,7 +355,7 @@ __device__ __forceinline__ void add64_owned(uint32_t *lo, uint32_t *hi, int i, u
 }
 
 template <int MODE, bool UNITW, bool JK, bool EXACT>
-__global__ void __launch_bounds__(NT, 2) pair_count_kernel(const KParams P) {
+__global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr bool kNeedAux = (MODE != MODE_MONOPOLE);
     const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK);
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(NT, 2) pair_count_kernel(const KParams P) {
     const ExactArgs EA{P.a.xyz, P.a.unit, P.b.xyz, P.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2};
     const PreciseArgs PA{P.n1, P.n2, P.min_r_sq, P.max_r_sq, P.g_s2, P.g_pi, P.g_a, P.c1_mu, P.c2_mu, P.g_mu0};
     Counters cnt;
-    unsigned long long n_cand = 0, n_flush = 0;
+    unsigned long long n_cand = 0, n_flush = 0, tot_in = 0, tot_guard = 0;
     unsigned tcount = 0;  // tiles staged so far by this CTA (selects buffer and phase)
 
     auto issue = [&](unsigned tc, int start, int len) {
@@ -424,6 +424,9 @@ __global__ void __launch_bounds__(NT, 2) pair_count_kernel(const KParams P) {
         const int item = s_item[0];
         if (item >= P.n_items) break;
         const WorkItem it = P.items[item];
+        tot_in += cnt.in_range;
+        tot_guard += cnt.guard;
+        cnt.in_range = cnt.guard = 0;
 
         // ---- phase mapping: Pn groups of G threads; each group holds the
         // whole A chunk (G * R slots) and takes every Pn-th B point, so short
@@ -662,7 +665,7 @@ __global__ void __launch_bounds__(NT, 2) pair_count_kernel(const KParams P) {
         }
     }
     // ---- counters
-    unsigned long long v0 = cnt.in_range, v1 = cnt.guard;
+    unsigned long long v0 = tot_in + cnt.in_range, v1 = tot_guard + cnt.guard;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
         v0 += __shfl_down_sync(0xffffffffu, v0, o);
