@@ -27,8 +27,8 @@ OUT="$HERE/_ref"
 CXX=${TPCF_CXX:-g++}
 
 if [ ! -f "$REF/src/correlators.cpp" ]; then
-    echo "build_ref.sh: reference sources not found under $REF" >&2
-    exit 2
+    echo "build_ref.sh: reference sources not found under $REF; keeping any prebuilt oracle/_ref" >&2
+    exit 0
 fi
 mkdir -p "$OUT"
 
