@@ -123,6 +123,38 @@ int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int c
 int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                int precision, double *full_out, double *region_out, tpcf_stats *stats);
 
+/* tpcf_count without device allocation.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc while they count: applications
+ * whose memory manager has reserved the device's memory for its own pool,
+ * where a foreign allocation fails or fragments it, and latency-bound loops
+ * that cannot take the device-wide synchronisation cudaFree implies.  Same
+ * arguments, results and errors as tpcf_count; the caller passes the
+ * catalogues, the binning and the output arrays as before.
+ *
+ * - Scratch: every device buffer the count needs (work list, segment list,
+ *   fixed-point histograms, counters, tables) lives in one static device
+ *   array of 32 MiB (33554432 bytes) that each device loading the library
+ *   holds until the process exits.  A count that needs more (many work items,
+ *   or bins x jackknife regions above ~4M) is refused with
+ *   TPCF_E_UNSUPPORTED and a message giving the size; tpcf_count handles it.
+ * - Set-up: the first call on a device looks up the array's device address
+ *   (cudaGetSymbolAddress) with that device current; make that first call
+ *   before any stream capture.
+ * - Cell grids: the call builds none.  The catalogues must already hold the
+ *   grid for this binning, refinement and precision, which an earlier
+ *   tpcf_count (or tpcf_auto/cross_pair_count) of the same catalogues caches;
+ *   otherwise TPCF_E_INVALID_ARG.  tpcf_catalog_release_cache drops them.
+ * - Sharing: every call on a device uses the same array, which keeps the
+ *   last call's contents; each call clears what it accumulates into.  Calls
+ *   whose work overlaps on the GPU (contexts on different streams of one
+ *   device, driven from several host threads) race on the array.  Calls from
+ *   one thread never overlap: each returns after its results are read back.
+ * - stats->ms_kernel is not measured (0); host staging buffers use the C++
+ *   heap. */
+int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                       int precision, double *full_out, double *region_out, tpcf_stats *stats);
+
 /* The reference's counting entry points with its output convention: the
  * histograms after invert_jk_hists() and, for auto counts, multiply_hists(2.0)
  * — what auto_pair_count_{monopole,sigma_pi,s_mu}(const GalaxyBoxes*, JKHists*)

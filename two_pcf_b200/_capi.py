@@ -58,6 +58,7 @@ _PROTOTYPES = {
     "tpcf_binning_total_bins": (C.c_int, [_vp]),
     "tpcf_binning_thresholds": (C.c_int, [_vp, C.c_int, _vp, C.c_int]),
     "tpcf_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_count_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),

@@ -392,6 +392,44 @@ int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, cons
     return TPCF_OK;
 }
 
+int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                       int precision, double *full_out, double *region_out, tpcf_stats *stats) {
+    if (!ctx || !a || !bin || !full_out) return TPCF_E_INVALID_ARG;
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
+    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "angular binning: use the angular counter");
+    if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
+        return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    auto t0 = std::chrono::steady_clock::now();
+    const int nb = bin->b.nb;
+    if (a->c.n_kept == 0 || (b && b->c.n_kept == 0)) {
+        std::memset(full_out, 0, sizeof(double) * nb);
+        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return TPCF_OK;
+    }
+    tpcf::CountRequest req;
+    req.a = &a->c;
+    req.b = b ? &b->c : nullptr;
+    req.bin = &bin->b;
+    req.exact_fp64 = precision == TPCF_FP64;
+    tpcf::Stats st;
+    tpcf::Error err{0, ""};
+    int rc = tpcf::run_count_static(&ctx->c, req, full_out, region_out, &st, &err);
+    if (rc) return fail(ctx, rc, err.msg);
+    if (stats) {
+        stats->candidates = st.candidates;
+        stats->in_range = st.in_range;
+        stats->guard_evals = st.guard;
+        stats->overflow_updates = st.overflow;
+        stats->work_items = st.items;
+        stats->ms_kernel = 0.0;
+        stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return TPCF_OK;
+}
+
 static int reference_form(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                           int precision, double *full, double *sub, tpcf_stats *stats) {
     if (!sub) return fail(ctx, TPCF_E_INVALID_ARG, "sub_hist is NULL");

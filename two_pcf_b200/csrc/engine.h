@@ -121,6 +121,9 @@ struct Ctx {
 
 // grid.cu
 int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_fp64, Grid **out, Error *err);
+// The grid build_grid would return when it is already cached, else nullptr;
+// never allocates.
+Grid *find_grid(Catalog *cat, double side, bool subset_kept, bool want_fp64);
 
 // pair_count.cu
 struct CountRequest {
@@ -132,6 +135,12 @@ struct CountRequest {
     int refinement = 0;
 };
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);
+// run_count without device allocation: every scratch buffer is carved from
+// one static device array of kStaticScratchBytes, and the catalogues' cell
+// grids must already be cached.
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
+                     Error *err);
 
 // diag.cu
 int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err);

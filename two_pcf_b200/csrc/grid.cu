@@ -234,6 +234,14 @@ __global__ void regions_kernel(GeomDev g, int ncell, const int *__restrict__ bst
         }                                                                                \
     } while (0)
 
+Grid *find_grid(Catalog *cat, double side, bool subset_kept, bool want_fp64) {
+    char key[96];
+    snprintf(key, sizeof(key), "%a|%d", side, subset_kept ? 1 : 0);
+    auto it = cat->grids.find(key);
+    if (it == cat->grids.end() || (want_fp64 && !it->second->has_fp64)) return nullptr;
+    return it->second.get();
+}
+
 int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_fp64, Grid **out, Error *err) {
     char key[96];
     snprintf(key, sizeof(key), "%a|%d", side, subset_kept ? 1 : 0);

@@ -26,6 +26,8 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "engine.h"
@@ -1166,6 +1168,274 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
         st->overflow += hc[3];
         st->items += items.size();
         st->ms_kernel += ms;
+    }
+    return 0;
+}
+
+
+// ---------------------------------------------------------------------------
+// Counting without device allocation.
+//
+// Some callers cannot call cudaMalloc while they count: applications whose
+// memory manager has reserved the device's memory for its own pool (a
+// framework's caching allocator, a serving process sized to the whole card),
+// where a foreign allocation fails or fragments that pool, and latency-bound
+// loops that cannot take the device-wide synchronisation cudaFree implies.
+// For them every scratch buffer of run_count — the work list, the segment
+// list, the 64-bit fixed-point histograms, the counters, the work-queue head,
+// the error flag, the threshold and lookup tables — is carved from the one
+// static array below, of kStaticScratchBytes (32 MiB).  Each device that
+// loads the library holds that array until the process exits.
+//
+// The array is shared by every call on a device and keeps the contents of
+// the last call; each call clears the histograms, counters, queue head and
+// error flag before its launch.  Two calls whose work overlaps on the GPU
+// (two contexts on one device, on different streams, from different host
+// threads) race on it.  Calls from one thread do not overlap: each waits for
+// its results before it returns.
+static __device__ __align__(256) unsigned char g_count_scratch[kStaticScratchBytes];
+
+namespace {
+
+constexpr int kMaxScratchDevices = 64;
+std::mutex g_scratch_mutex;
+void *g_scratch_addr[kMaxScratchDevices];
+
+// Device address of g_count_scratch on `device`, which must be current.  In
+// host code g_count_scratch only names the symbol; its address on a device
+// comes from cudaGetSymbolAddress, looked up on the first call per device
+// and remembered.
+int scratch_address(int device, void **out, Error *err) {
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess || cur != device || device < 0 || device >= kMaxScratchDevices) {
+        err->status = 3;
+        err->msg = "static scratch: device " + std::to_string(device) + " is not current or out of range";
+        return err->status;
+    }
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[device]) {
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_count_scratch);
+        if (e != cudaSuccess || !p) {
+            err->status = 3;
+            err->msg = std::string("static scratch: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e);
+            return err->status;
+        }
+        g_scratch_addr[device] = p;
+    }
+    *out = g_scratch_addr[device];
+    return 0;
+}
+
+// Byte offsets of the buffers inside the static array, each 256-aligned.
+struct ScratchPlan {
+    size_t items, segs, full, sub, cnt, head, err, t1, t2, l1, l2, total = 0;
+    size_t take(size_t bytes) {
+        const size_t off = total;
+        total += (std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
+        return off;
+    }
+};
+
+}  // namespace
+
+int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
+                     Error *err) {
+    const Binning *bin = req.bin;
+    Catalog *A = const_cast<Catalog *>(req.a);
+    Catalog *B = const_cast<Catalog *>(req.b ? req.b : req.a);
+    const bool is_auto = (req.b == nullptr);
+    const int nb = bin->nb;
+    const int n_jk = bin->n_jk;
+    const bool jk = n_jk > 1;
+    const double rb = bin->rmax_bound;
+
+    // The same cell size as run_count, so that the grids it cached are found.
+    int m = req.refinement > 0 ? req.refinement : ctx->refinement;
+    if (m <= 0) {
+        double vol = 1;
+        for (int k = 0; k < 3; ++k) vol *= std::max(A->hi_kept[k] - A->lo_kept[k], rb);
+        const double per_cell = A->n_kept * (rb / 2) * (rb / 2) * (rb / 2) / vol;
+        m = per_cell >= 256 ? 2 : 1;
+    }
+    const double side = rb / m * (1.0 + 1e-9);
+
+    // Scratch layout.  The histogram and table part is known before the work
+    // list is built; refuse an oversized binning before anything else.
+    ScratchPlan plan;
+    plan.full = plan.take(sizeof(unsigned long long) * nb);
+    plan.sub = plan.take(sizeof(unsigned long long) * (size_t)nb * n_jk);
+    plan.cnt = plan.take(sizeof(unsigned long long) * 4);
+    plan.head = plan.take(sizeof(int));
+    plan.err = plan.take(sizeof(int));
+    plan.t1 = plan.take(sizeof(float) * bin->t1.size());
+    plan.t2 = plan.take(sizeof(float) * std::max<size_t>(bin->t2.size(), 1));
+    plan.l1 = plan.take(LUT1_N);
+    plan.l2 = plan.take(LUT2_N);
+    auto too_big = [&](size_t n_items, size_t n_segs) {
+        err->status = 6;
+        err->msg = "count needs " + std::to_string(plan.total) + " bytes of scratch (" + std::to_string(nb) +
+                   " bins x " + std::to_string(n_jk) + " regions, " + std::to_string(n_items) + " work items, " +
+                   std::to_string(n_segs) + " segments); the static scratch holds " +
+                   std::to_string(kStaticScratchBytes) + " bytes: use tpcf_count";
+        return err->status;
+    };
+    if (plan.total > kStaticScratchBytes) return too_big(0, 0);
+
+    Grid *ga = find_grid(A, side, true, req.exact_fp64);
+    Grid *gb = is_auto ? ga : find_grid(B, side, true, req.exact_fp64);
+    if (!ga || !gb) {
+        err->status = 1;
+        err->msg = std::string("no cell grid cached on catalogue ") + (!ga ? "a" : "b") +
+                   " for this binning, refinement and precision: the allocation-free count does not build "
+                   "grids; count the same catalogues once with tpcf_count first";
+        return err->status;
+    }
+
+    std::vector<WorkItem> items;
+    std::vector<Segment> segs;
+    build_work_items(*ga, *gb, is_auto, m, side, rb, items, segs);
+
+    plan.items = plan.take(sizeof(WorkItem) * items.size());
+    plan.segs = plan.take(sizeof(Segment) * segs.size());
+    if (plan.total > kStaticScratchBytes) return too_big(items.size(), segs.size());
+
+    const bool unitw = A->unit_weights && B->unit_weights;
+    float wscale = 1.0f;
+    if (!unitw) {
+        const double wmax = (double)A->w_max * (double)B->w_max * (1.0 + 1e-6);
+        int S = (int)std::floor(30.0 - std::log2(std::max(wmax, 1e-30)));
+        S = std::min(S, 100);
+        wscale = std::ldexp(1.0f, S);
+    }
+    const SmemLayout L = smem_layout(nb, bin->nb1, bin->nb2, req.exact_fp64, jk);
+    if (L.total + 1024 > ctx->smem_optin) {
+        err->status = 6;
+        err->msg = "histogram does not fit in shared memory";
+        return err->status;
+    }
+    const Guards g = compute_guards(side, m, rb);
+    const Luts luts = build_luts(*bin, g);
+
+    void *base = nullptr;
+    if (scratch_address(ctx->device, &base, err)) return err->status;
+    unsigned char *sp = static_cast<unsigned char *>(base);
+    WorkItem *d_items = reinterpret_cast<WorkItem *>(sp + plan.items);
+    Segment *d_segs = reinterpret_cast<Segment *>(sp + plan.segs);
+    unsigned long long *d_full = reinterpret_cast<unsigned long long *>(sp + plan.full);
+    unsigned long long *d_sub = reinterpret_cast<unsigned long long *>(sp + plan.sub);
+    unsigned long long *d_cnt = reinterpret_cast<unsigned long long *>(sp + plan.cnt);
+    int *d_head = reinterpret_cast<int *>(sp + plan.head);
+    int *d_err = reinterpret_cast<int *>(sp + plan.err);
+    float *d_t1 = reinterpret_cast<float *>(sp + plan.t1);
+    float *d_t2 = reinterpret_cast<float *>(sp + plan.t2);
+    unsigned char *d_l1 = sp + plan.l1;
+    unsigned char *d_l2 = sp + plan.l2;
+
+    cudaStream_t stm = ctx->stream;
+    if (!items.empty()) {
+        TPCF_TRY(cudaMemcpyAsync(d_items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemcpyAsync(d_segs, segs.data(), sizeof(Segment) * segs.size(), cudaMemcpyHostToDevice, stm));
+    }
+    TPCF_TRY(cudaMemcpyAsync(d_t1, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
+    if (!bin->t2.empty())
+        TPCF_TRY(cudaMemcpyAsync(d_t2, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(d_l1, luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(d_l2, luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
+    // What the kernel accumulates into starts at zero on every call.
+    TPCF_TRY(cudaMemsetAsync(d_full, 0, sizeof(unsigned long long) * nb, stm));
+    TPCF_TRY(cudaMemsetAsync(d_sub, 0, sizeof(unsigned long long) * (size_t)nb * n_jk, stm));
+    TPCF_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, stm));
+    TPCF_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), stm));
+    TPCF_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stm));
+
+    KParams P;
+    std::memset(&P, 0, sizeof(P));
+    auto fill = [&](GridK &k, const Grid &gr, const Catalog &c) {
+        k.pos = gr.pos.p;
+        k.aux = gr.aux.p;
+        k.idx = gr.idx.p;
+        k.xyz_s = gr.xyz_s.p;
+        k.unit_s = gr.unit_s.p;
+        k.coord = gr.cell_coord.p;
+        k.kmin0 = gr.kmin[0];
+        k.kmin1 = gr.kmin[1];
+        k.kmin2 = gr.kmin[2];
+        k.xyz = c.xyz.p;
+        k.unit = c.unit.p;
+    };
+    fill(P.a, *ga, *A);
+    fill(P.b, *gb, *B);
+    P.items = d_items;
+    P.segs = d_segs;
+    P.n_items = (int)items.size();
+    P.head = d_head;
+    P.side = side;
+    P.n1 = bin->nb1;
+    P.n2 = bin->mode == MODE_MONOPOLE ? 0 : bin->nb2;
+    P.nb = nb;
+    P.min_r_sq = bin->min_r_sq;
+    P.max_r_sq = bin->max_r_sq;
+    P.g_s2 = g.g_s2;
+    P.g_pi = g.g_pi;
+    P.g_a = g.g_a;
+    P.c1_mu = g.c1_mu;
+    P.c2_mu = g.c2_mu;
+    P.g_mu0 = g.g_mu0;
+    P.s2_lut_min = luts.s2_lut_min;
+    P.lo_cut = bin->min_r_sq - g.g_s2;
+    P.hi_cut = bin->max_r_sq + g.g_s2;
+    P.t1g = d_t1;
+    P.t2g = d_t2;
+    P.lut1g = d_l1;
+    P.lut2g = d_l2;
+    P.lut1_base = luts.base1;
+    P.lut2_scale = luts.scale2;
+    P.g_full = d_full;
+    P.g_sub = d_sub;
+    P.n_jk = n_jk;
+    P.wscale = wscale;
+    P.counters = d_cnt;
+    P.err = d_err;
+
+    KernelFn fn = pick(bin->mode, unitw, jk, req.exact_fp64);
+    TPCF_TRY(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+    int per_sm = 1;
+    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, L.total));
+    per_sm = std::max(per_sm, 1);
+    if (!items.empty()) {
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)items.size());
+        fn<<<grid, NT, L.total, stm>>>(P);
+        ++ctx->launches;
+        TPCF_TRY(cudaGetLastError());
+    }
+    std::vector<unsigned long long> hf(nb), hs((size_t)nb * n_jk), hc(4);
+    int herr = 0;
+    TPCF_TRY(cudaMemcpyAsync(hf.data(), d_full, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(hs.data(), d_sub, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(hc.data(), d_cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaStreamSynchronize(stm));
+    if (herr) {
+        err->status = 4;
+        err->msg = "device wait exceeded its iteration limit; results discarded";
+        return err->status;
+    }
+    const double inv = unitw ? 1.0 : 1.0 / (double)wscale;
+    for (int b = 0; b < nb; ++b) full_out[b] = (double)(long long)hf[b] * inv;
+    if (region_out) {
+        if (jk)
+            for (size_t k = 0; k < hs.size(); ++k) region_out[k] = (double)(long long)hs[k] * inv;
+        else
+            for (int b = 0; b < nb; ++b) region_out[b] = full_out[b];
+    }
+    if (st) {
+        st->candidates += hc[0];
+        st->in_range += hc[1];
+        st->guard += hc[2];
+        st->overflow += hc[3];
+        st->items += items.size();
     }
     return 0;
 }
