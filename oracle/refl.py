@@ -186,3 +186,99 @@ def count_3d(mode, cat1, cat2=None, *, is_auto, n_jk=1, axes, n_threads=0):
     if rc != 0:
         raise RuntimeError("ref_count_3d failed")
     return full, sub.reshape(n_jk, nb), used
+
+
+# ----------------------------------------------------------- inverse-p build
+
+N_MASK_INTS_INVP = 32  # _N_MASK_INTS of the inverse-p build (oracle/build_ref.sh)
+
+
+def invp_params(*, n_jk=1, healpix_order=5, theta_max=0.175, theta_n_bins=40, theta_log_base=1.6,
+                n_bitwise_runs=2048, monopole=(0.0, 100.0, 30, 1.3), sigma=(0.0, 50.0, 50, 1.0),
+                pi=(0.0, 50.0, 50, 1.0), s=(0.0, 100.0, 40, 1.3), mu_n_bins=50,
+                dd_file="ang_dd.hdf5", ddi_file="ang_dd_invp.hdf5", dr_file="ang_dr.hdf5",
+                dri_file="ang_dr_invp.hdf5") -> str:
+    """A parameter file for the inverse-p build with every key set (the
+    reference leaves absent keys uninitialised, src/io.cpp:16-237)."""
+    kv = {
+        "data_filename": "data.hdf5", "data_file_type": "hdf5", "random_filename": "rand.hdf5",
+        "random_file_type": "hdf5", "coord_system": "cartesian", "ra_x_dataset_name": "x",
+        "dec_y_dataset_name": "y", "z_z_dataset_name": "z", "weight_dataset_name": "w",
+        "jk_dataset_name": "jk", "bitwise_weight_dataset_name": "bw", "dither_weight_dataset_name": "dw",
+        "use_weights": 1, "n_jk_regions": n_jk, "omega_m": 0.25, "h": 1.0, "z_min": 0.0, "z_max": 1.0,
+        "plot_monopole": 0, "plot_sigma_pi": 0, "plot_s_mu": 0, "monopole_filename": "mono.txt",
+        "monopole_output_type": "ascii", "monopole_min": monopole[0], "monopole_max": monopole[1],
+        "monopole_n_bins": monopole[2], "monopole_log_base": monopole[3], "sigma_pi_filename": "sp.txt",
+        "sigma_pi_output_type": "ascii", "sigma_min": sigma[0], "sigma_max": sigma[1],
+        "sigma_n_bins": sigma[2], "sigma_log_base": sigma[3], "pi_min": pi[0], "pi_max": pi[1],
+        "pi_n_bins": pi[2], "pi_log_base": pi[3], "s_mu_filename": "smu.txt", "s_mu_output_type": "ascii",
+        "s_min": s[0], "s_max": s[1], "s_n_bins": s[2], "s_log_base": s[3], "mu_n_bins": mu_n_bins,
+        "n_threads": 1, "healpix_order": healpix_order, "theta_max": repr(float(theta_max)),
+        "theta_n_bins": theta_n_bins, "theta_log_base": theta_log_base, "n_bitwise_runs": n_bitwise_runs,
+        "calculate_angular_dd": 0, "calculate_angular_dd_invpweights": 0, "calculate_angular_dr": 0,
+        "calculate_angular_dr_invpweights": 0, "angular_dd_filename": dd_file,
+        "angular_dd_invpweights_filename": ddi_file, "angular_dr_filename": dr_file,
+        "angular_dr_invpweights_filename": dri_file,
+    }
+    return "".join(f"{k} = {v}\n" for k, v in kv.items())
+
+
+def _invp_cat(cat):
+    """cat dict -> the 7 pointers + n of the harness (xyz, unit, dcom, w, iw,
+    jk, masks[n x 32] object-major)."""
+    if cat is None:
+        return [None] * 7 + [0], []
+    arrs = [_opt(cat["xyz"], np.float64), _opt(cat.get("unit"), np.float64), _opt(cat.get("dcom"), np.float64),
+            _opt(cat.get("w"), np.float32), _opt(cat.get("iw"), np.float32), _opt(cat.get("jk"), np.int32),
+            _opt(cat.get("masks"), np.int64)]
+    if arrs[6] is not None:
+        assert arrs[6].shape == (arrs[0].shape[0], N_MASK_INTS_INVP)
+    return [_ptr(a) for a in arrs] + [arrs[0].shape[0]], arrs
+
+
+def invp_angular(params: str, kind, cat1, cat2=None, *, n_jk, n_bins, n_threads=0):
+    """Angular stage: kind 0 DD, 1 DD inverse-p, 2 DR, 3 DR inverse-p
+    (src/correlators_invpweight.cpp:713-982).  Returns (full, sub[n_jk, nb])
+    after invert_jk_hists and (auto) x2."""
+    p1, keep1 = _invp_cat(cat1)
+    p2, keep2 = _invp_cat(cat2)
+    full = np.zeros(n_bins)
+    sub = np.zeros(n_bins * n_jk)
+    rc = invp().ref_invp_angular(params.encode(), int(kind), *p1, *p2, n_threads, full, sub)
+    if rc != 0:
+        raise RuntimeError("ref_invp_angular failed")
+    return full, sub.reshape(n_jk, n_bins)
+
+
+def invp_store_angular(params: str, fname: str, full, sub):
+    full = np.ascontiguousarray(full, np.float64)
+    sub = np.ascontiguousarray(sub, np.float64).reshape(-1)
+    if invp().ref_invp_store_angular(params.encode(), fname.encode(), full, sub) != 0:
+        raise RuntimeError("ref_invp_store_angular failed")
+
+
+def invp_interp(num_file: str, den_file: str, values) -> np.ndarray:
+    v = np.ascontiguousarray(values, np.float64)
+    out = np.empty_like(v)
+    if invp().ref_invp_interp(num_file.encode(), den_file.encode(), v, v.size, out) != 0:
+        raise RuntimeError("ref_invp_interp failed")
+    return out
+
+
+def invp_count_3d(params: str, mode, how, cat1, cat2=None, *, n_jk, nb, n_threads=0):
+    """3-D counts of the inverse-p build: how = 1 DD with inverse-p weights,
+    0 DR with the angular DR up-weight, 2 plain auto count.  The angular
+    histograms must have been stored under the params' file names."""
+    p1, keep1 = _invp_cat(cat1)
+    p2, keep2 = _invp_cat(cat2)
+    full = np.zeros(nb)
+    sub = np.zeros(nb * n_jk)
+    rc = invp().ref_invp_count_3d(params.encode(), int(mode), int(how), *p1, *p2, n_threads, full, sub)
+    if rc != 0:
+        raise RuntimeError("ref_invp_count_3d failed")
+    return full, sub.reshape(n_jk, nb)
+
+
+def invp_reset():
+    """Forget every in-memory HDF5 file of the stand-in library."""
+    invp().ref_h5_reset()
