@@ -36,7 +36,8 @@ typedef enum {
     TPCF_MONOPOLE = 0, /* Hist on s                        (src/correlators.cpp:127-153) */
     TPCF_SIGMA_PI = 1, /* Hist2D on (sigma, |pi|)          (src/correlators.cpp:280-307) */
     TPCF_S_MU = 2,     /* Hist2D on (s, mu), mu in [0, 1]  (src/correlators.cpp:432-459) */
-    TPCF_ANGULAR = 3   /* Hist on 1 - cos(theta)           (src/correlators_invpweight.cpp:985-1033) */
+    TPCF_ANGULAR = 3   /* Hist on 1 - cos(theta)           (src/correlators_invpweight.cpp:985-1033);
+                          ax1 = (0, 1 - cos(theta_max), theta_log_base, theta_n_bins) */
 } tpcf_mode;
 
 typedef enum {
@@ -123,6 +124,59 @@ int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int c
 int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                int precision, double *full_out, double *region_out, tpcf_stats *stats);
 
+/* Pair weighting of tpcf_count_weighted (the reference's _USE_INV_WEIGHTS
+ * build, src/correlators_invpweight.cpp). */
+typedef enum {
+    /* 3-D: weight1 * weight2 over the points kept by the d_comov partition.
+     * Angular: input_weight1 * input_weight2 over every point
+     * (auto/cross_pair_count_angular, :860-982). */
+    TPCF_WEIGHTS_PLAIN = 0,
+    /* Inverse-p DD: input_weight1 * input_weight2 * n_bitwise_runs / popc,
+     * popc = number of bits set in mask1 & mask2 (1 when none), times the
+     * angular up-weight in 3-D (auto_pair_count_*_invpweights, :14-709;
+     * auto_pair_count_angular_invpweights, :713-818).  Angular counts use the
+     * points with d_comov >= 0 (GalaxyPixels' require_redshift). */
+    TPCF_WEIGHTS_INVP_DD = 1,
+    /* Inverse-p DR: 3-D weight1 * weight2 * angular up-weight
+     * (cross_pair_count_*_invpweights); angular weight1 * weight2 over points
+     * with d_comov >= 0 (cross_pair_count_angular_invpweights). */
+    TPCF_WEIGHTS_INVP_DR = 2
+} tpcf_weighting;
+
+typedef struct {
+    int32_t weighting;       /* tpcf_weighting */
+    int32_t n_bitwise_runs;  /* Params::n_bitwise_runs */
+    /* 3-D inverse-p counts only: the angular up-weight is JKHists::interp
+     * (src/hist.cpp:369-391) of up_numerator / up_denominator bin by bin
+     * (divide_by_hist, :224-231) on theta_axis = (0, 1 - cos(theta_max),
+     * theta_log_base, theta_n_bins): the angular DD and DD-inverse-p full
+     * histograms for DD counts, DR and DR-inverse-p for DR counts, as the
+     * angular stage wrote them (calc_angular_upweight, :985-1033). */
+    tpcf_axis_spec theta_axis;
+    const double *up_numerator;
+    const double *up_denominator;
+} tpcf_weight_spec;
+
+/* tpcf_count with a pair weighting (spec NULL: TPCF_WEIGHTS_PLAIN).  Angular
+ * binnings (TPCF_ANGULAR) count (float)(1 - cos(theta)) of the unit vectors
+ * with no separation cut.  TPCF_WEIGHTS_INVP_DD needs bitmasks of the same
+ * width on both catalogues.  A pair whose up-weight is not finite (an empty
+ * angular bin makes 0/0) turns its bins into NaN or an infinity, as the
+ * reference's double sums do. */
+int tpcf_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                        const tpcf_weight_spec *spec, int precision, double *full_out, double *region_out,
+                        tpcf_stats *stats);
+/* The same with the reference's output convention (inverted jackknife
+ * histograms, x2 for auto counts): what the *_invpweights and *_angular
+ * counting functions leave in their JKHists. */
+int tpcf_pair_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                             const tpcf_weight_spec *spec, int precision, double *full_hist, double *sub_hist,
+                             tpcf_stats *stats);
+/* Host-side evaluation of the up-weight of a 3-D inverse-p spec at values of
+ * 1 - cos(theta), with the tables and arithmetic the kernels use; replaces
+ * JKHists::interp after divide_by_hist (src/hist.cpp:224-231, :369-391). */
+int tpcf_upweight_eval(const tpcf_weight_spec *spec, const double *values, int64_t n, double *out);
+
 /* tpcf_count without device allocation.  No counterpart in the reference.
  *
  * For callers that cannot call cudaMalloc while they count: applications
@@ -136,7 +190,7 @@ int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, cons
  *   fixed-point histograms, counters, tables) lives in one static device
  *   array of 32 MiB (33554432 bytes) that each device loading the library
  *   holds until the process exits.  A count that needs more (many work items,
- *   or bins x jackknife regions above ~4M) is refused with
+ *   or bins x jackknife regions above ~2M) is refused with
  *   TPCF_E_UNSUPPORTED and a message giving the size; tpcf_count handles it.
  * - Set-up: the first call on a device looks up the array's device address
  *   (cudaGetSymbolAddress) with that device current; make that first call

@@ -163,9 +163,79 @@ def make(name):
     return out
 
 
+# ---------------------------------------------------------- inverse-p build
+
+INVP_THETA = (0.175, 20, 1.0)   # theta_max, n_bins, log base (linear: every bin filled)
+INVP_THETA_LOG = (0.175, 40, 1.6)
+INVP_SMU = (0.0, 60.0, 1.3, 20, 0.0, 1.0, 0.0, 10)
+N_RUNS = 2048
+
+
+def case_sky(seed, n, n_jk, *, masks_all_set=False):
+    rng = np.random.default_rng(seed)
+    ra = rng.uniform(0.0, 14.0, n)
+    dec = np.degrees(np.arcsin(rng.uniform(np.sin(np.radians(-5)), np.sin(np.radians(5)), n)))
+    u = np.stack([np.cos(np.radians(dec)) * np.cos(np.radians(ra)),
+                  np.cos(np.radians(dec)) * np.sin(np.radians(ra)), np.sin(np.radians(dec))], 1)
+    u[1:11] = u[11:21]  # identical directions
+    d = rng.uniform(400.0, 700.0, n)
+    xyz = u * d[:, None]
+    from two_pcf_b200 import synthetic
+    masks = synthetic.bitwise_masks(seed + 5, n, n_runs=N_RUNS, all_set=masks_all_set)
+    return {"xyz": xyz, "unit": u, "dcom": d, "w": rng.lognormal(0, 0.2, n).astype(np.float32),
+            "iw": rng.lognormal(0, 0.3, n).astype(np.float32), "jk": rng.integers(0, n_jk, n).astype(np.int32),
+            "masks": masks}
+
+
+def make_invp():
+    """tests/golden/sky_invp.npz: the angular stage (DD, DD inverse-p, DR, DR
+    inverse-p; linear and log theta bins), the 3-D s-mu inverse-p DD and DR
+    that read it back, and the up-weight JKHists::interp at sample values.
+    Every point has a redshift: for points without one (x = 0) the plain
+    angular counts' pixel lookup (vec2pix of a zero vector) is undefined in
+    the reference."""
+    n_jk = 4
+    d = case_sky(41, 1000, n_jk)
+    r = case_sky(42, 2000, n_jk, masks_all_set=True)
+    out = {"n_jk": n_jk, "n_runs": N_RUNS, "theta": np.array(INVP_THETA), "theta_log": np.array(INVP_THETA_LOG),
+           "smu_axes": np.array(INVP_SMU)}
+    for tag, c in (("d", d), ("r", r)):
+        for k, v in c.items():
+            out[f"{tag}_{k}"] = v
+    refl.invp_reset()
+    tmax, nb, base = INVP_THETA
+    p = refl.invp_params(n_jk=n_jk, theta_max=tmax, theta_n_bins=nb, theta_log_base=base, n_bitwise_runs=N_RUNS,
+                         s=(INVP_SMU[0], INVP_SMU[1], INVP_SMU[3], INVP_SMU[2]), mu_n_bins=INVP_SMU[7])
+    files = ("ang_dd.hdf5", "ang_dd_invp.hdf5", "ang_dr.hdf5", "ang_dr_invp.hdf5")
+    for kind in range(4):
+        f, sb = refl.invp_angular(p, kind, d, None if kind < 2 else r, n_jk=n_jk, n_bins=nb)
+        out[f"ang{kind}_full"], out[f"ang{kind}_sub"] = f, sb
+        refl.invp_store_angular(p, files[kind], f, sb)
+    pl = refl.invp_params(n_jk=n_jk, theta_max=INVP_THETA_LOG[0], theta_n_bins=INVP_THETA_LOG[1],
+                          theta_log_base=INVP_THETA_LOG[2], n_bitwise_runs=N_RUNS, dd_file="l0", ddi_file="l1",
+                          dr_file="l2", dri_file="l3")
+    for kind in range(4):
+        f, sb = refl.invp_angular(pl, kind, d, None if kind < 2 else r, n_jk=n_jk, n_bins=INVP_THETA_LOG[1])
+        out[f"anglog{kind}_full"], out[f"anglog{kind}_sub"] = f, sb
+    nb3 = INVP_SMU[3] * INVP_SMU[7]
+    out["dd_invp_full"], out["dd_invp_sub"] = refl.invp_count_3d(p, SMU, 1, d, None, n_jk=n_jk, nb=nb3)
+    out["dr_invp_full"], out["dr_invp_sub"] = refl.invp_count_3d(p, SMU, 0, d, r, n_jk=n_jk, nb=nb3)
+    t = 1.0 - np.cos(tmax)
+    v = np.concatenate([np.linspace(-1e-4, t * 1.05, 4001), np.geomspace(1e-12, t, 1000)])
+    out["up_v"] = v
+    out["up_dd"] = refl.invp_interp(files[0], files[1], v)
+    out["up_dr"] = refl.invp_interp(files[2], files[3], v)
+    np.savez_compressed(os.path.join(HERE, "sky_invp.npz"), **out)
+    return out
+
+
 if __name__ == "__main__":
     if not refl.available("plain"):
         sys.exit("oracle/_ref not built: run oracle/build_ref.sh")
     for nm in CASES:
         o = make(nm)
         print(nm, {k: float(o[k].sum()) for k in ("dd_full", "dr_full", "rr_full")})
+    if refl.available("invp"):
+        o = make_invp()
+        print("sky_invp", {k: float(np.nansum(o[k])) for k in ("ang0_full", "ang1_full", "dd_invp_full",
+                                                                "dr_invp_full")})

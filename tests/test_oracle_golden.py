@@ -13,7 +13,8 @@ import pytest
 
 from oracle import port, refl
 
-GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz")))
+GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
+                if not os.path.basename(p).startswith("sky_"))  # 3-D plain-build fixtures
 W_RTOL = 1e-12
 
 
@@ -124,3 +125,54 @@ def test_axis_restatement_matches_reference_fields():
         rb = refl.axis_bin_num(vmin, vmax, n, base, vals)
         ob = np.array([port.lib().orc_axis_bin_num(C.byref(ax), float(v)) for v in vals], np.float32)
         assert np.array_equal(rb.view(np.uint32), ob.view(np.uint32))
+
+
+INVP = os.path.join(os.path.dirname(__file__), "golden", "sky_invp.npz")
+
+
+def invp_cat(g, tag):
+    return port.Cat(g[f"{tag}_xyz"], unit=g[f"{tag}_unit"], dcom=g[f"{tag}_dcom"], w=g[f"{tag}_w"],
+                    iw=g[f"{tag}_iw"], jk=g[f"{tag}_jk"], masks=g[f"{tag}_masks"])
+
+
+def test_oracle_matches_invp_golden():
+    """Angular stage, up-weight interpolation and 3-D s-mu inverse-p counts of
+    the reference's inverse-p build (tests/golden/make_golden.py)."""
+    g = load(INVP)
+    n_jk, n_runs = int(g["n_jk"]), int(g["n_runs"])
+    d, r = invp_cat(g, "d"), invp_cat(g, "r")
+    for pre, th in (("ang", g["theta"]), ("anglog", g["theta_log"])):
+        for kind in range(4):
+            f, s = port.count_angular(kind, d, None if kind < 2 else r, n_jk=n_jk, theta_max=th[0], n_theta=int(th[1]),
+                                      theta_log_base=th[2], n_runs=n_runs)
+            close(f, g[f"{pre}{kind}_full"], True)  # weighted: non-unit input weights
+            close(s, g[f"{pre}{kind}_sub"], True)
+    th = g["theta"]
+    tmax = 1.0 - np.cos(th[0])
+    up_dd = port.make_upweight(0.0, tmax, int(th[1]), th[2], g["ang0_full"] / g["ang1_full"])
+    up_dr = port.make_upweight(0.0, tmax, int(th[1]), th[2], g["ang2_full"] / g["ang3_full"])
+    L = port.lib()
+    for up, key in ((up_dd, "up_dd"), (up_dr, "up_dr")):
+        got = np.array([L.orc_interp(up, float(x)) for x in g["up_v"]])
+        assert np.array_equal(got, g[key], equal_nan=True)
+    ax = tuple(float(x) for x in g["smu_axes"])
+    ax = (ax[0], ax[1], ax[2], int(ax[3]), ax[4], ax[5], ax[6], int(ax[7]))
+    f, s, _ = port.count_3d(port.S_MU, d, None, is_auto=True, n_jk=n_jk, axes=ax, weight_kind=port.W_INVP_DD,
+                            up=up_dd, n_runs=n_runs)
+    close(f, g["dd_invp_full"], True)
+    close(s, g["dd_invp_sub"], True)
+    f, s, _ = port.count_3d(port.S_MU, d, r, is_auto=False, n_jk=n_jk, axes=ax, weight_kind=port.W_INVP_DR, up=up_dr)
+    close(f, g["dr_invp_full"], True)
+    close(s, g["dr_invp_sub"], True)
+
+
+def test_engine_upweight_matches_invp_golden():
+    """The engine's host-built interpolation tables against the reference's
+    JKHists::interp values stored in the fixture (no GPU needed)."""
+    import two_pcf_b200 as tp
+    g = load(INVP)
+    th = g["theta"]
+    axis = (0.0, 1.0 - np.cos(th[0]), th[2], int(th[1]))
+    for num, den, key in (("ang0_full", "ang1_full", "up_dd"), ("ang2_full", "ang3_full", "up_dr")):
+        w = tp.Weights(tp.WEIGHTS_INVP_DD, int(g["n_runs"]), axis, g[num], g[den])
+        assert np.array_equal(tp.upweight_eval(w, g["up_v"]), g[key], equal_nan=True)

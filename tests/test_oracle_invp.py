@@ -149,3 +149,28 @@ def test_3d_invp_counts_match_reference(mode, theta_base):
                                weight_kind=port.W_INVP_DR, up=up_dr)
     close(of, rf, True)
     close(os_, rs, True)
+
+
+@pytest.mark.parametrize("theta_base", [1.6, 1.0, 1.02, 1.3])
+def test_engine_upweight_tables_match_reference(theta_base):
+    """The engine's host-built interpolation tables (tpcf_upweight_eval, the
+    arithmetic the kernels run) give the reference's JKHists::interp exactly."""
+    import two_pcf_b200 as tp
+    n_jk = 2
+    nb = 25
+    d = sky(7, 1500, n_jk=n_jk)
+    p = refl.invp_params(n_jk=n_jk, theta_max=0.175, theta_n_bins=nb, theta_log_base=theta_base,
+                         n_bitwise_runs=N_RUNS)
+    refl.invp_reset()
+    num_f, num_s = refl.invp_angular(p, 0, d, None, n_jk=n_jk, n_bins=nb)
+    den_f, den_s = refl.invp_angular(p, 1, d, None, n_jk=n_jk, n_bins=nb)
+    refl.invp_store_angular(p, "n.h5", num_f, num_s)
+    refl.invp_store_angular(p, "d.h5", den_f, den_s)
+    tmax = 1.0 - np.cos(0.175)
+    rng = np.random.default_rng(1)
+    v = np.concatenate([np.linspace(-1e-3, tmax * 1.1, 20001), rng.uniform(0, tmax, 20000),
+                        np.geomspace(1e-14, tmax, 5000), [0.0, tmax, -0.0, np.float32(tmax), 2.0, -2.0]])
+    ref = refl.invp_interp("n.h5", "d.h5", v)
+    w = tp.Weights(tp.WEIGHTS_INVP_DD, N_RUNS, (0.0, tmax, theta_base, nb), num_f, den_f)
+    got = tp.upweight_eval(w, v)
+    assert np.array_equal(got, ref, equal_nan=True)

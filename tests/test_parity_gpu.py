@@ -116,3 +116,38 @@ def test_stats_consistent(ctx):
     assert st["in_range"] >= full.sum() / 2
     assert st["candidates"] >= st["in_range"]
     assert st["guard_evals"] < 0.05 * st["in_range"] + 100
+
+
+@pytest.mark.parametrize("precision", [tp.FP32_GUARD, tp.FP64])
+def test_wide_range_and_negative_weights(ctx, precision):
+    """Weights over six decades, some negative (the reference accepts any
+    float weight): the 64-bit shared / 128-bit global fixed-point sums agree
+    with the oracle's double sums to 1e-12 of the bin's absolute weight."""
+    rng = np.random.default_rng(8)
+    n_jk = 5
+    x1 = make_points(31, 3000)
+    x2 = make_points(37, 3600)
+    w1 = (10.0 ** rng.uniform(-3, 3, 3000) * rng.choice([-1.0, 1.0], 3000, p=[0.2, 0.8])).astype(np.float32)
+    w2 = (10.0 ** rng.uniform(-3, 3, 3600)).astype(np.float32)
+    j1 = rng.integers(0, n_jk, 3000).astype(np.int32)
+    j2 = rng.integers(0, n_jk, 3600).astype(np.int32)
+    mode, ax1, ax2 = AXES["s_mu_log"]
+    b = tp.Binning(ctx, mode, ax1, ax2, n_jk)
+    c1 = tp.Catalog(ctx, x1, weight=w1, jk_region=j1, n_jk_regions=n_jk)
+    c2 = tp.Catalog(ctx, x2, weight=w2, jk_region=j2, n_jk_regions=n_jk)
+    a1 = port.Cat(x1, w=np.abs(w1), jk=j1)
+    a2 = port.Cat(x2, w=w2, jk=j2)
+    for is_auto in (True, False):
+        full, sub, _ = tp.count(ctx, c1, None if is_auto else c2, b, precision)
+        of, os_, _ = port.count_3d(mode, port.Cat(x1, w=w1, jk=j1), None if is_auto else port.Cat(x2, w=w2, jk=j2),
+                                   is_auto=is_auto, n_jk=n_jk, axes=oracle_axes(mode, ax1, ax2))
+        af, asub, _ = port.count_3d(mode, a1, None if is_auto else a2, is_auto=is_auto, n_jk=n_jk,
+                                    axes=oracle_axes(mode, ax1, ax2))
+        k = 2.0 if is_auto else 1.0  # the oracle returns the reference's doubled, inverted form
+        ref_full = of / k
+        ref_sub = (of[None, :] - os_) / k
+        scale_full = af / k
+        scale_sub = (af[None, :] + np.abs(af[None, :] - asub)) / k
+        assert np.all(np.abs(full - ref_full) <= 1e-12 * scale_full + 1e-300)
+        assert np.all(np.abs(sub - ref_sub) <= 1e-12 * scale_sub + 1e-300)
+        assert np.abs(ref_full).max() > 0

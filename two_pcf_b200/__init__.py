@@ -27,11 +27,13 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from ._capi import ANGULAR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI, AxisSpec, Stats
+from ._capi import (ANGULAR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR,
+                    WEIGHTS_PLAIN, AxisSpec, Stats, WeightSpec)
 
-__all__ = ["Context", "Catalog", "Binning", "TpcfError", "count", "auto_pair_count", "cross_pair_count",
-           "normalise_auto", "normalise_cross", "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR",
-           "FP32_GUARD", "FP64"]
+__all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "auto_pair_count", "cross_pair_count",
+           "count_weighted", "pair_count_weighted", "upweight_eval", "normalise_auto", "normalise_cross",
+           "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
+           "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR"]
 
 
 class TpcfError(RuntimeError):
@@ -223,3 +225,55 @@ def ls_estimator(dd, dr, rr):
     f = _capi.lib().tpcf_ls_estimator
     out = np.array([f(float(x), float(y), float(z)) for x, y, z in zip(dd.ravel(), dr.ravel(), rr.ravel())])
     return out.reshape(dd.shape)
+
+
+class Weights:
+    """Pair weighting of the inverse-p build (tpcf_weight_spec).
+
+    weighting: WEIGHTS_PLAIN, WEIGHTS_INVP_DD or WEIGHTS_INVP_DR.  For 3-D
+    inverse-p counts, theta_axis = (0, 1 - cos(theta_max), theta_log_base,
+    theta_n_bins) and the angular up-weight is up_numerator / up_denominator
+    bin by bin (the angular DD and DD-inverse-p full histograms for DD, DR and
+    DR-inverse-p for DR)."""
+
+    def __init__(self, weighting: int = WEIGHTS_PLAIN, n_bitwise_runs: int = 0, theta_axis=None,
+                 up_numerator=None, up_denominator=None):
+        self._num = None if up_numerator is None else np.ascontiguousarray(up_numerator, np.float64)
+        self._den = None if up_denominator is None else np.ascontiguousarray(up_denominator, np.float64)
+        ax = _axis(theta_axis) if theta_axis is not None else AxisSpec(0.0, 0.0, 0.0, 0)
+        self.spec = WeightSpec(int(weighting), int(n_bitwise_runs), ax, _ptr(self._num), _ptr(self._den))
+
+
+def count_weighted(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, weights: Weights | None,
+                   precision: int = FP32_GUARD, with_regions: bool = True):
+    """Raw weighted count (tpcf_count_weighted): (full, regions or None, stats)."""
+    full = np.zeros(binning.nb)
+    reg = np.zeros((binning.n_jk, binning.nb)) if with_regions else None
+    st = Stats()
+    rc = _capi.lib().tpcf_count_weighted(ctx._h, a._h, b._h if b is not None else None, binning._h,
+                                         C.byref(weights.spec) if weights is not None else None, int(precision),
+                                         _ptr(full), _ptr(reg), C.byref(st))
+    _check(rc, ctx)
+    return full, reg, st.as_dict()
+
+
+def pair_count_weighted(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, weights: Weights | None,
+                        precision: int = FP32_GUARD):
+    """The *_invpweights / *_angular counting functions (src/correlators_invpweight.cpp): histograms after
+    invert_jk_hists and, for auto counts (b None), multiply_hists(2.0)."""
+    full = np.zeros(binning.nb)
+    sub = np.zeros((binning.n_jk, binning.nb))
+    st = Stats()
+    rc = _capi.lib().tpcf_pair_count_weighted(ctx._h, a._h, b._h if b is not None else None, binning._h,
+                                              C.byref(weights.spec) if weights is not None else None,
+                                              int(precision), _ptr(full), _ptr(sub), C.byref(st))
+    _check(rc, ctx)
+    return full, sub, st.as_dict()
+
+
+def upweight_eval(weights: Weights, values) -> np.ndarray:
+    """The angular up-weight of a 3-D inverse-p spec at values of 1 - cos(theta), as the kernels form it."""
+    v = np.ascontiguousarray(values, np.float64)
+    out = np.empty_like(v)
+    _check(_capi.lib().tpcf_upweight_eval(C.byref(weights.spec), _ptr(v), v.size, _ptr(out)))
+    return out

@@ -36,6 +36,14 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+WEIGHTS_PLAIN, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR = 0, 1, 2
+
+
+class WeightSpec(C.Structure):
+    _fields_ = [("weighting", C.c_int32), ("n_bitwise_runs", C.c_int32), ("theta_axis", AxisSpec),
+                ("up_numerator", C.c_void_p), ("up_denominator", C.c_void_p)]
+
+
 # Every symbol the header declares, with (restype, argtypes).
 _vp = C.c_void_p
 _PROTOTYPES = {
@@ -59,6 +67,11 @@ _PROTOTYPES = {
     "tpcf_binning_thresholds": (C.c_int, [_vp, C.c_int, _vp, C.c_int]),
     "tpcf_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_count_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_count_weighted": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(WeightSpec), C.c_int, _vp, _vp,
+                                      C.POINTER(Stats)]),
+    "tpcf_pair_count_weighted": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(WeightSpec), C.c_int, _vp, _vp,
+                                           C.POINTER(Stats)]),
+    "tpcf_upweight_eval": (C.c_int, [C.POINTER(WeightSpec), _vp, C.c_int64, _vp]),
     "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),

@@ -3,9 +3,12 @@
 // double operation rounds once, as in the reference's x86-64 build.
 #include "axis.h"
 
+#include "engine.h"
+
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <algorithm>
 #include <limits>
 
 namespace tpcf {
@@ -136,6 +139,70 @@ bool check_monotone(const AxisParams &ax, ValueSpace vs, float lo, float hi) {
         prev = cur;
     }
     return true;
+}
+
+namespace {
+
+// Interval of JKHists::interp (src/hist.cpp:369-391) for a float argument x
+// in [min, max]: bin_num = (float)(Axis::bin_num(x) - 0.5); -1 when it is
+// negative, n when it exceeds n - 1, else (int)bin_num.
+int up_category(const AxisParams &ax, float x) {
+    const float bn = (float)((double)axis_bin_num(ax, x) - 0.5);
+    if (bn < 0) return -1;
+    if (bn > ax.n_bins - 1) return ax.n_bins;
+    return (int)bn;
+}
+
+}  // namespace
+
+UpTable make_up_table(const AxisParams &ax, const double *num, const double *den) {
+    UpTable t;
+    t.ax = ax;
+    const int n = ax.n_bins;
+    t.bins.resize(n + 1);
+    t.centre.resize(n + 1);
+    for (int b = 0; b < n; ++b) t.bins[b] = num[b] / den[b];
+    // The reference reads bins[n] when (int)bin_num == n - 1 exactly (one
+    // past its array); the table repeats the last bin there.
+    t.bins[n] = t.bins[n - 1];
+    for (int b = 0; b <= n; ++b) t.centre[b] = axis_bin_centre(ax, b);
+    t.abs_max = 0;
+    for (int b = 0; b < n; ++b)
+        if (std::isfinite(t.bins[b])) t.abs_max = std::max(t.abs_max, std::fabs(t.bins[b]));
+    // Thresholds: thr[k] = smallest float x in [min, max] with category >= k,
+    // +inf when none; the category of x is #{k : thr[k] <= x} - 1.  The
+    // category is non-decreasing in x because bin_num is (check_monotone).
+    t.thr.assign(n + 1, std::numeric_limits<float>::infinity());
+    const float lo = ax.min, hi = ax.max;
+    const uint32_t klo = key_of(lo), khi = key_of(hi);
+    for (int k = 0; k <= n; ++k) {
+        if (up_category(ax, lo) >= k) {
+            t.thr[k] = lo;
+            continue;
+        }
+        if (up_category(ax, hi) < k) continue;
+        uint32_t a = klo, b = khi;
+        while (b - a > 1) {
+            const uint32_t mid = a + (b - a) / 2;
+            if (up_category(ax, float_of(mid)) >= k) b = mid;
+            else a = mid;
+        }
+        t.thr[k] = float_of(b);
+    }
+    return t;
+}
+
+double up_eval(const UpTable &t, double v) {
+    const int n = t.ax.n_bins;
+    if (v < (double)t.ax.min) return t.bins[0];
+    if (v > (double)t.ax.max) return t.bins[n - 1];
+    const float x = (float)v;
+    int c = -1;
+    for (int k = 0; k <= n; ++k)
+        if (t.thr[k] <= x) c = k;
+    if (c < 0) return t.bins[0];
+    if (c >= n) return t.bins[n - 1];
+    return t.bins[c] + (t.bins[c + 1] - t.bins[c]) * (v - t.centre[c]) / (t.centre[c + 1] - t.centre[c]);
 }
 
 }  // namespace tpcf

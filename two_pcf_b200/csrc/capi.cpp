@@ -198,7 +198,7 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
     for (int k = 0; k < c.n_kept; ++k) is_kept[c.h_kept[k]] = 1;
     for (int i = 0; i < N; ++i) {
         const float a = std::fabs(c.h_w[i]);
-        if (is_kept[i]) c.w_max = std::max(c.w_max, a);
+        c.w_max = std::max(c.w_max, a);
         for (int m = 0; m < 3; ++m) {
             const double v = xyz[3 * (size_t)i + m];
             c.lo_all[m] = std::min(c.lo_all[m], v);
@@ -209,9 +209,38 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
             }
         }
     }
+    // Unit vectors: bounding boxes (angular cells) and the largest deviation
+    // of |x_norm|^2 from 1 (a term of the angular error bound).
+    for (int m = 0; m < 3; ++m) {
+        c.ulo_kept[m] = c.ulo_all[m] = 1e300;
+        c.uhi_kept[m] = c.uhi_all[m] = -1e300;
+    }
+    c.norm_dev = 0;
+    for (int i = 0; i < N; ++i) {
+        const double *u = x_norm + 3 * (size_t)i;
+        for (int m = 0; m < 3; ++m) {
+            if (!std::isfinite(u[m]))
+                return fail(ctx, TPCF_E_INVALID_ARG, "non-finite x_norm at index " + std::to_string(i));
+            c.ulo_all[m] = std::min(c.ulo_all[m], u[m]);
+            c.uhi_all[m] = std::max(c.uhi_all[m], u[m]);
+            if (is_kept[i]) {
+                c.ulo_kept[m] = std::min(c.ulo_kept[m], u[m]);
+                c.uhi_kept[m] = std::max(c.uhi_kept[m], u[m]);
+            }
+        }
+        c.norm_dev = std::max(c.norm_dev, std::fabs(u[0] * u[0] + u[1] * u[1] + u[2] * u[2] - 1.0));
+    }
     c.iw_max = c.w_max;
-    if (input_weight)
-        for (int i = 0; i < N; ++i) c.iw_max = std::max(c.iw_max, std::fabs(input_weight[i]));
+    c.iw_unit = c.unit_weights;
+    if (input_weight) {
+        c.iw_max = 0;
+        c.iw_unit = true;
+        for (int i = 0; i < N; ++i) {
+            if (!std::isfinite(input_weight[i])) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite input_weight");
+            c.iw_max = std::max(c.iw_max, std::fabs(input_weight[i]));
+            if (input_weight[i] != 1.0f) c.iw_unit = false;
+        }
+    }
 
     cudaStream_t st = ctx->c.stream;
 #define CAT_TRY(expr)                                            \
@@ -350,35 +379,68 @@ int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int c
     return (int)t.size();
 }
 
-int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
-               int precision, double *full_out, double *region_out, tpcf_stats *stats) {
+}  // extern "C"
+
+namespace {
+
+// Validates a weight spec and builds the request's up-weight table.
+int prepare_weights(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                    const tpcf_weight_spec *spec, tpcf::CountRequest &req, tpcf::UpTable &up) {
+    req.weighting = spec ? spec->weighting : TPCF_WEIGHTS_PLAIN;
+    if (req.weighting < TPCF_WEIGHTS_PLAIN || req.weighting > TPCF_WEIGHTS_INVP_DR)
+        return fail(ctx, TPCF_E_INVALID_ARG, "bad weighting");
+    if (req.weighting == TPCF_WEIGHTS_PLAIN) return TPCF_OK;
+    req.n_runs = spec->n_bitwise_runs;
+    if (req.weighting == TPCF_WEIGHTS_INVP_DD) {
+        const tpcf::Catalog &ca = a->c, &cb = b ? b->c : a->c;
+        if (ca.n_mask < 1 || ca.n_mask != cb.n_mask)
+            return fail(ctx, TPCF_E_INVALID_ARG, "inverse-p DD weights need bitmasks of one width on both catalogues");
+    }
+    if (bin->b.mode != TPCF_ANGULAR) {
+        const tpcf_axis_spec &t = spec->theta_axis;
+        if (!spec->up_numerator || !spec->up_denominator || t.n_bins < 1 || t.n_bins > tpcf::kMaxBins1D ||
+            !std::isfinite(t.min) || !std::isfinite(t.max) || !(t.max > t.min))
+            return fail(ctx, TPCF_E_INVALID_ARG, "3-D inverse-p counts need the angular up-weight histograms and axis");
+        up = tpcf::make_up_table(tpcf::make_axis(t.min, t.max, t.n_bins, t.log_base), spec->up_numerator,
+                                 spec->up_denominator);
+        req.up = &up;
+    }
+    return TPCF_OK;
+}
+
+int count_impl(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+               const tpcf_weight_spec *spec, int precision, double *full_out, double *region_out, tpcf_stats *stats,
+               bool noalloc) {
     if (!ctx || !a || !bin || !full_out) return TPCF_E_INVALID_ARG;
     if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
-    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "angular binning: use the angular counter");
     if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
         return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
+    tpcf::CountRequest req;
+    tpcf::UpTable up;
+    int rc = prepare_weights(ctx, a, b, bin, spec, req, up);
+    if (rc) return rc;
     cudaError_t e = cudaSetDevice(ctx->c.device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
     auto t0 = std::chrono::steady_clock::now();
-    tpcf::CountRequest req;
     req.a = &a->c;
     req.b = b ? &b->c : nullptr;
     req.bin = &bin->b;
     req.exact_fp64 = precision == TPCF_FP64;
+    const int nb = bin->b.nb;
+    // Points a count uses: every point for plain angular counts, the d_comov
+    // partition otherwise.
+    const bool all_points = bin->b.mode == TPCF_ANGULAR && req.weighting == TPCF_WEIGHTS_PLAIN;
+    auto used = [&](const tpcf_catalog *c) { return all_points ? c->c.n_all : (int64_t)c->c.n_kept; };
+    if (used(a) == 0 || (b && used(b) == 0)) {
+        std::memset(full_out, 0, sizeof(double) * nb);
+        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
+        if (stats) std::memset(stats, 0, sizeof(*stats));
+        return TPCF_OK;
+    }
     tpcf::Stats st;
     tpcf::Error err{0, ""};
-    const int nb = bin->b.nb;
-    if ((b ? b->c.n_kept : 0) == 0 && b) {
-        std::memset(full_out, 0, sizeof(double) * nb);
-        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
-        return TPCF_OK;
-    }
-    if (a->c.n_kept == 0) {
-        std::memset(full_out, 0, sizeof(double) * nb);
-        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
-        return TPCF_OK;
-    }
-    int rc = tpcf::run_count(&ctx->c, req, full_out, region_out, &st, &err);
+    rc = noalloc ? tpcf::run_count_static(&ctx->c, req, full_out, region_out, &st, &err)
+                 : tpcf::run_count(&ctx->c, req, full_out, region_out, &st, &err);
     if (rc) return fail(ctx, rc, err.msg);
     if (stats) {
         stats->candidates = st.candidates;
@@ -392,48 +454,10 @@ int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, cons
     return TPCF_OK;
 }
 
-int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
-                       int precision, double *full_out, double *region_out, tpcf_stats *stats) {
-    if (!ctx || !a || !bin || !full_out) return TPCF_E_INVALID_ARG;
-    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
-    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "angular binning: use the angular counter");
-    if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
-        return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
-    cudaError_t e = cudaSetDevice(ctx->c.device);
-    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
-    auto t0 = std::chrono::steady_clock::now();
-    const int nb = bin->b.nb;
-    if (a->c.n_kept == 0 || (b && b->c.n_kept == 0)) {
-        std::memset(full_out, 0, sizeof(double) * nb);
-        if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
-        if (stats) std::memset(stats, 0, sizeof(*stats));
-        return TPCF_OK;
-    }
-    tpcf::CountRequest req;
-    req.a = &a->c;
-    req.b = b ? &b->c : nullptr;
-    req.bin = &bin->b;
-    req.exact_fp64 = precision == TPCF_FP64;
-    tpcf::Stats st;
-    tpcf::Error err{0, ""};
-    int rc = tpcf::run_count_static(&ctx->c, req, full_out, region_out, &st, &err);
-    if (rc) return fail(ctx, rc, err.msg);
-    if (stats) {
-        stats->candidates = st.candidates;
-        stats->in_range = st.in_range;
-        stats->guard_evals = st.guard;
-        stats->overflow_updates = st.overflow;
-        stats->work_items = st.items;
-        stats->ms_kernel = 0.0;
-        stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
-    }
-    return TPCF_OK;
-}
-
-static int reference_form(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
-                          int precision, double *full, double *sub, tpcf_stats *stats) {
+int reference_form(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                   const tpcf_weight_spec *spec, int precision, double *full, double *sub, tpcf_stats *stats) {
     if (!sub) return fail(ctx, TPCF_E_INVALID_ARG, "sub_hist is NULL");
-    int rc = tpcf_count(ctx, a, b, bin, precision, full, sub, stats);
+    int rc = count_impl(ctx, a, b, bin, spec, precision, full, sub, stats, false);
     if (rc) return rc;
     const int nb = bin->b.nb, nj = bin->b.n_jk;
     // invert_jk_hists (src/hist.cpp:270-277, :464-471)
@@ -447,15 +471,53 @@ static int reference_form(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catal
     return TPCF_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+               int precision, double *full_out, double *region_out, tpcf_stats *stats) {
+    return count_impl(ctx, a, b, bin, nullptr, precision, full_out, region_out, stats, false);
+}
+
+int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                       int precision, double *full_out, double *region_out, tpcf_stats *stats) {
+    return count_impl(ctx, a, b, bin, nullptr, precision, full_out, region_out, stats, true);
+}
+
+int tpcf_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                        const tpcf_weight_spec *spec, int precision, double *full_out, double *region_out,
+                        tpcf_stats *stats) {
+    return count_impl(ctx, a, b, bin, spec, precision, full_out, region_out, stats, false);
+}
+
+int tpcf_pair_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                             const tpcf_weight_spec *spec, int precision, double *full_hist, double *sub_hist,
+                             tpcf_stats *stats) {
+    return reference_form(ctx, a, b, bin, spec, precision, full_hist, sub_hist, stats);
+}
+
+int tpcf_upweight_eval(const tpcf_weight_spec *spec, const double *values, int64_t n, double *out) {
+    if (!spec || !spec->up_numerator || !spec->up_denominator || n < 0 || (n > 0 && (!values || !out)))
+        return TPCF_E_INVALID_ARG;
+    const tpcf_axis_spec &t = spec->theta_axis;
+    if (t.n_bins < 1 || t.n_bins > tpcf::kMaxBins1D || !(t.max > t.min)) return TPCF_E_INVALID_ARG;
+    const tpcf::UpTable up =
+        tpcf::make_up_table(tpcf::make_axis(t.min, t.max, t.n_bins, t.log_base), spec->up_numerator,
+                            spec->up_denominator);
+    for (int64_t i = 0; i < n; ++i) out[i] = tpcf::up_eval(up, values[i]);
+    return TPCF_OK;
+}
+
 int tpcf_auto_pair_count(tpcf_ctx *ctx, const tpcf_catalog *cat, const tpcf_binning *bin, int precision,
                          double *full_hist, double *sub_hist, tpcf_stats *stats) {
-    return reference_form(ctx, cat, nullptr, bin, precision, full_hist, sub_hist, stats);
+    return reference_form(ctx, cat, nullptr, bin, nullptr, precision, full_hist, sub_hist, stats);
 }
 
 int tpcf_cross_pair_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                           int precision, double *full_hist, double *sub_hist, tpcf_stats *stats) {
     if (!b) return TPCF_E_INVALID_ARG;
-    return reference_form(ctx, a, b, bin, precision, full_hist, sub_hist, stats);
+    return reference_form(ctx, a, b, bin, nullptr, precision, full_hist, sub_hist, stats);
 }
 
 int tpcf_normalise_auto(const tpcf_catalog *cat, int32_t nb, double *full, double *sub) {

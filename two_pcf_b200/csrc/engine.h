@@ -47,6 +47,8 @@ struct Error {
 // jackknife region.  Replaces GalaxyBoxes (src/boxes.cpp:10-163).
 struct Grid {
     double side = 0;
+    bool angular = false;  // cells over the unit vectors instead of the positions
+    bool input_w = false;  // the weight slot holds input_weight instead of weight
     int kmin[3] = {0, 0, 0};
     int dim[3] = {1, 1, 1};
     bool morton = false;  // dense cell id = Morton code of the local cell coords
@@ -81,6 +83,9 @@ struct Catalog {
     bool unit_weights = true;  // every weight == 1.0f
     float w_min = 1, w_max = 1, iw_min = 1, iw_max = 1;
     double lo_kept[3], hi_kept[3], lo_all[3], hi_all[3];
+    double ulo_kept[3], uhi_kept[3], ulo_all[3], uhi_all[3];  // bounding boxes of the unit vectors
+    double norm_dev = 0;          // max | x_norm . x_norm - 1 |
+    bool iw_unit = true;          // every input weight == 1.0f
     DevBuf<double> xyz, unit;
     DevBuf<float> w, iw;
     DevBuf<int> jk;
@@ -120,18 +125,51 @@ struct Ctx {
 };
 
 // grid.cu
-int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_fp64, Grid **out, Error *err);
+// Which grid of a catalogue: cell side, the point subset (the d_comov
+// partition or every point), the coordinates it is built on and the weight
+// it carries.
+struct GridSpec {
+    double side = 0;
+    bool subset_kept = true;
+    bool angular = false;
+    bool input_w = false;
+};
+int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Grid **out, Error *err);
 // The grid build_grid would return when it is already cached, else nullptr;
 // never allocates.
-Grid *find_grid(Catalog *cat, double side, bool subset_kept, bool want_fp64);
+Grid *find_grid(Catalog *cat, const GridSpec &spec, bool want_fp64);
 
 // pair_count.cu
+// Angular up-weight of the 3-D inverse-p counts: JKHists::interp
+// (src/hist.cpp:369-391) of the ratio of two angular histograms.
+struct UpTable {
+    AxisParams ax;
+    std::vector<double> bins;    // n + 1: the ratio per bin, plus a spare copy of the last
+    std::vector<double> centre;  // n + 1: Axis::bin_centre(b), host libm exp
+    std::vector<float> thr;      // n + 1: interpolation-interval thresholds (see make_up_table)
+    double abs_max = 0;          // largest finite |ratio|
+};
+// Builds the table from numerator and denominator histograms
+// (JKHists::divide_by_hist, src/hist.cpp:224-231).
+UpTable make_up_table(const AxisParams &ax, const double *num, const double *den);
+// The interpolation exactly as the kernels evaluate it.
+double up_eval(const UpTable &t, double v);
+
+// Pair weighting of a count (reference build and function in brackets).
+enum Weighting {
+    WEIGHTS_PLAIN = 0,    // w1 * w2 [3-D]; input_weight products [angular DD / DR]
+    WEIGHTS_INVP_DD = 1,  // inverse-p popcount weights [*_invpweights DD]
+    WEIGHTS_INVP_DR = 2,  // angular DR up-weight [3-D DR]; w1 * w2 [angular DR inverse-p]
+};
+
 struct CountRequest {
     const Catalog *a = nullptr;
     const Catalog *b = nullptr;  // nullptr: auto count of a
     const Binning *bin = nullptr;
     bool exact_fp64 = false;     // plain FP64 path for every candidate
-    int weight_kind = W_PLAIN;
+    int weighting = WEIGHTS_PLAIN;
+    const UpTable *up = nullptr; // 3-D inverse-p counts
+    int n_runs = 0;              // Params::n_bitwise_runs
     int refinement = 0;
 };
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);

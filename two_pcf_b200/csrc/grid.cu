@@ -12,6 +12,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <string>
 
 #include "engine.h"
 
@@ -234,28 +235,45 @@ __global__ void regions_kernel(GeomDev g, int ncell, const int *__restrict__ bst
         }                                                                                \
     } while (0)
 
-Grid *find_grid(Catalog *cat, double side, bool subset_kept, bool want_fp64) {
-    char key[96];
-    snprintf(key, sizeof(key), "%a|%d", side, subset_kept ? 1 : 0);
-    auto it = cat->grids.find(key);
+namespace {
+std::string grid_key(const GridSpec &spec) {
+    char key[128];
+    snprintf(key, sizeof(key), "%a|%d|%d|%d", spec.side, spec.subset_kept ? 1 : 0, spec.angular ? 1 : 0,
+             spec.input_w ? 1 : 0);
+    return key;
+}
+}  // namespace
+
+Grid *find_grid(Catalog *cat, const GridSpec &spec, bool want_fp64) {
+    auto it = cat->grids.find(grid_key(spec));
     if (it == cat->grids.end() || (want_fp64 && !it->second->has_fp64)) return nullptr;
     return it->second.get();
 }
 
-int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_fp64, Grid **out, Error *err) {
-    char key[96];
-    snprintf(key, sizeof(key), "%a|%d", side, subset_kept ? 1 : 0);
+int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Grid **out, Error *err) {
+    const std::string key = grid_key(spec);
     auto it = cat->grids.find(key);
     if (it != cat->grids.end() && (!want_fp64 || it->second->has_fp64)) {
         *out = it->second.get();
         return 0;
     }
+    const double side = spec.side;
+    const bool subset_kept = spec.subset_kept;
     cudaStream_t st = ctx->stream;
     std::unique_ptr<Grid> g(new Grid());
     g->side = side;
     g->subset_kept = subset_kept;
-    const double *lo = subset_kept ? cat->lo_kept : cat->lo_all;
-    const double *hi = subset_kept ? cat->hi_kept : cat->hi_all;
+    g->angular = spec.angular;
+    g->input_w = spec.input_w;
+    const double *lo = spec.angular ? (subset_kept ? cat->ulo_kept : cat->ulo_all)
+                                    : (subset_kept ? cat->lo_kept : cat->lo_all);
+    const double *hi = spec.angular ? (subset_kept ? cat->uhi_kept : cat->uhi_all)
+                                    : (subset_kept ? cat->hi_kept : cat->hi_all);
+    // Coordinates the cells are built on, and the weight each point carries.
+    const double *coords = spec.angular ? cat->unit.p : cat->xyz.p;
+    const float *wsrc = nullptr;
+    if (spec.input_w) wsrc = cat->iw.p ? cat->iw.p : (cat->unit_weights ? nullptr : cat->w.p);
+    else wsrc = cat->unit_weights ? nullptr : cat->w.p;
     int n = subset_kept ? cat->n_kept : (int)cat->n_all;
     g->n = n;
     int maxdim = 1;
@@ -306,7 +324,7 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
     const int *subset = subset_kept ? cat->kept.p : nullptr;
     const int *jk = cat->n_jk > 1 ? cat->jk.p : nullptr;
     if (n > 0) {
-        assign_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, cat->xyz.p, jk, subset, n, bucket.p, counts.p);
+        assign_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, coords, jk, subset, n, bucket.p, counts.p);
         ++ctx->launches;
         TPCF_CUDA_TRY(cudaGetLastError());
     }
@@ -316,7 +334,7 @@ int build_grid(Ctx *ctx, Catalog *cat, double side, bool subset_kept, bool want_
     TPCF_CUDA_TRY(fill.alloc(nbucket));
     TPCF_CUDA_TRY(cudaMemsetAsync(fill.p, 0, sizeof(int) * nbucket, st));
     if (n > 0) {
-        scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, cat->xyz.p, cat->unit.p, cat->unit_weights ? nullptr : cat->w.p,
+        scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, coords, cat->unit.p, wsrc,
                                                         jk, subset, n, bucket.p, counts.p, fill.p, g->pos.p,
                                                         g->aux.p, g->idx.p, want_fp64 ? g->xyz_s.p : nullptr,
                                                         want_fp64 ? g->unit_s.p : nullptr);

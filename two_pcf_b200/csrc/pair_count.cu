@@ -78,11 +78,22 @@ struct KParams {
     const unsigned char *lut1g, *lut2g;
     unsigned lut1_base;  // (bits of the lowest bucket) >> (23 - LUT1_BITS)
     float lut2_scale;    // bucket = (int)(value * lut2_scale)
-    unsigned long long *g_full, *g_sub;
+    unsigned long long *g_full, *g_sub;  // 128-bit fixed-point sums (low, high word pairs)
     int n_jk;
     float wscale;
     unsigned long long *counters;  // candidates, in_range, guard, flushes
     int *err;
+    // inverse-p weights and the angular up-weight
+    const long long *a_masks, *b_masks;  // original catalogue bitmasks, object-major
+    int n_mask;
+    float n_runs_f;
+    double n_runs_d;
+    const float *up_thr;                 // n_up + 1 interval thresholds
+    const double *up_bins, *up_centre;   // n_up + 1 each
+    int n_up;
+    double up_min, up_max;
+    float g_ang;       // error bound of the FP32 1 - cos(theta)
+    unsigned *flags;   // (1 + n_jk) * nb: non-finite weights met per bin (1 NaN, 2 +inf, 4 -inf)
 };
 
 struct SmemLayout {
@@ -171,9 +182,27 @@ __device__ __forceinline__ int exact_bin(const ExactArgs &E, const float *t1, co
 }
 
 // Guard-band re-evaluation from the original double arrays.
+// 1 - cos(theta) of two unit vectors with the reference's sequence
+// (src/correlators_invpweight.cpp:51-54, :738-741): ((1 - a0 b0) - a1 b1) -
+// a2 b2 in double, each product and difference rounded once.
+__device__ __forceinline__ double omct_exact(double a0, double a1, double a2, double b0, double b1, double b2) {
+    double v = __dsub_rn(1.0, __dmul_rn(a0, b0));
+    v = __dsub_rn(v, __dmul_rn(a1, b1));
+    return __dsub_rn(v, __dmul_rn(a2, b2));
+}
+
 template <int MODE>
 __device__ __forceinline__ int exact_pair(const ExactArgs E, const float *t1, const float *t2, int ia, int jb,
                                        bool *in_range) {
+    if (MODE == MODE_ANGULAR) {
+        // The angular histogram takes (float)(1 - cos(theta)) with no range
+        // test (JKHists::add_pair's float value, src/hist.cpp:246).
+        const double *u1 = E.a_unit + 3 * (size_t)ia, *u2 = E.b_unit + 3 * (size_t)jb;
+        const float v = __double2float_rn(omct_exact(u1[0], u1[1], u1[2], u2[0], u2[1], u2[2]));
+        const int b = dev::locate_exact(t1, E.n1, v);
+        *in_range = b >= 0 && b < E.n1;
+        return *in_range ? b : -1;
+    }
     const double *x1 = E.a_xyz + 3 * (size_t)ia, *x2 = E.b_xyz + 3 * (size_t)jb;
     float d0 = __double2float_rn(__dsub_rn(x1[0], x2[0]));
     float d1 = __double2float_rn(__dsub_rn(x1[1], x2[1]));
@@ -263,88 +292,187 @@ struct Counters {
     unsigned in_range = 0, guard = 0;  // per thread, folded into 64-bit totals per item
 };
 
-// Bin one pair that passed the guard-widened range test, from its FP32 s^2,
-// pi and weight.  ia/jb are the pair's positions in the sorted grids (the
-// exact path follows them back to the original arrays).
-template <int MODE, bool UNITW>
-__device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
-                                         const float *s_t1, const float *s_t2, const unsigned char *s_l1,
-                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi, float s2,
-                                         float pi, float w, int ia, int jb, Counters &cnt) {
-    int bin;
-    bool amb;
-    if (MODE == MODE_SIGMA_PI) {
-        if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return;  // certainly out of range
-        amb = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
-        const float a = fmaf(-pi, pi, s2);
-        unsigned c1 = (a <= P.g_a) ? LUT_AMB : s_l1[lut1_index(P.lut1_base, a)];
-        if (a < -P.g_a) c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
-        const unsigned c2 = s_l2[lut2_index(P.lut2_scale, fabsf(pi))];
-        if (!amb && (c1 == LUT_INV || c2 == LUT_INV)) {
-            cnt.in_range += 1;
+// JKHists::interp (src/hist.cpp:369-391) of the angular up-weight at
+// v = 1 - cos(theta): the interval comes from the host-built thresholds on
+// (float)v (the reference's bin_num runs on glibc log1pf), the
+// interpolation is the reference's double expression.
+__device__ __forceinline__ double upweight(const KParams &P, double v) {
+    if (v < P.up_min) return __ldg(P.up_bins);
+    if (v > P.up_max) return __ldg(P.up_bins + P.n_up - 1);
+    const int c = dev::locate_exact(P.up_thr, P.n_up, __double2float_rn(v));
+    if (c < 0) return __ldg(P.up_bins);
+    if (c >= P.n_up) return __ldg(P.up_bins + P.n_up - 1);
+    const double b0 = __ldg(P.up_bins + c), b1 = __ldg(P.up_bins + c + 1);
+    const double c0 = __ldg(P.up_centre + c), c1 = __ldg(P.up_centre + c + 1);
+    return __dadd_rn(b0, __ddiv_rn(__dmul_rn(__dsub_rn(b1, b0), __dsub_rn(v, c0)), __dsub_rn(c1, c0)));
+}
+
+// Pair weight of the inverse-p kinds from the product of the two grid
+// weights (input weights for W_INVP_DD / W_ANG_INVP, weights for
+// W_INVP_DR) and the original indices i (catalogue A), j (catalogue B):
+//   W_INVP_DD  (iw1 iw2) (float)(interp(1-cos) n_runs / popc)
+//              (src/correlators_invpweight.cpp:51-77)
+//   W_INVP_DR  (float)((w1 w2) interp(1-cos))         (:184-189)
+//   W_ANG_INVP (iw1 iw2) (n_runs / popc), float division (:742-764)
+// popc = float sum of the popcounts of mask1 & mask2, plus 1 when zero.
+template <int WK>
+__device__ __forceinline__ float pair_weight(const KParams &P, float wprod, int i, int j) {
+    auto omct = [&]() {
+        const double *u1 = P.a.unit + 3 * (size_t)i, *u2 = P.b.unit + 3 * (size_t)j;
+        return omct_exact(u1[0], u1[1], u1[2], u2[0], u2[1], u2[2]);
+    };
+    if (WK == W_INVP_DR) return __double2float_rn(__dmul_rn((double)wprod, upweight(P, omct())));
+    const long long *m1 = P.a_masks + (size_t)i * P.n_mask;
+    const long long *m2 = P.b_masks + (size_t)j * P.n_mask;
+    int c = 0;
+    for (int k = 0; k < P.n_mask; ++k) c += __popcll((unsigned long long)(__ldg(m1 + k) & __ldg(m2 + k)));
+    float pw = (float)c;  // exact: at most 64 * kMaxMaskInts
+    if (pw < 0.5f) pw += 1.0f;
+    if (WK == W_ANG_INVP) return __fmul_rn(wprod, __fdiv_rn(P.n_runs_f, pw));
+    const float f = __double2float_rn(__ddiv_rn(__dmul_rn(upweight(P, omct()), P.n_runs_d), (double)pw));
+    return __fmul_rn(wprod, f);
+}
+
+// A non-finite pair weight (an up-weight from an empty angular bin) cannot
+// go into the fixed-point sums: record it for the bin in the full histogram
+// and in the rows of both regions; the host turns the flags into the NaN or
+// infinity that double accumulation gives.
+__device__ __noinline__ void flag_nonfinite(const KParams &P, int bin, int ra, int rb, float w) {
+    const unsigned f = isnan(w) ? 1u : (w > 0 ? 2u : 4u);
+    atomicOr(&P.flags[bin], f);
+    atomicOr(&P.flags[(size_t)(1 + ra) * P.nb + bin], f);
+    if (rb != ra) atomicOr(&P.flags[(size_t)(1 + rb) * P.nb + bin], f);
+}
+
+// Add one binned pair: weight from the queue (product of the grid weights)
+// or, for the inverse-p kinds, formed here; fixed-point shared add.
+template <bool UNITW, int WK>
+__device__ __forceinline__ void add_binned(const KParams &P, uint32_t *s_lo, uint32_t *s_hi, int bin, float w,
+                                           int ia, int jb, int ra, int rb) {
+    if (WK != W_PLAIN) {
+        w = pair_weight<WK>(P, w, P.a.idx[ia], P.b.idx[jb]);
+        if (!isfinite(w)) {
+            flag_nonfinite(P, bin, ra, rb, w);
             return;
         }
-        amb = amb || c1 >= LUT_INV || c2 >= LUT_INV;
-        if (!amb) cnt.in_range += 1;
-        bin = (int)(c1 * P.n2 + c2);
-    } else {
-        const unsigned c1 = s_l1[lut1_index(P.lut1_base, s2)];
-        if (c1 == LUT_INV) {
-            // certainly outside the range or the bins; the range status is
-            // the same for every value of the widened bucket
-            cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
-            return;
-        }
-        amb = (c1 == LUT_AMB);
-        unsigned c2 = 0;
-        if (MODE == MODE_S_MU) {
-            const float mu = fabsf(pi) * rsqrtf(s2);
-            c2 = s_l2[lut2_index(P.lut2_scale, mu)];
-            if (c2 == LUT_INV && !amb && s2 >= P.s2_lut_min) {
-                cnt.in_range += 1;
-                return;
-            }
-            amb = amb || c2 >= LUT_INV || s2 < P.s2_lut_min;
-        }
-        if (!amb) cnt.in_range += 1;
-        bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
     }
-    if (amb) {
-        bool inr, guarded;
-        bin = precise_bin<MODE>(PA, E, s_t1, s_t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
-        cnt.in_range += inr ? 1 : 0;
-        cnt.guard += guarded ? 1 : 0;
-        if (bin < 0) return;
-    }
-    const long long q = UNITW ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
+    const long long q = (UNITW && WK == W_PLAIN) ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
     dev::acc_add(s_lo, s_hi, bin, q);
 }
 
-// Bin one pair of the plain FP64 path from its exact separation (d0, d1,
-// d2); ia/jb are its positions in the sorted grids.
-template <int MODE, bool UNITW>
+// Bin one pair that passed the guard-widened range test, from its FP32 s^2
+// (the squared chord for angular counts), pi and grid-weight product.
+// ia/jb are the pair's positions in the sorted grids (the exact path follows
+// them back to the original arrays); ra/rb the regions of its two points.
+template <int MODE, bool UNITW, int WK>
+__device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
+                                         const float *s_t1, const float *s_t2, const unsigned char *s_l1,
+                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi, float s2,
+                                         float pi, float w, int ia, int jb, int ra, int rb, Counters &cnt) {
+    int bin;
+    bool amb;
+    if constexpr (MODE == MODE_ANGULAR) {
+        // v = |n1 - n2|^2 / 2 approximates 1 - cos(theta) within g_ang
+        const float v = 0.5f * s2;
+        const unsigned c1 = s_l1[lut1_index(P.lut1_base, v)];
+        if (c1 == LUT_INV) return;
+        if (c1 != LUT_AMB) {
+            cnt.in_range += 1;
+            bin = (int)c1;
+        } else {
+            const dev::AxisK ax1{s_t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
+            int b = dev::locate_exact(s_t1, P.n1, v);
+            bool inr;
+            if (dev::near_edge(ax1, v, b, P.g_ang)) {
+                cnt.guard += 1;
+                b = exact_pair<MODE_ANGULAR>(E, s_t1, s_t2, P.a.idx[ia], P.b.idx[jb], &inr);
+            } else {
+                inr = b >= 0 && b < P.n1;
+            }
+            cnt.in_range += inr ? 1 : 0;
+            if (!inr) return;
+            bin = b;
+        }
+        add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
+        return;
+    } else {
+        if (MODE == MODE_SIGMA_PI) {
+            if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return;  // certainly out of range
+            amb = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
+            const float a = fmaf(-pi, pi, s2);
+            unsigned c1 = (a <= P.g_a) ? LUT_AMB : s_l1[lut1_index(P.lut1_base, a)];
+            if (a < -P.g_a) c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
+            const unsigned c2 = s_l2[lut2_index(P.lut2_scale, fabsf(pi))];
+            if (!amb && (c1 == LUT_INV || c2 == LUT_INV)) {
+                cnt.in_range += 1;
+                return;
+            }
+            amb = amb || c1 >= LUT_INV || c2 >= LUT_INV;
+            if (!amb) cnt.in_range += 1;
+            bin = (int)(c1 * P.n2 + c2);
+        } else {
+            const unsigned c1 = s_l1[lut1_index(P.lut1_base, s2)];
+            if (c1 == LUT_INV) {
+                // certainly outside the range or the bins; the range status is
+                // the same for every value of the widened bucket
+                cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
+                return;
+            }
+            amb = (c1 == LUT_AMB);
+            unsigned c2 = 0;
+            if (MODE == MODE_S_MU) {
+                const float mu = fabsf(pi) * rsqrtf(s2);
+                c2 = s_l2[lut2_index(P.lut2_scale, mu)];
+                if (c2 == LUT_INV && !amb && s2 >= P.s2_lut_min) {
+                    cnt.in_range += 1;
+                    return;
+                }
+                amb = amb || c2 >= LUT_INV || s2 < P.s2_lut_min;
+            }
+            if (!amb) cnt.in_range += 1;
+            bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
+        }
+        if (amb) {
+            bool inr, guarded;
+            bin = precise_bin<MODE>(PA, E, s_t1, s_t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
+            cnt.in_range += inr ? 1 : 0;
+            cnt.guard += guarded ? 1 : 0;
+            if (bin < 0) return;
+        }
+        add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
+    }
+}
+
+// Bin one pair of the plain FP64 path: from its exact separation (d0, d1,
+// d2), or for angular counts from its exact (float)(1 - cos(theta)) in d0;
+// ia/jb are its positions in the sorted grids.
+template <int MODE, bool UNITW, int WK>
 __device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, const float *s_t1, const float *s_t2,
                                           uint32_t *s_lo, uint32_t *s_hi, float d0, float d1, float d2, int ia,
-                                          int jb, Counters &cnt) {
-    double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
-    if (MODE != MODE_MONOPOLE) {
-        const double4 u1 = P.a.unit_s[ia];
-        const double4 u2 = P.b.unit_s[jb];
-        n1x = u1.x;
-        n1y = u1.y;
-        n1z = u1.z;
-        n2x = u2.x;
-        n2y = u2.y;
-        n2z = u2.z;
+                                          int jb, int ra, int rb, Counters &cnt) {
+    int bin;
+    if constexpr (MODE == MODE_ANGULAR) {
+        bin = dev::locate_exact(s_t1, P.n1, d0);  // in [0, n1): the candidate test checked it
+        cnt.in_range += 1;
+    } else {
+        double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
+        if (MODE != MODE_MONOPOLE) {
+            const double4 u1 = P.a.unit_s[ia];
+            const double4 u2 = P.b.unit_s[jb];
+            n1x = u1.x;
+            n1y = u1.y;
+            n1z = u1.z;
+            n2x = u2.x;
+            n2y = u2.y;
+            n2z = u2.z;
+        }
+        bool inr;
+        bin = exact_bin<MODE>(E, s_t1, s_t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
+        cnt.in_range += inr ? 1 : 0;
+        if (bin < 0) return;
     }
-    bool inr;
-    const int bin = exact_bin<MODE>(E, s_t1, s_t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
-    cnt.in_range += inr ? 1 : 0;
-    if (bin < 0) return;
-    const long long q =
-        UNITW ? 1LL
-              : __float2ll_rn(__fmul_rn(__fmul_rn((float)P.a.xyz_s[ia].w, (float)P.b.xyz_s[jb].w), P.wscale));
-    dev::acc_add(s_lo, s_hi, bin, q);
+    const float w = UNITW ? 1.0f : __fmul_rn((float)P.a.xyz_s[ia].w, (float)P.b.xyz_s[jb].w);
+    add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
 }
 
 // Add a 64-bit value held as two 32-bit words into another such pair (the
@@ -356,10 +484,10 @@ __device__ __forceinline__ void add64_owned(uint32_t *lo, uint32_t *hi, int i, u
     hi[i] = hi[i] + vh + ((old + vl) < old ? 1u : 0u);
 }
 
-template <int MODE, bool UNITW, bool JK, bool EXACT>
+template <int MODE, bool UNITW, bool JK, bool EXACT, int WK>
 __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
-    constexpr bool kNeedAux = (MODE != MODE_MONOPOLE);
+    constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
     const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
@@ -529,12 +657,19 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         bool hit[R];
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
-                            d0[r] = __double2float_rn(__dsub_rn(dax[r], pb.x));
-                            d1[r] = __double2float_rn(__dsub_rn(day[r], pb.y));
-                            d2[r] = __double2float_rn(__dsub_rn(daz[r], pb.z));
-                            const float s2 = __fadd_rn(__fadd_rn(__fmul_rn(d0[r], d0[r]), __fmul_rn(d1[r], d1[r])),
-                                                       __fmul_rn(d2[r], d2[r]));
-                            hit[r] = jv && (s2 < P.max_r_sq) && (s2 > P.min_r_sq) && (!self || jg > ai[r]);
+                            if (MODE == MODE_ANGULAR) {
+                                // tiles hold unit vectors: the binned value itself
+                                d0[r] = __double2float_rn(omct_exact(dax[r], day[r], daz[r], pb.x, pb.y, pb.z));
+                                d1[r] = d2[r] = 0.0f;
+                                hit[r] = jv && (d0[r] >= s_t1[0]) && (d0[r] < s_t1[P.n1]) && (!self || jg > ai[r]);
+                            } else {
+                                d0[r] = __double2float_rn(__dsub_rn(dax[r], pb.x));
+                                d1[r] = __double2float_rn(__dsub_rn(day[r], pb.y));
+                                d2[r] = __double2float_rn(__dsub_rn(daz[r], pb.z));
+                                const float s2 = __fadd_rn(
+                                    __fadd_rn(__fmul_rn(d0[r], d0[r]), __fmul_rn(d1[r], d1[r])), __fmul_rn(d2[r], d2[r]));
+                                hit[r] = jv && (s2 < P.max_r_sq) && (s2 > P.min_r_sq) && (!self || jg > ai[r]);
+                            }
                         }
 #pragma unroll
                         for (int r = 0; r < R; ++r) {
@@ -548,8 +683,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                             __syncwarp();
                             const float4 e = s_q[qn - 32 + lane];
                             const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
-                                                   it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
+                                                       it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region, rb,
+                                                       cnt);
                             __syncwarp();
                             qn -= 32;
                         }
@@ -559,8 +695,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         if (lane < qn) {
                             const float4 e = s_q[lane];
                             const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
-                                                   it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
+                                                       it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region, rb,
+                                                       cnt);
                         }
                         __syncwarp();
                     }
@@ -603,8 +740,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                             __syncwarp();
                             const float4 e = s_q[qn - 32 + lane];
                             const int pk = __float_as_int(e.w);
-                            bin_fast<MODE, UNITW>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y, e.z,
-                                                  it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y,
+                                                      e.z, it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
+                                                      rb, cnt);
                             __syncwarp();
                             qn -= 32;
                         }
@@ -615,8 +753,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         if (lane < qn) {
                             const float4 e = s_q[lane];
                             const int pk = __float_as_int(e.w);
-                            bin_fast<MODE, UNITW>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y, e.z,
-                                                  it.a_start + (pk >> 8), jbase + (pk & 0xff), cnt);
+                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y,
+                                                      e.z, it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
+                                                      rb, cnt);
                         }
                         __syncwarp();
                     }
@@ -634,7 +773,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
                         if (!v) continue;
                         add64_owned(s_alo, s_ahi, b, v);
-                        if (rb != it.a_region) atomicAdd(&P.g_sub[(size_t)rb * P.nb + b], v);
+                        if (rb != it.a_region) dev::acc_add_global(P.g_sub, (size_t)rb * P.nb + b, v);
                         s_lo[b] = 0;
                         s_hi[b] = 0;
                     }
@@ -649,8 +788,8 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             for (int b = tid; b < P.nb; b += NT) {
                 const unsigned long long v = ((unsigned long long)s_ahi[b] << 32) | s_alo[b];
                 if (!v) continue;
-                atomicAdd(&P.g_full[b], v);
-                atomicAdd(&P.g_sub[(size_t)it.a_region * P.nb + b], v);
+                dev::acc_add_global(P.g_full, b, v);
+                dev::acc_add_global(P.g_sub, (size_t)it.a_region * P.nb + b, v);
                 s_alo[b] = 0;
                 s_ahi[b] = 0;
             }
@@ -663,7 +802,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     if (!JK) {
         for (int b = tid; b < P.nb; b += NT) {
             const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
-            if (v) atomicAdd(&P.g_full[b], v);
+            if (v) dev::acc_add_global(P.g_full, b, v);
         }
     }
     // ---- counters
@@ -685,21 +824,38 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
 
 typedef void (*KernelFn)(const KParams);
 
-template <int MODE>
+template <int MODE, int WK>
 KernelFn pick_kernel(bool unitw, bool jk, bool exact) {
-    if (exact) {
-        if (unitw) return jk ? pair_count_kernel<MODE, true, true, true> : pair_count_kernel<MODE, true, false, true>;
-        return jk ? pair_count_kernel<MODE, false, true, true> : pair_count_kernel<MODE, false, false, true>;
+    if constexpr (WK == W_PLAIN) {
+        if (unitw) {
+            if (exact)
+                return jk ? pair_count_kernel<MODE, true, true, true, WK> : pair_count_kernel<MODE, true, false, true, WK>;
+            return jk ? pair_count_kernel<MODE, true, true, false, WK> : pair_count_kernel<MODE, true, false, false, WK>;
+        }
     }
-    if (unitw) return jk ? pair_count_kernel<MODE, true, true, false> : pair_count_kernel<MODE, true, false, false>;
-    return jk ? pair_count_kernel<MODE, false, true, false> : pair_count_kernel<MODE, false, false, false>;
+    if (exact) return jk ? pair_count_kernel<MODE, false, true, true, WK> : pair_count_kernel<MODE, false, false, true, WK>;
+    return jk ? pair_count_kernel<MODE, false, true, false, WK> : pair_count_kernel<MODE, false, false, false, WK>;
 }
 
-KernelFn pick(int mode, bool unitw, bool jk, bool exact) {
+template <int MODE>
+KernelFn pick_3d(int wk, bool unitw, bool jk, bool exact) {
+    switch (wk) {
+    case W_INVP_DD: return pick_kernel<MODE, W_INVP_DD>(unitw, jk, exact);
+    case W_INVP_DR: return pick_kernel<MODE, W_INVP_DR>(unitw, jk, exact);
+    default: return pick_kernel<MODE, W_PLAIN>(unitw, jk, exact);
+    }
+}
+
+// Kernel for a mode, weight kind (W_PLAIN, W_INVP_DD, W_INVP_DR for 3-D;
+// W_PLAIN, W_ANG_INVP for angular), unit weights, jackknife and precision.
+KernelFn pick(int mode, int wk, bool unitw, bool jk, bool exact) {
     switch (mode) {
-    case MODE_MONOPOLE: return pick_kernel<MODE_MONOPOLE>(unitw, jk, exact);
-    case MODE_SIGMA_PI: return pick_kernel<MODE_SIGMA_PI>(unitw, jk, exact);
-    default: return pick_kernel<MODE_S_MU>(unitw, jk, exact);
+    case MODE_MONOPOLE: return pick_3d<MODE_MONOPOLE>(wk, unitw, jk, exact);
+    case MODE_SIGMA_PI: return pick_3d<MODE_SIGMA_PI>(wk, unitw, jk, exact);
+    case MODE_S_MU: return pick_3d<MODE_S_MU>(wk, unitw, jk, exact);
+    default:
+        return wk == W_ANG_INVP ? pick_kernel<MODE_ANGULAR, W_ANG_INVP>(unitw, jk, exact)
+                                : pick_kernel<MODE_ANGULAR, W_PLAIN>(unitw, jk, exact);
     }
 }
 
@@ -903,6 +1059,7 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
 // sigma^2 = s^2 - pi^2 and mu = |pi| / s, each doubled for safety.
 struct Guards {
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
+    float g_ang = 0;  // angular counts: bound on |chord^2 / 2 - (1 - cos(theta))_ref|
 };
 
 Guards compute_guards(double side, int m, double rb) {
@@ -934,8 +1091,8 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     L.l1.assign(LUT1_N, LUT_AMB);
     L.l2.assign(LUT2_N, LUT_AMB);
     // Table 1 over the float bits of s^2 (monopole, s-mu; the range test is
-    // folded in) or of sigma^2 (sigma-pi).
-    const bool s_axis = bin.mode != MODE_SIGMA_PI;
+    // folded in), of sigma^2 (sigma-pi) or of 1 - cos(theta) (angular).
+    const bool s_axis = bin.mode == MODE_MONOPOLE || bin.mode == MODE_S_MU;
     Category c1{&bin.t1, bin.nb1, s_axis, bin.min_r_sq, bin.max_r_sq};
     std::vector<double> e1(bin.t1.begin(), bin.t1.end());
     if (s_axis) {
@@ -948,7 +1105,7 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     const int elo = ehi - LUT1_OCTAVES;
     const uint32_t sh = 23 - LUT1_BITS;
     L.base1 = bits_of(std::ldexp(1.0f, elo)) >> sh;
-    const double g1 = s_axis ? g.g_s2 : g.g_a;
+    const double g1 = s_axis ? g.g_s2 : (bin.mode == MODE_ANGULAR ? g.g_ang : g.g_a);
     for (int i = 1; i < LUT1_N - 1; ++i) {
         const double v0 = f_from_bits((L.base1 + i) << sh);
         const double v1 = f_from_bits((L.base1 + i + 1) << sh);
@@ -961,7 +1118,7 @@ Luts build_luts(const Binning &bin, const Guards &g) {
         if (s_axis && v0 - g1 > bin.max_r_sq) L.l1[LUT1_N - 1] = LUT_INV;
         if (!s_axis && std::isfinite(bin.t1[bin.nb1]) && v0 - g1 > bin.t1[bin.nb1]) L.l1[LUT1_N - 1] = LUT_INV;
     }
-    if (bin.mode != MODE_MONOPOLE) {
+    if (bin.mode == MODE_SIGMA_PI || bin.mode == MODE_S_MU) {
         // Table 2, linear buckets: mu on [0, 1.25) or |pi| on [0, 1.25 rmax).
         const double xmax2 = bin.mode == MODE_S_MU ? 1.25 : 1.25 * std::sqrt((double)bin.max_r_sq);
         L.scale2 = (float)(LUT2_N / xmax2);
@@ -990,89 +1147,161 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     return L;
 }
 
-int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
+namespace {
+
+// Largest number of pairs one flush of a shared-memory histogram can hold:
+// a work item's A points times the B points of all its segments.
+long long max_item_pairs(const std::vector<WorkItem> &items, const std::vector<Segment> &segs) {
+    long long pmax = 1;
+    for (const WorkItem &w : items) {
+        long long bl = 0;
+        for (int k = w.seg_begin; k < w.seg_end; ++k) bl += segs[k].b_len;
+        pmax = std::max(pmax, (long long)w.a_len * bl);
+    }
+    return pmax;
+}
+
+// Fixed-point shift S: a pair weight w is added as round(w * 2^S) to 64-bit
+// shared-memory sums and 128-bit global sums.  S keeps the largest flush
+// (pmax pairs of weight at most wmax) below 2^62; every float weight of at
+// least 2^(23-S) is then represented exactly, and smaller ones to 2^-(S+1).
+int fixed_point_shift(double wmax, long long pmax) {
+    const double lg = std::log2(std::max(wmax * (1.0 + 1e-6), 1e-30)) + std::log2((double)std::max(pmax, 1LL));
+    const int S = (int)std::floor(62.0 - lg);
+    return std::max(-100, std::min(S, 100));
+}
+
+// A 128-bit two's-complement fixed-point sum (low word, high word) as a
+// double, rounded once, times inv = 2^-S.
+double fixed_to_double(const unsigned long long *p, double inv) {
+    const unsigned __int128 u = ((unsigned __int128)p[1] << 64) | (unsigned __int128)p[0];
+    return (double)(__int128)u * inv;
+}
+
+// Everything a count needs before device buffers exist: grids, work list,
+// kernel choice, fixed-point scale, guards, tables, and the kernel
+// parameters other than buffer addresses.
+struct CountPlan {
+    const Binning *bin = nullptr;
+    const UpTable *up = nullptr;
+    bool is_auto = false, jk = false, unitw = false, angular = false;
+    int nb = 0, n_jk = 1, wk = W_PLAIN;
+    double inv = 1.0;  // 2^-S
+    std::vector<WorkItem> items;
+    std::vector<Segment> segs;
+    SmemLayout L;
+    Luts luts;
+    KParams P;
+    KernelFn fn = nullptr;
+    size_t n_flags() const { return wk == W_PLAIN ? 0 : (size_t)(1 + n_jk) * nb; }
+    size_t n_up() const { return up ? up->thr.size() : 0; }
+};
+
+// Device addresses of the per-count buffers.
+struct CountBuffers {
+    WorkItem *items = nullptr;
+    Segment *segs = nullptr;
+    unsigned long long *full = nullptr, *sub = nullptr, *cnt = nullptr;
+    int *head = nullptr, *err = nullptr;
+    float *t1 = nullptr, *t2 = nullptr, *up_thr = nullptr;
+    unsigned char *l1 = nullptr, *l2 = nullptr;
+    unsigned *flags = nullptr;
+    double *up_bins = nullptr, *up_centre = nullptr;
+};
+
+int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Error *err) {
     const Binning *bin = req.bin;
     Catalog *A = const_cast<Catalog *>(req.a);
     Catalog *B = const_cast<Catalog *>(req.b ? req.b : req.a);
-    const bool is_auto = (req.b == nullptr);
-    const int nb = bin->nb;
-    const int n_jk = bin->n_jk;
-    const bool jk = n_jk > 1;
-    const double rb = bin->rmax_bound;
+    C.bin = bin;
+    C.up = req.up;
+    C.is_auto = (req.b == nullptr);
+    C.angular = bin->mode == MODE_ANGULAR;
+    C.nb = bin->nb;
+    C.n_jk = bin->n_jk;
+    C.jk = C.n_jk > 1;
+    const int wt = req.weighting;
+    // Weight kind, the weight each grid point carries, and the points
+    // counted: 3-D counts use the d_comov partition (GalaxyBoxes); angular
+    // counts use every point unless inverse-p weights ask for a redshift
+    // (GalaxyPixels' require_redshift, src/correlators_invpweight.cpp:990-1028).
+    if (C.angular) C.wk = wt == WEIGHTS_INVP_DD ? W_ANG_INVP : W_PLAIN;
+    else C.wk = wt == WEIGHTS_INVP_DD ? W_INVP_DD : (wt == WEIGHTS_INVP_DR ? W_INVP_DR : W_PLAIN);
+    const bool input_w = C.angular ? wt != WEIGHTS_INVP_DR : wt == WEIGHTS_INVP_DD;
+    const bool subset = C.angular ? wt != WEIGHTS_PLAIN : true;
+    auto wmax_of = [&](const Catalog *c) { return (double)(input_w ? c->iw_max : c->w_max); };
+    auto unit_of = [&](const Catalog *c) { return input_w ? c->iw_unit : c->unit_weights; };
+    C.unitw = C.wk == W_PLAIN && unit_of(A) && unit_of(B);
 
+    // Per-axis bound on the separation of every counted pair: the maximum
+    // separation (3-D), or the chord of the largest binned 1 - cos(theta),
+    // widened by the double rounding of the reference's value and by how far
+    // the unit vectors are from unit length (angular).
+    double rb = bin->rmax_bound;
+    double norm_dev = 0, tn = 2.0;
+    if (C.angular) {
+        if (std::isfinite(bin->t1[bin->nb1])) tn = std::max((double)bin->t1[bin->nb1], 0.0);
+        norm_dev = std::max(A->norm_dev, B->norm_dev);
+        rb = std::sqrt(2.0 * tn + 4e-15 + 2.0 * norm_dev) * (1.0 + 1e-6) + 1e-12;
+    }
     int m = req.refinement > 0 ? req.refinement : ctx->refinement;
     if (m <= 0) {
         // Automatic: refine to side rb/2 when cells of that size would still
         // hold a few hundred points on average.
+        const double *lo = C.angular ? (subset ? A->ulo_kept : A->ulo_all) : A->lo_kept;
+        const double *hi = C.angular ? (subset ? A->uhi_kept : A->uhi_all) : A->hi_kept;
+        const double n = subset ? (double)A->n_kept : (double)A->n_all;
         double vol = 1;
-        for (int k = 0; k < 3; ++k) vol *= std::max(A->hi_kept[k] - A->lo_kept[k], rb);
-        const double per_cell = A->n_kept * (rb / 2) * (rb / 2) * (rb / 2) / vol;
+        for (int k = 0; k < 3; ++k) vol *= std::max(hi[k] - lo[k], rb);
+        const double per_cell = n * (rb / 2) * (rb / 2) * (rb / 2) / vol;
         m = per_cell >= 256 ? 2 : 1;
     }
     const double side = rb / m * (1.0 + 1e-9);
-
+    GridSpec gs;
+    gs.side = side;
+    gs.subset_kept = subset;
+    gs.angular = C.angular;
+    gs.input_w = input_w;
     Grid *ga = nullptr, *gb = nullptr;
-    if (build_grid(ctx, A, side, true, req.exact_fp64, &ga, err)) return err->status;
-    if (is_auto) gb = ga;
-    else if (build_grid(ctx, B, side, true, req.exact_fp64, &gb, err)) return err->status;
-
-    std::vector<WorkItem> items;
-    std::vector<Segment> segs;
-    build_work_items(*ga, *gb, is_auto, m, side, rb, items, segs);
-
-    // Fixed-point scale: the largest pair weight stays below 2^31.
-    const bool unitw = A->unit_weights && B->unit_weights;
-    float wscale = 1.0f;
-    if (!unitw) {
-        const double wmax = (double)A->w_max * (double)B->w_max * (1.0 + 1e-6);
-        int S = (int)std::floor(30.0 - std::log2(std::max(wmax, 1e-30)));
-        S = std::min(S, 100);
-        wscale = std::ldexp(1.0f, S);
+    if (build) {
+        if (build_grid(ctx, A, gs, req.exact_fp64, &ga, err)) return err->status;
+        if (C.is_auto) gb = ga;
+        else if (build_grid(ctx, B, gs, req.exact_fp64, &gb, err)) return err->status;
+    } else {
+        ga = find_grid(A, gs, req.exact_fp64);
+        gb = C.is_auto ? ga : find_grid(B, gs, req.exact_fp64);
+        if (!ga || !gb) {
+            err->status = 1;
+            err->msg = std::string("no cell grid cached on catalogue ") + (!ga ? "a" : "b") +
+                       " for this binning, weighting, refinement and precision: the allocation-free count does "
+                       "not build grids; count the same catalogues once with tpcf_count first";
+            return err->status;
+        }
     }
+    build_work_items(*ga, *gb, C.is_auto, m, side, rb, C.items, C.segs);
 
-    const SmemLayout L = smem_layout(nb, bin->nb1, bin->nb2, req.exact_fp64, jk);
-    if (L.total + 1024 > ctx->smem_optin) {
+    float wscale = 1.0f;
+    if (!C.unitw) {
+        double wmax = wmax_of(A) * wmax_of(B);
+        const double up_max = C.up ? 4.0 * C.up->abs_max : 0.0;  // interpolation stays within 4x the bins
+        if (C.wk == W_INVP_DD) wmax *= up_max * std::max(req.n_runs, 1);
+        else if (C.wk == W_INVP_DR) wmax *= up_max;
+        else if (C.wk == W_ANG_INVP) wmax *= std::max(req.n_runs, 1);
+        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
+        wscale = std::ldexp(1.0f, S);
+        C.inv = std::ldexp(1.0, -S);
+    }
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk);
+    if (C.L.total + 1024 > ctx->smem_optin) {
         err->status = 6;
         err->msg = "histogram does not fit in shared memory";
         return err->status;
     }
-    const Guards g = compute_guards(side, m, rb);
-    const Luts luts = build_luts(*bin, g);
+    Guards g = compute_guards(side, m, rb);
+    if (C.angular) g.g_ang = (float)((0.5 * g.g_s2 + 2.0 * norm_dev + 2e-15) * (1.0 + 1e-6));
+    C.luts = build_luts(*bin, g);
 
-    DevBuf<WorkItem> d_items;
-    DevBuf<Segment> d_segs;
-    DevBuf<unsigned long long> d_full, d_sub, d_cnt;
-    DevBuf<int> d_head, d_err;
-    DevBuf<float> d_t1, d_t2;
-    DevBuf<unsigned char> d_l1, d_l2;
-    cudaStream_t stm = ctx->stream;
-    TPCF_TRY(d_items.alloc(items.size()));
-    TPCF_TRY(d_segs.alloc(segs.size()));
-    TPCF_TRY(d_full.alloc(nb));
-    TPCF_TRY(d_sub.alloc((size_t)nb * n_jk));
-    TPCF_TRY(d_cnt.alloc(4));
-    TPCF_TRY(d_head.alloc(1));
-    TPCF_TRY(d_err.alloc(1));
-    TPCF_TRY(d_t1.alloc(bin->t1.size()));
-    TPCF_TRY(d_t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
-    TPCF_TRY(d_l1.alloc(LUT1_N));
-    TPCF_TRY(d_l2.alloc(LUT2_N));
-    if (!items.empty()) {
-        TPCF_TRY(cudaMemcpyAsync(d_items.p, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, stm));
-        TPCF_TRY(cudaMemcpyAsync(d_segs.p, segs.data(), sizeof(Segment) * segs.size(), cudaMemcpyHostToDevice, stm));
-    }
-    TPCF_TRY(cudaMemcpyAsync(d_t1.p, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
-    if (!bin->t2.empty())
-        TPCF_TRY(cudaMemcpyAsync(d_t2.p, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(d_l1.p, luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(d_l2.p, luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemsetAsync(d_full.p, 0, sizeof(unsigned long long) * nb, stm));
-    TPCF_TRY(cudaMemsetAsync(d_sub.p, 0, sizeof(unsigned long long) * nb * n_jk, stm));
-    TPCF_TRY(cudaMemsetAsync(d_cnt.p, 0, sizeof(unsigned long long) * 4, stm));
-    TPCF_TRY(cudaMemsetAsync(d_head.p, 0, sizeof(int), stm));
-    TPCF_TRY(cudaMemsetAsync(d_err.p, 0, sizeof(int), stm));
-
-    KParams P;
+    KParams &P = C.P;
     std::memset(&P, 0, sizeof(P));
     auto fill = [&](GridK &k, const Grid &gr, const Catalog &c) {
         k.pos = gr.pos.p;
@@ -1089,14 +1318,11 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     };
     fill(P.a, *ga, *A);
     fill(P.b, *gb, *B);
-    P.items = d_items.p;
-    P.segs = d_segs.p;
-    P.n_items = (int)items.size();
-    P.head = d_head.p;
+    P.n_items = (int)C.items.size();
     P.side = side;
     P.n1 = bin->nb1;
-    P.n2 = bin->mode == MODE_MONOPOLE ? 0 : bin->nb2;
-    P.nb = nb;
+    P.n2 = (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) ? bin->nb2 : 0;
+    P.nb = C.nb;
     P.min_r_sq = bin->min_r_sq;
     P.max_r_sq = bin->max_r_sq;
     P.g_s2 = g.g_s2;
@@ -1105,73 +1331,204 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     P.c1_mu = g.c1_mu;
     P.c2_mu = g.c2_mu;
     P.g_mu0 = g.g_mu0;
-    P.s2_lut_min = luts.s2_lut_min;
-    P.lo_cut = bin->min_r_sq - g.g_s2;
-    P.hi_cut = bin->max_r_sq + g.g_s2;
-    P.t1g = d_t1.p;
-    P.t2g = d_t2.p;
-    P.lut1g = d_l1.p;
-    P.lut2g = d_l2.p;
-    P.lut1_base = luts.base1;
-    P.lut2_scale = luts.scale2;
-    P.g_full = d_full.p;
-    P.g_sub = d_sub.p;
-    P.n_jk = n_jk;
+    P.g_ang = g.g_ang;
+    P.s2_lut_min = C.luts.s2_lut_min;
+    if (C.angular) {
+        // candidate test on the squared chord: v = chord^2 / 2 < T[n] + g_ang
+        P.lo_cut = -1.0f;
+        P.hi_cut = (float)(2.0 * (tn + g.g_ang) * (1.0 + 1e-6));
+    } else {
+        P.lo_cut = bin->min_r_sq - g.g_s2;
+        P.hi_cut = bin->max_r_sq + g.g_s2;
+    }
+    P.lut1_base = C.luts.base1;
+    P.lut2_scale = C.luts.scale2;
+    P.n_jk = C.n_jk;
     P.wscale = wscale;
-    P.counters = d_cnt.p;
-    P.err = d_err.p;
+    P.a_masks = A->masks.p;
+    P.b_masks = B->masks.p;
+    P.n_mask = A->n_mask;
+    P.n_runs_f = (float)req.n_runs;
+    P.n_runs_d = (double)req.n_runs;
+    if (C.up) {
+        P.n_up = C.up->ax.n_bins;
+        P.up_min = (double)C.up->ax.min;
+        P.up_max = (double)C.up->ax.max;
+    }
+    C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
+    return 0;
+}
 
-    KernelFn fn = pick(bin->mode, unitw, jk, req.exact_fp64);
-    TPCF_TRY(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
+// Upload the tables and the work list, clear the accumulators, launch, read
+// back, and convert the fixed-point sums; timed: record the kernel's device
+// time in the stats.
+int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, double *region_out, Stats *st,
+            Error *err, bool timed) {
+    const Binning *bin = C.bin;
+    const int nb = C.nb, n_jk = C.n_jk;
+    cudaStream_t stm = ctx->stream;
+    if (!C.items.empty()) {
+        TPCF_TRY(cudaMemcpyAsync(D.items, C.items.data(), sizeof(WorkItem) * C.items.size(), cudaMemcpyHostToDevice,
+                                 stm));
+        TPCF_TRY(cudaMemcpyAsync(D.segs, C.segs.data(), sizeof(Segment) * C.segs.size(), cudaMemcpyHostToDevice, stm));
+    }
+    TPCF_TRY(cudaMemcpyAsync(D.t1, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
+    if (!bin->t2.empty())
+        TPCF_TRY(cudaMemcpyAsync(D.t2, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(D.l1, C.luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(D.l2, C.luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
+    if (C.up) {
+        const size_t k = C.n_up();
+        TPCF_TRY(cudaMemcpyAsync(D.up_thr, C.up->thr.data(), sizeof(float) * k, cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemcpyAsync(D.up_bins, C.up->bins.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemcpyAsync(D.up_centre, C.up->centre.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stm));
+    }
+    // What the kernel accumulates into starts at zero on every call.
+    TPCF_TRY(cudaMemsetAsync(D.full, 0, sizeof(unsigned long long) * 2 * nb, stm));
+    TPCF_TRY(cudaMemsetAsync(D.sub, 0, sizeof(unsigned long long) * 2 * (size_t)nb * n_jk, stm));
+    TPCF_TRY(cudaMemsetAsync(D.cnt, 0, sizeof(unsigned long long) * 4, stm));
+    TPCF_TRY(cudaMemsetAsync(D.head, 0, sizeof(int), stm));
+    TPCF_TRY(cudaMemsetAsync(D.err, 0, sizeof(int), stm));
+    if (C.n_flags()) TPCF_TRY(cudaMemsetAsync(D.flags, 0, sizeof(unsigned) * C.n_flags(), stm));
+
+    KParams P = C.P;
+    P.items = D.items;
+    P.segs = D.segs;
+    P.head = D.head;
+    P.t1g = D.t1;
+    P.t2g = D.t2;
+    P.lut1g = D.l1;
+    P.lut2g = D.l2;
+    P.g_full = D.full;
+    P.g_sub = D.sub;
+    P.counters = D.cnt;
+    P.err = D.err;
+    P.flags = D.flags;
+    P.up_thr = D.up_thr;
+    P.up_bins = D.up_bins;
+    P.up_centre = D.up_centre;
+
+    TPCF_TRY(cudaFuncSetAttribute((const void *)C.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.L.total));
     int per_sm = 1;
-    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, L.total));
+    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, C.fn, NT, C.L.total));
     per_sm = std::max(per_sm, 1);
-    cudaEvent_t e0, e1;
-    TPCF_TRY(cudaEventCreate(&e0));
-    TPCF_TRY(cudaEventCreate(&e1));
-    TPCF_TRY(cudaEventRecord(e0, stm));
-    if (!items.empty()) {
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)items.size());
-        fn<<<grid, NT, L.total, stm>>>(P);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (timed) {
+        TPCF_TRY(cudaEventCreate(&e0));
+        TPCF_TRY(cudaEventCreate(&e1));
+        TPCF_TRY(cudaEventRecord(e0, stm));
+    }
+    if (!C.items.empty()) {
+        const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)C.items.size());
+        C.fn<<<grid, NT, C.L.total, stm>>>(P);
         ++ctx->launches;
         TPCF_TRY(cudaGetLastError());
     }
-    TPCF_TRY(cudaEventRecord(e1, stm));
-    std::vector<unsigned long long> hf(nb), hs((size_t)nb * n_jk), hc(4);
+    if (timed) TPCF_TRY(cudaEventRecord(e1, stm));
+    std::vector<unsigned long long> hf(2 * (size_t)nb), hs(2 * (size_t)nb * n_jk), hc(4);
+    std::vector<unsigned> hflags(C.n_flags());
     int herr = 0;
-    TPCF_TRY(cudaMemcpyAsync(hf.data(), d_full.p, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hs.data(), d_sub.p, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hc.data(), d_cnt.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(&herr, d_err.p, sizeof(int), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(hf.data(), D.full, sizeof(unsigned long long) * hf.size(), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(hs.data(), D.sub, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(hc.data(), D.cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(&herr, D.err, sizeof(int), cudaMemcpyDeviceToHost, stm));
+    if (!hflags.empty())
+        TPCF_TRY(cudaMemcpyAsync(hflags.data(), D.flags, sizeof(unsigned) * hflags.size(), cudaMemcpyDeviceToHost,
+                                 stm));
     TPCF_TRY(cudaStreamSynchronize(stm));
     float ms = 0;
-    cudaEventElapsedTime(&ms, e0, e1);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
+    if (timed) {
+        cudaEventElapsedTime(&ms, e0, e1);
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
     if (herr) {
         err->status = 4;
         err->msg = "device wait exceeded its iteration limit; results discarded";
         return err->status;
     }
-    const double inv = unitw ? 1.0 : 1.0 / (double)wscale;
-    for (int b = 0; b < nb; ++b) full_out[b] = (double)(long long)hf[b] * inv;
+    // A bin that met a non-finite pair weight holds what double
+    // accumulation would: NaN, or an infinity of one sign.
+    auto flagged = [](unsigned f, double v) {
+        if ((f & 1u) || ((f & 2u) && (f & 4u))) return std::numeric_limits<double>::quiet_NaN();
+        if (f & 2u) return std::numeric_limits<double>::infinity();
+        if (f & 4u) return -std::numeric_limits<double>::infinity();
+        return v;
+    };
+    for (int b = 0; b < nb; ++b) {
+        full_out[b] = fixed_to_double(&hf[2 * (size_t)b], C.inv);
+        if (!hflags.empty()) full_out[b] = flagged(hflags[b], full_out[b]);
+    }
     if (region_out) {
-        if (jk)
-            for (size_t k = 0; k < hs.size(); ++k) region_out[k] = (double)(long long)hs[k] * inv;
-        else
+        if (C.jk) {
+            for (size_t k = 0; k < (size_t)nb * n_jk; ++k) {
+                region_out[k] = fixed_to_double(&hs[2 * k], C.inv);
+                if (!hflags.empty()) region_out[k] = flagged(hflags[nb + k], region_out[k]);
+            }
+        } else {
             for (int b = 0; b < nb; ++b) region_out[b] = full_out[b];
+        }
     }
     if (st) {
         st->candidates += hc[0];
         st->in_range += hc[1];
         st->guard += hc[2];
         st->overflow += hc[3];
-        st->items += items.size();
+        st->items += C.items.size();
         st->ms_kernel += ms;
     }
     return 0;
 }
 
+}  // namespace
+
+int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
+    CountPlan C;
+    if (plan_count(ctx, req, true, C, err)) return err->status;
+    const Binning *bin = req.bin;
+    DevBuf<WorkItem> d_items;
+    DevBuf<Segment> d_segs;
+    DevBuf<unsigned long long> d_full, d_sub, d_cnt;
+    DevBuf<int> d_head, d_err;
+    DevBuf<float> d_t1, d_t2, d_up_thr;
+    DevBuf<unsigned char> d_l1, d_l2;
+    DevBuf<unsigned> d_flags;
+    DevBuf<double> d_up_bins, d_up_centre;
+    TPCF_TRY(d_items.alloc(C.items.size()));
+    TPCF_TRY(d_segs.alloc(C.segs.size()));
+    TPCF_TRY(d_full.alloc(2 * (size_t)C.nb));
+    TPCF_TRY(d_sub.alloc(2 * (size_t)C.nb * C.n_jk));
+    TPCF_TRY(d_cnt.alloc(4));
+    TPCF_TRY(d_head.alloc(1));
+    TPCF_TRY(d_err.alloc(1));
+    TPCF_TRY(d_t1.alloc(bin->t1.size()));
+    TPCF_TRY(d_t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
+    TPCF_TRY(d_l1.alloc(LUT1_N));
+    TPCF_TRY(d_l2.alloc(LUT2_N));
+    if (C.n_flags()) TPCF_TRY(d_flags.alloc(C.n_flags()));
+    if (C.up) {
+        TPCF_TRY(d_up_thr.alloc(C.n_up()));
+        TPCF_TRY(d_up_bins.alloc(C.n_up()));
+        TPCF_TRY(d_up_centre.alloc(C.n_up()));
+    }
+    CountBuffers D;
+    D.items = d_items.p;
+    D.segs = d_segs.p;
+    D.full = d_full.p;
+    D.sub = d_sub.p;
+    D.cnt = d_cnt.p;
+    D.head = d_head.p;
+    D.err = d_err.p;
+    D.t1 = d_t1.p;
+    D.t2 = d_t2.p;
+    D.l1 = d_l1.p;
+    D.l2 = d_l2.p;
+    D.flags = C.n_flags() ? d_flags.p : nullptr;
+    D.up_thr = d_up_thr.p;
+    D.up_bins = d_up_bins.p;
+    D.up_centre = d_up_centre.p;
+    return execute(ctx, C, D, full_out, region_out, st, err, true);
+}
 
 // ---------------------------------------------------------------------------
 // Counting without device allocation.
@@ -1182,17 +1539,17 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
 // where a foreign allocation fails or fragments that pool, and latency-bound
 // loops that cannot take the device-wide synchronisation cudaFree implies.
 // For them every scratch buffer of run_count — the work list, the segment
-// list, the 64-bit fixed-point histograms, the counters, the work-queue head,
-// the error flag, the threshold and lookup tables — is carved from the one
-// static array below, of kStaticScratchBytes (32 MiB).  Each device that
+// list, the fixed-point histograms, the counters, the work-queue head, the
+// error flag, the threshold, lookup and up-weight tables — is carved from the
+// one static array below, of kStaticScratchBytes (32 MiB).  Each device that
 // loads the library holds that array until the process exits.
 //
 // The array is shared by every call on a device and keeps the contents of
-// the last call; each call clears the histograms, counters, queue head and
-// error flag before its launch.  Two calls whose work overlaps on the GPU
-// (two contexts on one device, on different streams, from different host
-// threads) race on it.  Calls from one thread do not overlap: each waits for
-// its results before it returns.
+// the last call; each call clears the histograms, counters, queue head, error
+// flag and non-finite flags before its launch.  Two calls whose work
+// overlaps on the GPU (two contexts on one device, on different streams,
+// from different host threads) race on it.  Calls from one thread do not
+// overlap: each waits for its results before it returns.
 static __device__ __align__(256) unsigned char g_count_scratch[kStaticScratchBytes];
 
 namespace {
@@ -1230,7 +1587,7 @@ int scratch_address(int device, void **out, Error *err) {
 
 // Byte offsets of the buffers inside the static array, each 256-aligned.
 struct ScratchPlan {
-    size_t items, segs, full, sub, cnt, head, err, t1, t2, l1, l2, total = 0;
+    size_t total = 0;
     size_t take(size_t bytes) {
         const size_t off = total;
         total += (std::max<size_t>(bytes, 1) + 255) & ~size_t(255);
@@ -1243,201 +1600,61 @@ struct ScratchPlan {
 int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
                      Error *err) {
     const Binning *bin = req.bin;
-    Catalog *A = const_cast<Catalog *>(req.a);
-    Catalog *B = const_cast<Catalog *>(req.b ? req.b : req.a);
-    const bool is_auto = (req.b == nullptr);
-    const int nb = bin->nb;
-    const int n_jk = bin->n_jk;
-    const bool jk = n_jk > 1;
-    const double rb = bin->rmax_bound;
-
-    // The same cell size as run_count, so that the grids it cached are found.
-    int m = req.refinement > 0 ? req.refinement : ctx->refinement;
-    if (m <= 0) {
-        double vol = 1;
-        for (int k = 0; k < 3; ++k) vol *= std::max(A->hi_kept[k] - A->lo_kept[k], rb);
-        const double per_cell = A->n_kept * (rb / 2) * (rb / 2) * (rb / 2) / vol;
-        m = per_cell >= 256 ? 2 : 1;
-    }
-    const double side = rb / m * (1.0 + 1e-9);
-
-    // Scratch layout.  The histogram and table part is known before the work
+    const int nb = bin->nb, n_jk = bin->n_jk;
+    // The histogram and table part of the scratch is known before the work
     // list is built; refuse an oversized binning before anything else.
-    ScratchPlan plan;
-    plan.full = plan.take(sizeof(unsigned long long) * nb);
-    plan.sub = plan.take(sizeof(unsigned long long) * (size_t)nb * n_jk);
-    plan.cnt = plan.take(sizeof(unsigned long long) * 4);
-    plan.head = plan.take(sizeof(int));
-    plan.err = plan.take(sizeof(int));
-    plan.t1 = plan.take(sizeof(float) * bin->t1.size());
-    plan.t2 = plan.take(sizeof(float) * std::max<size_t>(bin->t2.size(), 1));
-    plan.l1 = plan.take(LUT1_N);
-    plan.l2 = plan.take(LUT2_N);
+    ScratchPlan sp;
+    const size_t o_full = sp.take(sizeof(unsigned long long) * 2 * nb);
+    const size_t o_sub = sp.take(sizeof(unsigned long long) * 2 * (size_t)nb * n_jk);
+    const size_t o_cnt = sp.take(sizeof(unsigned long long) * 4);
+    const size_t o_head = sp.take(sizeof(int));
+    const size_t o_err = sp.take(sizeof(int));
+    const size_t o_t1 = sp.take(sizeof(float) * bin->t1.size());
+    const size_t o_t2 = sp.take(sizeof(float) * std::max<size_t>(bin->t2.size(), 1));
+    const size_t o_l1 = sp.take(LUT1_N);
+    const size_t o_l2 = sp.take(LUT2_N);
+    const size_t n_flags = req.weighting == WEIGHTS_PLAIN ? 0 : (size_t)(1 + n_jk) * nb;
+    const size_t o_flags = sp.take(sizeof(unsigned) * n_flags);
+    const size_t n_up = req.up ? req.up->thr.size() : 0;
+    const size_t o_up_thr = sp.take(sizeof(float) * n_up);
+    const size_t o_up_bins = sp.take(sizeof(double) * n_up);
+    const size_t o_up_centre = sp.take(sizeof(double) * n_up);
     auto too_big = [&](size_t n_items, size_t n_segs) {
         err->status = 6;
-        err->msg = "count needs " + std::to_string(plan.total) + " bytes of scratch (" + std::to_string(nb) +
+        err->msg = "count needs " + std::to_string(sp.total) + " bytes of scratch (" + std::to_string(nb) +
                    " bins x " + std::to_string(n_jk) + " regions, " + std::to_string(n_items) + " work items, " +
                    std::to_string(n_segs) + " segments); the static scratch holds " +
                    std::to_string(kStaticScratchBytes) + " bytes: use tpcf_count";
         return err->status;
     };
-    if (plan.total > kStaticScratchBytes) return too_big(0, 0);
+    if (sp.total > kStaticScratchBytes) return too_big(0, 0);
 
-    Grid *ga = find_grid(A, side, true, req.exact_fp64);
-    Grid *gb = is_auto ? ga : find_grid(B, side, true, req.exact_fp64);
-    if (!ga || !gb) {
-        err->status = 1;
-        err->msg = std::string("no cell grid cached on catalogue ") + (!ga ? "a" : "b") +
-                   " for this binning, refinement and precision: the allocation-free count does not build "
-                   "grids; count the same catalogues once with tpcf_count first";
-        return err->status;
-    }
-
-    std::vector<WorkItem> items;
-    std::vector<Segment> segs;
-    build_work_items(*ga, *gb, is_auto, m, side, rb, items, segs);
-
-    plan.items = plan.take(sizeof(WorkItem) * items.size());
-    plan.segs = plan.take(sizeof(Segment) * segs.size());
-    if (plan.total > kStaticScratchBytes) return too_big(items.size(), segs.size());
-
-    const bool unitw = A->unit_weights && B->unit_weights;
-    float wscale = 1.0f;
-    if (!unitw) {
-        const double wmax = (double)A->w_max * (double)B->w_max * (1.0 + 1e-6);
-        int S = (int)std::floor(30.0 - std::log2(std::max(wmax, 1e-30)));
-        S = std::min(S, 100);
-        wscale = std::ldexp(1.0f, S);
-    }
-    const SmemLayout L = smem_layout(nb, bin->nb1, bin->nb2, req.exact_fp64, jk);
-    if (L.total + 1024 > ctx->smem_optin) {
-        err->status = 6;
-        err->msg = "histogram does not fit in shared memory";
-        return err->status;
-    }
-    const Guards g = compute_guards(side, m, rb);
-    const Luts luts = build_luts(*bin, g);
+    CountPlan C;
+    if (plan_count(ctx, req, false, C, err)) return err->status;
+    const size_t o_items = sp.take(sizeof(WorkItem) * C.items.size());
+    const size_t o_segs = sp.take(sizeof(Segment) * C.segs.size());
+    if (sp.total > kStaticScratchBytes) return too_big(C.items.size(), C.segs.size());
 
     void *base = nullptr;
     if (scratch_address(ctx->device, &base, err)) return err->status;
-    unsigned char *sp = static_cast<unsigned char *>(base);
-    WorkItem *d_items = reinterpret_cast<WorkItem *>(sp + plan.items);
-    Segment *d_segs = reinterpret_cast<Segment *>(sp + plan.segs);
-    unsigned long long *d_full = reinterpret_cast<unsigned long long *>(sp + plan.full);
-    unsigned long long *d_sub = reinterpret_cast<unsigned long long *>(sp + plan.sub);
-    unsigned long long *d_cnt = reinterpret_cast<unsigned long long *>(sp + plan.cnt);
-    int *d_head = reinterpret_cast<int *>(sp + plan.head);
-    int *d_err = reinterpret_cast<int *>(sp + plan.err);
-    float *d_t1 = reinterpret_cast<float *>(sp + plan.t1);
-    float *d_t2 = reinterpret_cast<float *>(sp + plan.t2);
-    unsigned char *d_l1 = sp + plan.l1;
-    unsigned char *d_l2 = sp + plan.l2;
-
-    cudaStream_t stm = ctx->stream;
-    if (!items.empty()) {
-        TPCF_TRY(cudaMemcpyAsync(d_items, items.data(), sizeof(WorkItem) * items.size(), cudaMemcpyHostToDevice, stm));
-        TPCF_TRY(cudaMemcpyAsync(d_segs, segs.data(), sizeof(Segment) * segs.size(), cudaMemcpyHostToDevice, stm));
-    }
-    TPCF_TRY(cudaMemcpyAsync(d_t1, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
-    if (!bin->t2.empty())
-        TPCF_TRY(cudaMemcpyAsync(d_t2, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(d_l1, luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(d_l2, luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
-    // What the kernel accumulates into starts at zero on every call.
-    TPCF_TRY(cudaMemsetAsync(d_full, 0, sizeof(unsigned long long) * nb, stm));
-    TPCF_TRY(cudaMemsetAsync(d_sub, 0, sizeof(unsigned long long) * (size_t)nb * n_jk, stm));
-    TPCF_TRY(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long) * 4, stm));
-    TPCF_TRY(cudaMemsetAsync(d_head, 0, sizeof(int), stm));
-    TPCF_TRY(cudaMemsetAsync(d_err, 0, sizeof(int), stm));
-
-    KParams P;
-    std::memset(&P, 0, sizeof(P));
-    auto fill = [&](GridK &k, const Grid &gr, const Catalog &c) {
-        k.pos = gr.pos.p;
-        k.aux = gr.aux.p;
-        k.idx = gr.idx.p;
-        k.xyz_s = gr.xyz_s.p;
-        k.unit_s = gr.unit_s.p;
-        k.coord = gr.cell_coord.p;
-        k.kmin0 = gr.kmin[0];
-        k.kmin1 = gr.kmin[1];
-        k.kmin2 = gr.kmin[2];
-        k.xyz = c.xyz.p;
-        k.unit = c.unit.p;
-    };
-    fill(P.a, *ga, *A);
-    fill(P.b, *gb, *B);
-    P.items = d_items;
-    P.segs = d_segs;
-    P.n_items = (int)items.size();
-    P.head = d_head;
-    P.side = side;
-    P.n1 = bin->nb1;
-    P.n2 = bin->mode == MODE_MONOPOLE ? 0 : bin->nb2;
-    P.nb = nb;
-    P.min_r_sq = bin->min_r_sq;
-    P.max_r_sq = bin->max_r_sq;
-    P.g_s2 = g.g_s2;
-    P.g_pi = g.g_pi;
-    P.g_a = g.g_a;
-    P.c1_mu = g.c1_mu;
-    P.c2_mu = g.c2_mu;
-    P.g_mu0 = g.g_mu0;
-    P.s2_lut_min = luts.s2_lut_min;
-    P.lo_cut = bin->min_r_sq - g.g_s2;
-    P.hi_cut = bin->max_r_sq + g.g_s2;
-    P.t1g = d_t1;
-    P.t2g = d_t2;
-    P.lut1g = d_l1;
-    P.lut2g = d_l2;
-    P.lut1_base = luts.base1;
-    P.lut2_scale = luts.scale2;
-    P.g_full = d_full;
-    P.g_sub = d_sub;
-    P.n_jk = n_jk;
-    P.wscale = wscale;
-    P.counters = d_cnt;
-    P.err = d_err;
-
-    KernelFn fn = pick(bin->mode, unitw, jk, req.exact_fp64);
-    TPCF_TRY(cudaFuncSetAttribute((const void *)fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.total));
-    int per_sm = 1;
-    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, L.total));
-    per_sm = std::max(per_sm, 1);
-    if (!items.empty()) {
-        const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)items.size());
-        fn<<<grid, NT, L.total, stm>>>(P);
-        ++ctx->launches;
-        TPCF_TRY(cudaGetLastError());
-    }
-    std::vector<unsigned long long> hf(nb), hs((size_t)nb * n_jk), hc(4);
-    int herr = 0;
-    TPCF_TRY(cudaMemcpyAsync(hf.data(), d_full, sizeof(unsigned long long) * nb, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hs.data(), d_sub, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hc.data(), d_cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(&herr, d_err, sizeof(int), cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaStreamSynchronize(stm));
-    if (herr) {
-        err->status = 4;
-        err->msg = "device wait exceeded its iteration limit; results discarded";
-        return err->status;
-    }
-    const double inv = unitw ? 1.0 : 1.0 / (double)wscale;
-    for (int b = 0; b < nb; ++b) full_out[b] = (double)(long long)hf[b] * inv;
-    if (region_out) {
-        if (jk)
-            for (size_t k = 0; k < hs.size(); ++k) region_out[k] = (double)(long long)hs[k] * inv;
-        else
-            for (int b = 0; b < nb; ++b) region_out[b] = full_out[b];
-    }
-    if (st) {
-        st->candidates += hc[0];
-        st->in_range += hc[1];
-        st->guard += hc[2];
-        st->overflow += hc[3];
-        st->items += items.size();
-    }
-    return 0;
+    unsigned char *p = static_cast<unsigned char *>(base);
+    CountBuffers D;
+    D.items = reinterpret_cast<WorkItem *>(p + o_items);
+    D.segs = reinterpret_cast<Segment *>(p + o_segs);
+    D.full = reinterpret_cast<unsigned long long *>(p + o_full);
+    D.sub = reinterpret_cast<unsigned long long *>(p + o_sub);
+    D.cnt = reinterpret_cast<unsigned long long *>(p + o_cnt);
+    D.head = reinterpret_cast<int *>(p + o_head);
+    D.err = reinterpret_cast<int *>(p + o_err);
+    D.t1 = reinterpret_cast<float *>(p + o_t1);
+    D.t2 = reinterpret_cast<float *>(p + o_t2);
+    D.l1 = p + o_l1;
+    D.l2 = p + o_l2;
+    D.flags = n_flags ? reinterpret_cast<unsigned *>(p + o_flags) : nullptr;
+    D.up_thr = reinterpret_cast<float *>(p + o_up_thr);
+    D.up_bins = reinterpret_cast<double *>(p + o_up_bins);
+    D.up_centre = reinterpret_cast<double *>(p + o_up_centre);
+    return execute(ctx, C, D, full_out, region_out, st, err, false);
 }
 
 }  // namespace tpcf

@@ -119,8 +119,14 @@ __device__ __forceinline__ void acc_add(uint32_t *lo, uint32_t *hi, int i, long 
     if (up) atomicAdd(&hi[i], up);
 }
 
-__device__ __forceinline__ void acc_add_global(unsigned long long *g, size_t i, long long q) {
-    atomicAdd(&g[i], (unsigned long long)q);
+// 128-bit two's-complement accumulation in global memory: g[2i] is the low
+// word, g[2i+1] the high word; v is a signed 64-bit value.  Each atomicAdd
+// returns the low word just before its own add, so the carry it detects is
+// exact under any interleaving.
+__device__ __forceinline__ void acc_add_global(unsigned long long *g, size_t i, unsigned long long v) {
+    const unsigned long long old = atomicAdd(&g[2 * i], v);
+    const unsigned long long up = ((old + v) < old ? 1ull : 0ull) + ((long long)v < 0 ? ~0ull : 0ull);
+    if (up) atomicAdd(&g[2 * i + 1], up);
 }
 
 }  // namespace dev
