@@ -120,7 +120,13 @@ int tpcf_binning_thresholds(const tpcf_binning *bin, int axis, float *out, int c
  *   region_out[n_jk * nb]   per region r: sum over pairs with either end in r
  *                           (JKHists::add_pair, src/hist.cpp:246-260), before
  *                           invert_jk_hists; may be NULL
- * Neither is doubled for auto counts. */
+ * Neither is doubled for auto counts.
+ * Unit-weight counts are exact integers.  Weighted sums add each float pair
+ * weight in fixed point (64-bit in shared memory, 128-bit in global memory)
+ * with resolution 2^-(S+1), S = floor(62 - log2(wmax * P)), wmax a bound on
+ * the pair weights and P the pairs of the largest work item (about 2^24):
+ * every float pair weight of at least 2^(23-S), about wmax * 2^-15, is added
+ * exactly, smaller ones to 2^-(S+1). */
 int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                int precision, double *full_out, double *region_out, tpcf_stats *stats);
 
