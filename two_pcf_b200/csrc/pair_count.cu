@@ -28,6 +28,7 @@
 #include <limits>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "engine.h"
@@ -41,7 +42,9 @@ constexpr int NWARP = NT / 32;
 constexpr int R = 4;           // A points per thread
 constexpr int TA = NT * R;     // A chunk
 constexpr int TB = 256;        // B points per staged tile
-constexpr int QCAP = 32 + 32 * R;  // queue entries per warp: a partial round plus one step's pushes
+constexpr int QPUSH = 2;                 // A slots pushed between two consume checks
+constexpr int QCAP = 32 + 32 * QPUSH;   // queue entries per warp: a partial round plus QPUSH ballots
+static_assert(R % QPUSH == 0, "the push loops consume after every QPUSH A slots");
 constexpr int LUT1_BITS = 8;   // buckets per octave of the float-indexed table
 constexpr int LUT1_OCTAVES = 24;
 constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
@@ -72,6 +75,7 @@ struct KParams {
     double side;
     int n1, n2, nb;
     float min_r_sq, max_r_sq, lo_cut, hi_cut;
+    float cut_mid, cut_half;  // candidate test |s^2 - cut_mid| < cut_half covers [lo_cut, hi_cut]
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
     float s2_lut_min;   // below this s^2 the mu table's guard does not hold
     const float *t1g, *t2g;
@@ -97,7 +101,7 @@ struct KParams {
 };
 
 struct SmemLayout {
-    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, tile0, tile1, misc, total;
+    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, achunk, tile0, tile1, misc, total;
 };
 
 __host__ __device__ inline size_t tile_bytes(bool exact) { return (size_t)TB * (exact ? 64 : 32); }
@@ -126,6 +130,8 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o = (o + 15) / 16 * 16;
     L.queue = o;
     o += (size_t)NWARP * QCAP * 16;
+    L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
+    if (!exact) o += (size_t)TA * 16;
     o = (o + 127) / 128 * 128;
     L.tile0 = o;
     o += tile_bytes(exact);
@@ -360,15 +366,31 @@ __device__ __forceinline__ void add_binned(const KParams &P, uint32_t *s_lo, uin
     dev::acc_add(s_lo, s_hi, bin, q);
 }
 
-// Bin one pair that passed the guard-widened range test, from its FP32 s^2
-// (the squared chord for angular counts), pi and grid-weight product.
-// ia/jb are the pair's positions in the sorted grids (the exact path follows
-// them back to the original arrays); ra/rb the regions of its two points.
+// Bin one pair that passed the guard-widened range test, from its FP32
+// separation in the B cell's frame: s^2 (the squared chord for angular
+// counts), pi from the two unit vectors and the grid-weight product.  The
+// pair's positions in the sorted grids (the exact path follows them back to
+// the original arrays) come from the queue entry; ra/rb are the regions of
+// its two points.
 template <int MODE, bool UNITW, int WK>
 __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
                                          const float *s_t1, const float *s_t2, const unsigned char *s_l1,
-                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi, float s2,
-                                         float pi, float w, int ia, int jb, int ra, int rb, Counters &cnt) {
+                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi,
+                                         const float4 *s_pos, const float4 *s_aux, const float4 *s_achunk,
+                                         const float4 e, int a_start, int jbase, int ra, int rb, Counters &cnt) {
+    // queue entry: (dx, dy, dz, A chunk index << 8 | tile index)
+    const int pk = __float_as_int(e.w);
+    const int ka = pk >> 8, jl = pk & 0xff;
+    const int ia = a_start + ka, jb = jbase + jl;
+    const float dx = e.x, dy = e.y, dz = e.z;
+    const float s2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));  // as in the candidate test
+    const float4 qa = s_achunk[ka];
+    const float w = UNITW ? 1.0f : __fmul_rn(qa.w, s_pos[jl].w);
+    float pi = 0.f;
+    if constexpr (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU) {
+        const float4 ab = s_aux[jl];
+        pi = 0.5f * fmaf(dz, qa.z + ab.z, fmaf(dy, qa.y + ab.y, dx * (qa.x + ab.x)));
+    }
     int bin;
     bool amb;
     if constexpr (MODE == MODE_ANGULAR) {
@@ -497,7 +519,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     float *s_t2 = (float *)(smem + L.t2);
     unsigned char *s_l1 = smem + L.lut1;
     unsigned char *s_l2 = smem + L.lut2;
-    unsigned char *tiles[2] = {smem + L.tile0, smem + L.tile1};
+    unsigned char *const tile_base = smem + L.tile0;
+    const size_t tile_stride = L.tile1 - L.tile0;
+    float4 *s_achunk = (float4 *)(smem + L.achunk);
     int *s_item = (int *)(smem + L.misc);
     uint64_t *bar = (uint64_t *)(smem + L.misc + 16);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -530,7 +554,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     unsigned tcount = 0;  // tiles staged so far by this CTA (selects buffer and phase)
 
     auto issue = [&](unsigned tc, int start, int len) {
-        unsigned char *dst = tiles[tc & 1];
+        unsigned char *dst = tile_base + (tc & 1) * tile_stride;
         dev::fence_proxy_async();
         if (EXACT) {
             const uint32_t by = (uint32_t)len * 32u;
@@ -588,6 +612,21 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             }
         }
 
+        if (!EXACT) {
+            // unit vector and weight of every A point of the chunk, read by the
+            // consume step (pi, pair weight) at full warp occupancy
+            for (int k = tid; k < it.a_len; k += NT) {
+                const int gi = it.a_start + k;
+                const float wk = P.a.pos[gi].w;
+                if (kNeedAux) {
+                    const float4 q = P.a.aux[gi];
+                    s_achunk[k] = make_float4(q.x, q.y, q.z, wk);
+                } else {
+                    s_achunk[k] = make_float4(0.f, 0.f, 0.f, wk);
+                }
+            }
+            __syncthreads();
+        }
         if (tid == 0) {
             const Segment s0 = P.segs[it.seg_begin];
             issue(tcount, s0.b_start, min(TB, s0.b_len));
@@ -605,24 +644,17 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             const float offx = (float)((double)((P.a.kmin0 + ca.x) - (P.b.kmin0 + cb.x)) * P.side);
             const float offy = (float)((double)((P.a.kmin1 + ca.y) - (P.b.kmin1 + cb.y)) * P.side);
             const float offz = (float)((double)((P.a.kmin2 + ca.z) - (P.b.kmin2 + cb.z)) * P.side);
-            float ax[R], ay[R], az[R], aw[R], anx[R], any_[R], anz[R];
+            float ax[R], ay[R], az[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
+                // slots without a point sit far away: their s^2 overflows to
+                // +inf and never passes the candidate test
                 ax[r] = ay[r] = az[r] = 1e30f;
-                aw[r] = 0.0f;
-                anx[r] = any_[r] = anz[r] = 0.0f;
                 if (!EXACT && ai[r] != 0x7fffffff) {
                     const float4 p = P.a.pos[ai[r]];
                     ax[r] = p.x + offx;
                     ay[r] = p.y + offy;
                     az[r] = p.z + offz;
-                    aw[r] = p.w;
-                    if (kNeedAux) {
-                        const float4 q = P.a.aux[ai[r]];
-                        anx[r] = q.x;
-                        any_[r] = q.y;
-                        anz[r] = q.z;
-                    }
                 }
             }
             const int ntiles = (sg.b_len + TB - 1) / TB;
@@ -647,7 +679,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                 // queued the whole warp bins them (no divergent binning).
                 int qn = 0;  // queued entries of this warp (warp-uniform)
                 if (EXACT) {
-                    const double4 *s_xyz = (const double4 *)tiles[tcount & 1];
+                    const double4 *s_xyz = (const double4 *)(tile_base + (tcount & 1) * tile_stride);
                     for (int m = 0; m < nsteps; ++m) {
                         const int jj = grp + m * Pn;
                         const bool jv = thr_on && jj < tlen;
@@ -672,22 +704,26 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                             }
                         }
 #pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
-                            if (hit[r])
-                                s_q[qn + __popc(bal & lt_mask)] =
-                                    make_float4(d0[r], d1[r], d2[r], __int_as_float(apack[r] | jj));
-                            qn += __popc(bal);
-                        }
-                        while (qn >= 32) {
-                            __syncwarp();
-                            const float4 e = s_q[qn - 32 + lane];
-                            const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
-                                                       it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region, rb,
-                                                       cnt);
-                            __syncwarp();
-                            qn -= 32;
+                        for (int r0 = 0; r0 < R; r0 += QPUSH) {
+                            // at most 31 + 32 * QPUSH entries: within QCAP
+#pragma unroll
+                            for (int r = r0; r < r0 + QPUSH; ++r) {
+                                const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+                                if (hit[r])
+                                    s_q[qn + __popc(bal & lt_mask)] =
+                                        make_float4(d0[r], d1[r], d2[r], __int_as_float(apack[r] | jj));
+                                qn += __popc(bal);
+                            }
+                            while (qn >= 32) {
+                                __syncwarp();
+                                const float4 e = s_q[qn - 32 + lane];
+                                const int pk = __float_as_int(e.w);
+                                bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
+                                                           it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
+                                                           rb, cnt);
+                                __syncwarp();
+                                qn -= 32;
+                            }
                         }
                     }
                     if (qn > 0) {
@@ -702,61 +738,62 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         __syncwarp();
                     }
                 } else {
-                    const float4 *s_pos = (const float4 *)tiles[tcount & 1];
-                    const float4 *s_aux = (const float4 *)(tiles[tcount & 1] + (size_t)TB * 16);
-                    for (int m = 0; m < nsteps; ++m) {
-                        const int jj = grp + m * Pn;
-                        const int jc = min(jj, tlen - 1);
-                        const bool jv = thr_on && jj < tlen;
-                        const float4 pb = s_pos[jc];
-                        const int jg = jbase + jj;
-                        float s2[R], dx[R], dy[R], dz[R];
-                        bool hit[R];
+                    const unsigned char *tile = tile_base + (tcount & 1) * tile_stride;
+                    const float4 *s_pos = (const float4 *)tile;
+                    const float4 *s_aux = (const float4 *)(tile + (size_t)TB * 16);
+                    // Candidates: (dx, dy, dz) of the pair in the segment's cell
+                    // frame; those inside the guard-widened range are pushed
+                    // into the warp's queue with a ballot, and each time 32 are
+                    // queued the whole warp bins them (pi, weight, tables) at
+                    // full occupancy.  Self segments (auto counts) keep j > i.
+                    auto run = [&](auto self_c) {
+                        constexpr bool SELF = decltype(self_c)::value;
+                        for (int m = 0; m < nsteps; ++m) {
+                            const int jj = grp + m * Pn;
+                            const float4 pb = s_pos[min(jj, tlen - 1)];
+                            const bool jv = jj < tlen;
+                            const int jg = jbase + jj;
+                            float dx[R], dy[R], dz[R];
+                            bool hit[R];
 #pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            dx[r] = ax[r] - pb.x;
-                            dy[r] = ay[r] - pb.y;
-                            dz[r] = az[r] - pb.z;
-                            s2[r] = fmaf(dz[r], dz[r], fmaf(dy[r], dy[r], dx[r] * dx[r]));
-                            hit[r] = jv && (s2[r] < P.hi_cut) && (s2[r] > P.lo_cut) && (!self || jg > ai[r]);
-                        }
-                        float4 ab = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (kNeedAux) ab = s_aux[jc];
-#pragma unroll
-                        for (int r = 0; r < R; ++r) {
-                            const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
-                            if (hit[r]) {
-                                float pi = 0.f;
-                                if (kNeedAux)
-                                    pi = 0.5f * fmaf(dz[r], anz[r] + ab.z,
-                                                     fmaf(dy[r], any_[r] + ab.y, dx[r] * (anx[r] + ab.x)));
-                                const float w = UNITW ? 1.0f : __fmul_rn(aw[r], pb.w);
-                                s_q[qn + __popc(bal & lt_mask)] =
-                                    make_float4(s2[r], pi, w, __int_as_float(apack[r] | jj));
+                            for (int r = 0; r < R; ++r) {
+                                dx[r] = ax[r] - pb.x;
+                                dy[r] = ay[r] - pb.y;
+                                dz[r] = az[r] - pb.z;
+                                const float s2 = fmaf(dz[r], dz[r], fmaf(dy[r], dy[r], dx[r] * dx[r]));
+                                hit[r] = jv && fabsf(s2 - P.cut_mid) < P.cut_half;
+                                if (SELF) hit[r] = hit[r] && jg > ai[r];
                             }
-                            qn += __popc(bal);
+#pragma unroll
+                            for (int r0 = 0; r0 < R; r0 += QPUSH) {
+#pragma unroll
+                                for (int r = r0; r < r0 + QPUSH; ++r) {
+                                    const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+                                    if (hit[r])
+                                        s_q[qn + __popc(bal & lt_mask)] =
+                                            make_float4(dx[r], dy[r], dz[r], __int_as_float(apack[r] | jj));
+                                    qn += __popc(bal);
+                                }
+                                while (qn >= 32) {
+                                    __syncwarp();
+                                    const float4 e = s_q[qn - 32 + lane];
+                                    bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, s_pos,
+                                                              s_aux, s_achunk, e, it.a_start, jbase, it.a_region, rb,
+                                                              cnt);
+                                    __syncwarp();
+                                    qn -= 32;
+                                }
+                            }
                         }
-                        while (qn >= 32) {
-                            __syncwarp();
-                            const float4 e = s_q[qn - 32 + lane];
-                            const int pk = __float_as_int(e.w);
-                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y,
-                                                      e.z, it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
-                                                      rb, cnt);
-                            __syncwarp();
-                            qn -= 32;
-                        }
-                    }
+                    };
+                    if (self) run(std::true_type{});
+                    else run(std::false_type{});
                     // drain: the queued entries refer to this tile's positions
                     if (qn > 0) {
                         __syncwarp();
-                        if (lane < qn) {
-                            const float4 e = s_q[lane];
-                            const int pk = __float_as_int(e.w);
-                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, e.x, e.y,
-                                                      e.z, it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
-                                                      rb, cnt);
-                        }
+                        if (lane < qn)
+                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, s_pos, s_aux,
+                                                      s_achunk, s_q[lane], it.a_start, jbase, it.a_region, rb, cnt);
                         __syncwarp();
                     }
                 }
@@ -1341,6 +1378,11 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         P.lo_cut = bin->min_r_sq - g.g_s2;
         P.hi_cut = bin->max_r_sq + g.g_s2;
     }
+    // One compare: |s^2 - mid| < half, widened to cover the float rounding of
+    // mid, half and the subtraction.
+    P.cut_mid = (float)(0.5 * ((double)P.lo_cut + (double)P.hi_cut));
+    P.cut_half = (float)(0.5 * ((double)P.hi_cut - (double)P.lo_cut) * (1.0 + 1e-5) +
+                         1e-6 * std::fabs((double)P.cut_mid));
     P.lut1_base = C.luts.base1;
     P.lut2_scale = C.luts.scale2;
     P.n_jk = C.n_jk;
