@@ -58,6 +58,8 @@ def lib():
         L.orc_count_3d.argtypes = [C.c_int, C.c_int, C.POINTER(OrcCat), C.POINTER(OrcCat), C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_int, C.POINTER(OrcUpweight), C.c_int,
                                    C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_count_backward.argtypes = [C.c_int, C.c_int, C.POINTER(OrcCat), C.POINTER(OrcCat), C.c_void_p,
+                                         C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_count_angular.argtypes = [C.c_int, C.POINTER(OrcCat), C.POINTER(OrcCat), C.c_int, C.c_double,
                                         C.c_int, C.c_double, C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.orc_normalise_auto.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
@@ -149,3 +151,17 @@ def count_angular(kind, a: Cat, b: Cat | None, *, n_jk, theta_max, n_theta, thet
     lib().orc_count_angular(kind, C.byref(a.c), C.byref(bc), n_jk, theta_max, n_theta, theta_log_base, n_runs,
                             n_threads, full.ctypes.data, sub.ctypes.data)
     return full, sub.reshape(n_jk, n_theta)
+
+
+def count_backward(mode, a: Cat, b: Cat | None, *, is_auto, axes, G, n_threads=0):
+    """FP64 CPU adjoint of a plain-weight 3-D count: per-object dL/dw for
+    G = dL/d(raw full histogram, unordered pairs).  Returns (grad_a, grad_b)."""
+    min1, max1, base1, nb1, min2, max2, base2, nb2 = axes
+    axp = np.array([min1, max1, base1, min2, max2, base2], np.float64)
+    G = np.ascontiguousarray(G, np.float64)
+    ga = np.zeros(a.c.n)
+    gb = np.zeros(b.c.n if b is not None else 1)
+    bc = b.c if b is not None else a.c
+    lib().orc_count_backward(mode, int(is_auto), C.byref(a.c), C.byref(bc), axp.ctypes.data, nb1, nb2,
+                             G.ctypes.data, n_threads, ga.ctypes.data, gb.ctypes.data)
+    return ga, (None if is_auto else gb)

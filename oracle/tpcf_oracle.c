@@ -198,6 +198,15 @@ typedef struct {
     int n_runs;
 } orc_setup;
 
+/* Per-thread accumulators of a pair loop: histograms (full[nb], sub[n_jk*nb])
+ * for counts; per-object gradients ga[n_a], gb[n_b] and the per-bin
+ * derivative G[nb] for the adjoint. */
+typedef struct {
+    double *full, *sub;
+    double *ga, *gb;
+    const double *G;
+} orc_acc;
+
 static inline void add_pair(const orc_setup *s, double *full, double *sub, int jk1, int jk2, int b, float w) {
     full[b] += w;
     sub[(size_t)jk1 * s->nb + b] += w;
@@ -220,15 +229,14 @@ static inline double one_minus_cos(const double *n1, const double *n2) {
     return v;
 }
 
-/* One candidate pair (i from catalogue a, j from catalogue b). */
-static inline void eval_pair(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, double *full,
-                             double *sub) {
+/* One candidate pair (i from catalogue a, j from catalogue b): the flat bin
+ * it is added to, or -1, and its weight. */
+static inline int pair_bin_3d(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, float *w_out) {
     const double *x1 = a->xyz + 3 * (size_t)i, *x2 = b->xyz + 3 * (size_t)j;
     float d[3];
     for (int m = 0; m < 3; ++m) d[m] = (float)(x1[m] - x2[m]);
     float s2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
-    if (!(s2 < s->max_r_sq && s2 > s->min_r_sq)) return;
-    int jk1 = a->jk ? a->jk[i] : 0, jk2 = b->jk ? b->jk[j] : 0;
+    if (!(s2 < s->max_r_sq && s2 > s->min_r_sq)) return -1;
     float w1 = a->w ? a->w[i] : 1.0f, w2 = b->w ? b->w[j] : 1.0f;
     const double *n1 = a->unit + 3 * (size_t)i, *n2 = b->unit + 3 * (size_t)j;
 
@@ -248,10 +256,10 @@ static inline void eval_pair(const orc_setup *s, const orc_cat *a, int i, const 
         weight = (float)((double)(w1 * w2) * orc_interp(s->up, omct));
     }
 
+    *w_out = weight;
     if (s->mode == ORC_MONOPOLE) {
         int bin = orc_to_int(orc_axis_bin_num(&s->ax1, sqrtf(s2)));
-        if (bin < s->ax1.n_bins && bin >= 0) add_pair(s, full, sub, jk1, jk2, bin, weight);
-        return;
+        return (bin < s->ax1.n_bins && bin >= 0) ? bin : -1;
     }
     /* pi, _ANGULAR_PI_DEFN (src/correlators.cpp:166-170) */
     float pi = (float)((double)d[0] * (n1[0] + n2[0]));
@@ -270,8 +278,27 @@ static inline void eval_pair(const orc_setup *s, const orc_cat *a, int i, const 
     int b1 = orc_to_int(orc_axis_bin_num(&s->ax1, v1));
     if (b1 < s->ax1.n_bins && b1 >= 0) {
         int b2 = orc_to_int(orc_axis_bin_num(&s->ax2, v2));
-        if (b2 < s->ax2.n_bins && b2 >= 0) add_pair(s, full, sub, jk1, jk2, b1 * s->ax2.n_bins + b2, weight);
+        if (b2 < s->ax2.n_bins && b2 >= 0) return b1 * s->ax2.n_bins + b2;
     }
+    return -1;
+}
+
+static void eval_pair(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, orc_acc *acc) {
+    float w;
+    int bin = pair_bin_3d(s, a, i, b, j, &w);
+    if (bin < 0) return;
+    add_pair(s, acc->full, acc->sub, a->jk ? a->jk[i] : 0, b->jk ? b->jk[j] : 0, bin, w);
+}
+
+/* Adjoint of one pair of a plain-weight count: the pair adds w_i w_j to its
+ * bin, so dL/dw_i += G[bin] w_j and dL/dw_j += G[bin] w_i. */
+static void eval_pair_grad(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, orc_acc *acc) {
+    float w;
+    int bin = pair_bin_3d(s, a, i, b, j, &w);
+    if (bin < 0) return;
+    const double w1 = a->w ? a->w[i] : 1.0f, w2 = b->w ? b->w[j] : 1.0f;
+    acc->ga[i] += acc->G[bin] * w2;
+    acc->gb[j] += acc->G[bin] * w1;
 }
 
 static void setup_3d(orc_setup *s, int mode, const double axp[6], int nb1, int nb2, int n_jk) {
@@ -311,11 +338,13 @@ static void finish(const orc_setup *s, int is_auto, double *full, double *sub) {
 
 /* Pair loop over a uniform grid of the given side.  "pts" are the positions
  * the grid is built from (xyz for 3-D, x_norm for angular counts). */
-typedef void (*orc_eval_fn)(const orc_setup *, const orc_cat *, int, const orc_cat *, int, double *, double *);
+typedef void (*orc_eval_fn)(const orc_setup *, const orc_cat *, int, const orc_cat *, int, orc_acc *);
 
+/* out: the accumulators the per-thread ones are added into; histograms
+ * always, gradients (indexed by catalogue index) when out->ga is set. */
 static void pair_loop(const orc_setup *s, int is_auto, const orc_cat *a, const int *pa, int na, const orc_cat *b,
                       const int *pb, int nb_pts, int use_unit, double side, orc_eval_fn fn, int n_threads,
-                      double *full, double *sub) {
+                      orc_acc *out) {
     const double *ptsa = use_unit ? a->unit : a->xyz;
     const double *ptsb = use_unit ? b->unit : b->xyz;
     double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
@@ -348,7 +377,11 @@ static void pair_loop(const orc_setup *s, int is_auto, const orc_cat *a, const i
 #pragma omp parallel num_threads(n_threads)
     {
         double *h = (double *)calloc(hsz, sizeof(double));
-        double *hf = h, *hs = h + s->nb;
+        orc_acc acc = {h, h + s->nb, NULL, NULL, out->G};
+        if (out->ga) {
+            acc.ga = (double *)calloc((size_t)(a->n > 0 ? a->n : 1), sizeof(double));
+            acc.gb = is_auto ? acc.ga : (double *)calloc((size_t)(b->n > 0 ? b->n : 1), sizeof(double));
+        }
 #pragma omp for schedule(dynamic)
         for (long long c = 0; c < ncell; ++c) {
             int cx = (int)(c / ((long long)dim[1] * dim[2])), cy = (int)((c / dim[2]) % dim[1]), cz = (int)(c % dim[2]);
@@ -363,17 +396,26 @@ static void pair_loop(const orc_setup *s, int is_auto, const orc_cat *a, const i
                             if (is_auto && c2 < c) continue;
                             for (int j0 = g2->start[c2]; j0 < g2->start[c2 + 1]; ++j0) {
                                 if (is_auto && c2 == c && j0 <= i0) continue;
-                                fn(s, a, i, b, g2->idx[j0], hf, hs);
+                                fn(s, a, i, b, g2->idx[j0], &acc);
                             }
                         }
             }
         }
 #pragma omp critical
         {
-            for (size_t k = 0; k < (size_t)s->nb; ++k) full[k] += hf[k];
-            for (size_t k = 0; k < (size_t)s->nb * s->n_jk; ++k) sub[k] += hs[k];
+            for (size_t k = 0; k < (size_t)s->nb; ++k) out->full[k] += acc.full[k];
+            for (size_t k = 0; k < (size_t)s->nb * s->n_jk; ++k) out->sub[k] += acc.sub[k];
+            if (out->ga) {
+                for (int k = 0; k < a->n; ++k) out->ga[k] += acc.ga[k];
+                if (!is_auto)
+                    for (int k = 0; k < b->n; ++k) out->gb[k] += acc.gb[k];
+            }
         }
         free(h);
+        if (out->ga) {
+            free(acc.ga);
+            if (!is_auto) free(acc.gb);
+        }
     }
     grid_free(&ga);
     if (!is_auto) grid_free(&gb);
@@ -410,11 +452,44 @@ int orc_count_3d(int mode, int is_auto, const orc_cat *a, const orc_cat *b, int 
      * sqrt(max_r_sq) * (1 + 2^-22); the extra margin absorbs the rounding of
      * the cell-index division. */
     double side = sqrt((double)s.max_r_sq) * (1.0 + 1e-5) + 1e-12;
-    pair_loop(&s, is_auto, a, pa, na, is_auto ? a : b, is_auto ? pa : pb, nbp, 0, side, eval_pair, n_threads, full,
-              sub);
+    orc_acc out = {full, sub, NULL, NULL, NULL};
+    pair_loop(&s, is_auto, a, pa, na, is_auto ? a : b, is_auto ? pa : pb, nbp, 0, side, eval_pair, n_threads, &out);
     finish(&s, is_auto, full, sub);
     free(pa);
     free(pb);
+    return 0;
+}
+
+/* Adjoint of a plain-weight 3-D count (the FP64 CPU gradient of the weight
+ * derivative): with G[nb] = dL/d(raw full histogram) — the unordered-pair
+ * sums before the auto-count doubling — grad_a[i] = sum over the pairs (i, j)
+ * in a binned range of G[bin] * w_j, and grad_b likewise for catalogue b
+ * (auto: every pair adds to both ends in grad_a).  Arrays are indexed by
+ * catalogue index; points dropped by the d_comov partition get 0. */
+int orc_count_backward(int mode, int is_auto, const orc_cat *a, const orc_cat *b, const double axp[6], int nb1,
+                       int nb2, const double *G, int n_threads, double *grad_a, double *grad_b) {
+    orc_setup s;
+    setup_3d(&s, mode, axp, nb1, nb2, 1);
+    s.weight_kind = ORC_W_PLAIN;
+    double *full = (double *)calloc((size_t)s.nb, sizeof(double));
+    double *sub = (double *)calloc((size_t)s.nb, sizeof(double));
+    memset(grad_a, 0, sizeof(double) * (size_t)a->n);
+    if (!is_auto) memset(grad_b, 0, sizeof(double) * (size_t)b->n);
+    int *pa = (int *)malloc(sizeof(int) * (size_t)(a->n > 0 ? a->n : 1));
+    int na = orc_partition(a->dcom, a->n, pa);
+    int *pb = NULL, nbp = 0;
+    if (!is_auto) {
+        pb = (int *)malloc(sizeof(int) * (size_t)(b->n > 0 ? b->n : 1));
+        nbp = orc_partition(b->dcom, b->n, pb);
+    }
+    double side = sqrt((double)s.max_r_sq) * (1.0 + 1e-5) + 1e-12;
+    orc_acc out = {full, sub, grad_a, is_auto ? grad_a : grad_b, G};
+    pair_loop(&s, is_auto, a, pa, na, is_auto ? a : b, is_auto ? pa : pb, nbp, 0, side, eval_pair_grad, n_threads,
+              &out);
+    free(pa);
+    free(pb);
+    free(full);
+    free(sub);
     return 0;
 }
 
@@ -425,8 +500,7 @@ typedef struct {
     int kind;
 } orc_ang_setup;
 
-static void eval_angular(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, double *full,
-                         double *sub) {
+static void eval_angular(const orc_setup *s, const orc_cat *a, int i, const orc_cat *b, int j, orc_acc *acc) {
     const orc_ang_setup *as = (const orc_ang_setup *)s;
     const double *n1 = a->unit + 3 * (size_t)i, *n2 = b->unit + 3 * (size_t)j;
     double omct = one_minus_cos(n1, n2);
@@ -451,7 +525,7 @@ static void eval_angular(const orc_setup *s, const orc_cat *a, int i, const orc_
     }
     /* JKHists::add_pair takes the value as float (src/hist.cpp:246). */
     int bin = orc_to_int(orc_axis_bin_num(&s->ax1, (float)omct));
-    if (bin < s->ax1.n_bins && bin >= 0) add_pair(s, full, sub, jk1, jk2, bin, weight);
+    if (bin < s->ax1.n_bins && bin >= 0) add_pair(s, acc->full, acc->sub, jk1, jk2, bin, weight);
 }
 
 /* Angular count.  kind 0 = DD (all points), 1 = DD with inverse-p weights
@@ -483,8 +557,8 @@ int orc_count_angular(int kind, const orc_cat *a, const orc_cat *b, int n_jk, do
      * rounding, so unit vectors closer than sqrt(2 * 1.5 * max) in chord
      * include them all. */
     double side = sqrt(3.0 * (double)s->ax1.max) + 1e-9;
-    pair_loop(s, is_auto, a, pa, na, is_auto ? a : b, is_auto ? pa : pb, nbp, 1, side, eval_angular, n_threads, full,
-              sub);
+    orc_acc out = {full, sub, NULL, NULL, NULL};
+    pair_loop(s, is_auto, a, pa, na, is_auto ? a : b, is_auto ? pa : pb, nbp, 1, side, eval_angular, n_threads, &out);
     finish(s, is_auto, full, sub);
     free(pa);
     free(pb);

@@ -51,6 +51,12 @@ constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
 constexpr int LUT2_N = 4096;
 constexpr unsigned char LUT_INV = 254;  // every value of the bucket is dropped
 constexpr unsigned char LUT_AMB = 255;  // bucket within the guard of an edge
+// Edge-coded tables (axes of at most 126 bins): LUT_EDGE + k marks a bucket
+// whose guarded range holds exactly one threshold, T[k + 1], with bin k below
+// it and bin k + 1 above; the kernel compares the value with T[k + 1] and
+// only a value within its guard of it needs the exact path.
+constexpr unsigned char LUT_EDGE = 128;
+constexpr int kLutEdgeMaxBins = 126;
 constexpr uint32_t kWaitLimit = 1u << 22;
 constexpr long long kItemMaxB = 16384;  // B points per work item (load balance)
 
@@ -78,6 +84,7 @@ struct KParams {
     float cut_mid, cut_half;  // candidate test |s^2 - cut_mid| < cut_half covers [lo_cut, hi_cut]
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
     float s2_lut_min;   // below this s^2 the mu table's guard does not hold
+    int lut_edge1, lut_edge2;  // tables carry LUT_EDGE codes
     const float *t1g, *t2g;
     const unsigned char *lut1g, *lut2g;
     unsigned lut1_base;  // (bits of the lowest bucket) >> (23 - LUT1_BITS)
@@ -298,6 +305,20 @@ struct Counters {
     unsigned in_range = 0, guard = 0;  // per thread, folded into 64-bit totals per item
 };
 
+// Table entry -> bin for value x: a plain bin, LUT_INV (returned as is), or
+// for an edge-coded bucket the side of its threshold; *amb is set when x is
+// within its guard g of that threshold (or the bucket is ambiguous).
+__device__ __forceinline__ unsigned lut_decode(unsigned c, float x, const float *t, float g, int edge, bool *amb) {
+    *amb = (c == LUT_AMB);
+    if (edge && c >= LUT_EDGE && c < LUT_INV) {
+        const unsigned k = c - LUT_EDGE;
+        const float tk = t[k + 1];
+        *amb = fabsf(x - tk) <= g;
+        return k + (x >= tk ? 1u : 0u);
+    }
+    return c;
+}
+
 // JKHists::interp (src/hist.cpp:369-391) of the angular up-weight at
 // v = 1 - cos(theta): the interval comes from the host-built thresholds on
 // (float)v (the reference's bin_num runs on glibc log1pf), the
@@ -396,9 +417,10 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
     if constexpr (MODE == MODE_ANGULAR) {
         // v = |n1 - n2|^2 / 2 approximates 1 - cos(theta) within g_ang
         const float v = 0.5f * s2;
-        const unsigned c1 = s_l1[lut1_index(P.lut1_base, v)];
+        bool amb1;
+        const unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, v)], v, s_t1, P.g_ang, P.lut_edge1, &amb1);
         if (c1 == LUT_INV) return;
-        if (c1 != LUT_AMB) {
+        if (!amb1) {
             cnt.in_range += 1;
             bin = (int)c1;
         } else {
@@ -422,34 +444,45 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return;  // certainly out of range
             amb = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
             const float a = fmaf(-pi, pi, s2);
-            unsigned c1 = (a <= P.g_a) ? LUT_AMB : s_l1[lut1_index(P.lut1_base, a)];
-            if (a < -P.g_a) c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
-            const unsigned c2 = s_l2[lut2_index(P.lut2_scale, fabsf(pi))];
-            if (!amb && (c1 == LUT_INV || c2 == LUT_INV)) {
+            const float api = fabsf(pi);
+            bool amb1, amb2;
+            unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, a)], a, s_t1, P.g_a, P.lut_edge1, &amb1);
+            if (a <= P.g_a) {
+                c1 = LUT_AMB;
+                amb1 = true;
+            }
+            if (a < -P.g_a) {
+                c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
+                amb1 = false;
+            }
+            const unsigned c2 = lut_decode(s_l2[lut2_index(P.lut2_scale, api)], api, s_t2, P.g_pi, P.lut_edge2, &amb2);
+            if (!amb && ((c1 == LUT_INV && !amb1) || (c2 == LUT_INV && !amb2))) {
                 cnt.in_range += 1;
                 return;
             }
-            amb = amb || c1 >= LUT_INV || c2 >= LUT_INV;
+            amb = amb || amb1 || amb2 || c1 == LUT_INV || c2 == LUT_INV;
             if (!amb) cnt.in_range += 1;
             bin = (int)(c1 * P.n2 + c2);
         } else {
-            const unsigned c1 = s_l1[lut1_index(P.lut1_base, s2)];
+            const unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, s2)], s2, s_t1, P.g_s2, P.lut_edge1, &amb);
             if (c1 == LUT_INV) {
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
                 cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
                 return;
             }
-            amb = (c1 == LUT_AMB);
             unsigned c2 = 0;
             if (MODE == MODE_S_MU) {
-                const float mu = fabsf(pi) * rsqrtf(s2);
-                c2 = s_l2[lut2_index(P.lut2_scale, mu)];
-                if (c2 == LUT_INV && !amb && s2 >= P.s2_lut_min) {
+                const float inv_s = rsqrtf(s2);
+                const float mu = fabsf(pi) * inv_s;
+                const float gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
+                bool amb2;
+                c2 = lut_decode(s_l2[lut2_index(P.lut2_scale, mu)], mu, s_t2, gmu, P.lut_edge2, &amb2);
+                if (c2 == LUT_INV && !amb2 && !amb && s2 >= P.s2_lut_min) {
                     cnt.in_range += 1;
                     return;
                 }
-                amb = amb || c2 >= LUT_INV || s2 < P.s2_lut_min;
+                amb = amb || amb2 || c2 == LUT_INV || s2 < P.s2_lut_min;
             }
             if (!amb) cnt.in_range += 1;
             bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
@@ -962,13 +995,29 @@ struct Category {
 
 // Table entry for values in [v0, v1]: the category when every value within
 // g of the interval shares it, else ambiguous.
-unsigned char lut_entry(const Category &cat, const std::vector<double> &edges, double v0, double v1, double g) {
+unsigned char lut_entry(const Category &cat, const std::vector<double> &edges, double v0, double v1, double g,
+                        bool edge_code = false) {
     const double lo = v0 - g, hi = v1 + g;
+    int n_in = 0;
+    double e_in = 0;
     for (double e : edges)
-        if (e > lo && e <= hi) return LUT_AMB;
-    const int c = cat(0.5 * (v0 + v1));
-    if (c != cat(lo) || c != cat(hi)) return LUT_AMB;
-    return c < 0 ? LUT_INV : (unsigned char)c;
+        if (e > lo && e <= hi && (n_in == 0 || e != e_in)) {
+            ++n_in;
+            e_in = e;
+        }
+    if (n_in == 0) {
+        const int c = cat(0.5 * (v0 + v1));
+        if (c != cat(lo) || c != cat(hi)) return LUT_AMB;
+        return c < 0 ? LUT_INV : (unsigned char)c;
+    }
+    if (edge_code && n_in == 1) {
+        // one threshold inside: bin k below it, k + 1 above
+        const int k = cat(lo);
+        if (k >= 0 && k + 1 < cat.n && cat(hi) == k + 1 && (double)(*cat.t)[k + 1] == e_in &&
+            k < kLutEdgeMaxBins)
+            return (unsigned char)(LUT_EDGE + k);
+    }
+    return LUT_AMB;
 }
 
 }  // namespace
@@ -1118,6 +1167,7 @@ Guards compute_guards(double side, int m, double rb) {
 // Host-built binning tables for one binning and one set of guards.
 struct Luts {
     std::vector<unsigned char> l1, l2;
+    bool edge1 = false, edge2 = false;  // edge-coded tables (LUT_EDGE)
     unsigned base1 = 0;
     float scale2 = 0;
     float s2_lut_min = 0;
@@ -1143,10 +1193,11 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     const uint32_t sh = 23 - LUT1_BITS;
     L.base1 = bits_of(std::ldexp(1.0f, elo)) >> sh;
     const double g1 = s_axis ? g.g_s2 : (bin.mode == MODE_ANGULAR ? g.g_ang : g.g_a);
+    L.edge1 = bin.nb1 <= kLutEdgeMaxBins;
     for (int i = 1; i < LUT1_N - 1; ++i) {
         const double v0 = f_from_bits((L.base1 + i) << sh);
         const double v1 = f_from_bits((L.base1 + i + 1) << sh);
-        L.l1[i] = lut_entry(c1, e1, v0, v1, g1);
+        L.l1[i] = lut_entry(c1, e1, v0, v1, g1, L.edge1);
     }
     // Bucket 0 holds everything below the table (ambiguous); the last bucket
     // holds everything above it.
@@ -1173,10 +1224,11 @@ Luts build_luts(const Binning &bin, const Guards &g) {
             g2 = g.g_pi;
         }
         const double w = 1.0 / L.scale2;
+        L.edge2 = bin.nb2 <= kLutEdgeMaxBins;
         for (int i = 0; i < LUT2_N - 1; ++i) {
             const double v0 = i * w, v1 = (i + 1) * w;
             const double slack = 4.0 * std::ldexp(1.0, -23) * v1;  // bucket-edge rounding of (int)(x * scale)
-            L.l2[i] = lut_entry(c2, e2, v0, v1, g2 + slack);
+            L.l2[i] = lut_entry(c2, e2, v0, v1, g2 + slack, L.edge2);
         }
         const double vlast = (LUT2_N - 1) * w;
         if (c2(vlast - g2) < 0 && vlast - g2 > bin.t2[bin.nb2]) L.l2[LUT2_N - 1] = LUT_INV;
@@ -1384,6 +1436,8 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     P.cut_half = (float)(0.5 * ((double)P.hi_cut - (double)P.lo_cut) * (1.0 + 1e-5) +
                          1e-6 * std::fabs((double)P.cut_mid));
     P.lut1_base = C.luts.base1;
+    P.lut_edge1 = C.luts.edge1 ? 1 : 0;
+    P.lut_edge2 = C.luts.edge2 ? 1 : 0;
     P.lut2_scale = C.luts.scale2;
     P.n_jk = C.n_jk;
     P.wscale = wscale;
