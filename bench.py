@@ -52,7 +52,23 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--one-count", choices=["s_mu", "sigma_pi"], default=None,
+                   help="profiling case: one RR count of the workload's randoms at --scale, then exit")
     return p.parse_args()
+
+
+def one_count(args):
+    """A single FP32+guard RR count (weighted, jackknife) of the step's
+    randoms: the case the committed ncu summaries profile."""
+    import two_pcf_b200 as tp
+    w = make_workload(2, args.scale)
+    r = w["rand"]
+    ctx = tp.Context(0)
+    R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
+    axes = S_MU_AXES if args.one_count == "s_mu" else SIGMA_PI_AXES
+    b = tp.Binning(ctx, tp.S_MU if args.one_count == "s_mu" else tp.SIGMA_PI, *axes, w["n_jk"])
+    full, _, st = tp.count(ctx, R, None, b, tp.FP32_GUARD)
+    print(json.dumps({"one_count": args.one_count, "scale": args.scale, **st}))
 
 
 def dist_setup():
@@ -257,6 +273,9 @@ def run_reference_arm(args, ws, rank):
 
 def main():
     args = parse()
+    if args.one_count:
+        one_count(args)
+        return
     ws, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
