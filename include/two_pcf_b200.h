@@ -178,6 +178,22 @@ int tpcf_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog
 int tpcf_pair_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                              const tpcf_weight_spec *spec, int precision, double *full_hist, double *sub_hist,
                              tpcf_stats *stats);
+/* Adjoint of a plain-weight 3-D count (no counterpart in the reference; the
+ * weight gradient of a loss on DD/DR/RR and xi).  dL_dfull[nb] is the
+ * derivative of the loss with respect to the raw full histogram of
+ * tpcf_count (unordered pairs, before x2).  Every counted pair (i, j) in bin
+ * k adds w_j * dL_dfull[k] to dL_dw_a[i] and w_i * dL_dfull[k] to dL_dw_b[j]
+ * (auto counts: both to dL_dw_a).  Outputs are indexed by catalogue index
+ * (n points each; points dropped by the d_comov partition get 0) and summed
+ * in double.  Bin membership is the forward count's, decided by the same
+ * kernels; no pair is stored between the two passes. */
+int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                        int precision, const double *dL_dfull, double *dL_dw_a, double *dL_dw_b,
+                        tpcf_stats *stats);
+/* Replace a catalogue's weights (n floats, Galaxy::weight) in place: the
+ * device copy and every cached cell grid.  Positions and grids are kept. */
+int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight);
+
 /* Host-side evaluation of the up-weight of a 3-D inverse-p spec at values of
  * 1 - cos(theta), with the tables and arithmetic the kernels use; replaces
  * JKHists::interp after divide_by_hist (src/hist.cpp:224-231, :369-391). */

@@ -31,7 +31,8 @@ from ._capi import (ANGULAR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI, WEIGHTS
                     WEIGHTS_PLAIN, AxisSpec, Stats, WeightSpec)
 
 __all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "auto_pair_count", "cross_pair_count",
-           "count_weighted", "pair_count_weighted", "upweight_eval", "normalise_auto", "normalise_cross",
+           "count_weighted", "pair_count_weighted", "upweight_eval", "count_backward", "normalise_auto",
+           "normalise_cross",
            "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
            "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR"]
 
@@ -116,6 +117,11 @@ class Catalog:
     @property
     def n_used(self) -> int:
         return int(_capi.lib().tpcf_catalog_n_used(self._h))
+
+    def set_weights(self, weight):
+        """Replace Galaxy::weight of every point (device copy and cached cell grids)."""
+        w = np.ascontiguousarray(weight, np.float32).reshape(self.n)
+        _check(_capi.lib().tpcf_catalog_set_weights(self._h, _ptr(w)), self.ctx)
 
     def close(self):
         if getattr(self, "_h", None):
@@ -277,3 +283,17 @@ def upweight_eval(weights: Weights, values) -> np.ndarray:
     out = np.empty_like(v)
     _check(_capi.lib().tpcf_upweight_eval(C.byref(weights.spec), _ptr(v), v.size, _ptr(out)))
     return out
+
+
+def count_backward(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, dL_dfull,
+                   precision: int = FP32_GUARD):
+    """Adjoint of count(): per-point dL/dw of a and b (b None: auto count,
+    gradient of a only) for dL_dfull = dL/d(raw full histogram)."""
+    G = np.ascontiguousarray(dL_dfull, np.float64).reshape(binning.nb)
+    ga = np.zeros(a.n)
+    gb = np.zeros(b.n) if b is not None else None
+    st = Stats()
+    rc = _capi.lib().tpcf_count_backward(ctx._h, a._h, b._h if b is not None else None, binning._h, int(precision),
+                                         _ptr(G), _ptr(ga), _ptr(gb), C.byref(st))
+    _check(rc, ctx)
+    return ga, gb, st.as_dict()

@@ -72,6 +72,8 @@ _PROTOTYPES = {
     "tpcf_pair_count_weighted": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(WeightSpec), C.c_int, _vp, _vp,
                                            C.POINTER(Stats)]),
     "tpcf_upweight_eval": (C.c_int, [C.POINTER(WeightSpec), _vp, C.c_int64, _vp]),
+    "tpcf_count_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_catalog_set_weights": (C.c_int, [_vp, _vp]),
     "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),

@@ -497,6 +497,82 @@ int tpcf_pair_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_ca
     return reference_form(ctx, a, b, bin, spec, precision, full_hist, sub_hist, stats);
 }
 
+int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                        int precision, const double *dL_dfull, double *dL_dw_a, double *dL_dw_b, tpcf_stats *stats) {
+    if (!ctx || !a || !bin || !dL_dfull || !dL_dw_a || (b && !dL_dw_b)) return TPCF_E_INVALID_ARG;
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
+    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "the adjoint is defined for 3-D counts");
+    if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
+        return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    auto t0 = std::chrono::steady_clock::now();
+    std::memset(dL_dw_a, 0, sizeof(double) * a->c.n_all);
+    if (b) std::memset(dL_dw_b, 0, sizeof(double) * b->c.n_all);
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (a->c.n_kept == 0 || (b && b->c.n_kept == 0)) return TPCF_OK;
+    tpcf::CountRequest req;
+    req.a = &a->c;
+    req.b = b ? &b->c : nullptr;
+    req.bin = &bin->b;
+    req.exact_fp64 = precision == TPCF_FP64;
+    req.adj_G = dL_dfull;
+    req.grad_a = dL_dw_a;
+    req.grad_b = dL_dw_b;
+    tpcf::Stats st;
+    tpcf::Error err{0, ""};
+    int rc = tpcf::run_count(&ctx->c, req, nullptr, nullptr, &st, &err);
+    if (rc) return fail(ctx, rc, err.msg);
+    if (stats) {
+        stats->candidates = st.candidates;
+        stats->in_range = st.in_range;
+        stats->guard_evals = st.guard;
+        stats->work_items = st.items;
+        stats->ms_kernel = st.ms_kernel;
+        stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return TPCF_OK;
+}
+
+int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight) {
+    if (!cat || !weight) return TPCF_E_INVALID_ARG;
+    tpcf::Catalog &c = cat->c;
+    tpcf::Ctx *ctx = c.ctx;
+    const int N = (int)c.n_all;
+    bool unit = true;
+    float wmax = 0;
+    for (int i = 0; i < N; ++i) {
+        if (!std::isfinite(weight[i])) return TPCF_E_INVALID_ARG;
+        if (weight[i] != 1.0f) unit = false;
+        wmax = std::max(wmax, std::fabs(weight[i]));
+    }
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess && N > 0)
+        e = cudaMemcpyAsync(c.w.p, weight, sizeof(float) * N, cudaMemcpyHostToDevice, ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("set weights: ") + cudaGetErrorString(e);
+        return TPCF_E_CUDA;
+    }
+    std::copy(weight, weight + N, c.h_w.begin());
+    c.unit_weights = unit;
+    c.w_max = wmax;
+    if (!c.iw.p) {  // input weights default to the weights
+        c.iw_max = wmax;
+        c.iw_unit = unit;
+    }
+    tpcf::Error err{0, ""};
+    if (tpcf::reweight_grids(ctx, &c, &err)) {
+        ctx->last_error = err.msg;
+        return err.status;
+    }
+    e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        ctx->last_error = std::string("set weights: ") + cudaGetErrorString(e);
+        return TPCF_E_CUDA;
+    }
+    return TPCF_OK;
+}
+
 int tpcf_upweight_eval(const tpcf_weight_spec *spec, const double *values, int64_t n, double *out) {
     if (!spec || !spec->up_numerator || !spec->up_denominator || n < 0 || (n > 0 && (!values || !out)))
         return TPCF_E_INVALID_ARG;

@@ -138,6 +138,9 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
 // The grid build_grid would return when it is already cached, else nullptr;
 // never allocates.
 Grid *find_grid(Catalog *cat, const GridSpec &spec, bool want_fp64);
+// After the catalogue's weight array changed on the device: rewrite the
+// weight slot of every cached grid that carries it.
+int reweight_grids(Ctx *ctx, Catalog *cat, Error *err);
 
 // pair_count.cu
 // Angular up-weight of the 3-D inverse-p counts: JKHists::interp
@@ -171,6 +174,11 @@ struct CountRequest {
     const UpTable *up = nullptr; // 3-D inverse-p counts
     int n_runs = 0;              // Params::n_bitwise_runs
     int refinement = 0;
+    // adjoint of a plain-weight 3-D count: with adj_G = dL/d(raw full
+    // histogram) set, the count writes per-point dL/dw into grad_a (n_all of
+    // a) and grad_b (n_all of b; unused for auto counts) instead of histograms
+    const double *adj_G = nullptr;
+    double *grad_a = nullptr, *grad_b = nullptr;
 };
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);
 // run_count without device allocation: every scratch buffer is carved from

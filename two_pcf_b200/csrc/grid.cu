@@ -223,6 +223,17 @@ __global__ void regions_kernel(GeomDev g, int ncell, const int *__restrict__ bst
     }
 }
 
+// New weights for the points of a cached grid: pos.w (and xyz_s.w) from the
+// catalogue's weight array through the grid's index.
+__global__ void reweight_kernel(int n, const int *__restrict__ idx, const float *__restrict__ w,
+                                float4 *__restrict__ pos, double4 *__restrict__ xyz_s) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float wi = w[idx[k]];
+    pos[k].w = wi;
+    if (xyz_s) xyz_s[k].w = (double)wi;
+}
+
 }  // namespace
 
 #define TPCF_CUDA_TRY(expr)                                                              \
@@ -374,6 +385,19 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
     *out = g.get();
     cat->grids[key] = std::move(g);
+    return 0;
+}
+
+int reweight_grids(Ctx *ctx, Catalog *cat, Error *err) {
+    for (auto &kv : cat->grids) {
+        Grid *g = kv.second.get();
+        if (g->input_w && cat->iw.p) continue;  // carries input weights, which did not change
+        if (g->n == 0) continue;
+        reweight_kernel<<<(g->n + 255) / 256, 256, 0, ctx->stream>>>(g->n, g->idx.p, cat->w.p, g->pos.p,
+                                                                     g->has_fp64 ? g->xyz_s.p : nullptr);
+        ++ctx->launches;
+        TPCF_CUDA_TRY(cudaGetLastError());
+    }
     return 0;
 }
 

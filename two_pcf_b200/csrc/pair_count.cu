@@ -105,17 +105,30 @@ struct KParams {
     double up_min, up_max;
     float g_ang;       // error bound of the FP32 1 - cos(theta)
     unsigned *flags;   // (1 + n_jk) * nb: non-finite weights met per bin (1 NaN, 2 +inf, 4 -inf)
+    // adjoint (W_ADJ): dL/d(full histogram) and the per-point gradients,
+    // indexed by catalogue index (grad_b == grad_a for auto counts)
+    const double *adj_G;
+    double *grad_a, *grad_b;
+};
+
+// Shared-memory views the binning steps use.
+struct Shm {
+    const float *t1, *t2;          // threshold tables
+    const unsigned char *l1, *l2;  // lookup tables
+    uint32_t *lo, *hi;             // 64-bit fixed-point histogram as two 32-bit words per bin
+    const double *G;               // adjoint: dL/d(full histogram) (aliases lo/hi)
+    double *ga, *gb;               // adjoint: gradient sums of the A chunk and of the B tile
 };
 
 struct SmemLayout {
-    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, achunk, tile0, tile1, misc, total;
+    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, achunk, ga, gb, tile0, tile1, misc, total;
 };
 
 __host__ __device__ inline size_t tile_bytes(bool exact) { return (size_t)TB * (exact ? 64 : 32); }
 
 // lo/hi: the histogram pairs are added to (per segment region when there
 // are jackknife regions); alo/ahi: the item's A-side total (jackknife only).
-__host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk) {
+__host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk, bool adj = false) {
     SmemLayout L;
     size_t o = 0;
     L.lo = o;
@@ -139,6 +152,10 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o += (size_t)NWARP * QCAP * 16;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
     if (!exact) o += (size_t)TA * 16;
+    L.ga = o;      // adjoint: per-point gradient sums (double)
+    if (adj) o += (size_t)TA * 8;
+    L.gb = o;
+    if (adj) o += (size_t)TB * 8;
     o = (o + 127) / 128 * 128;
     L.tile0 = o;
     o += tile_bytes(exact);
@@ -374,8 +391,16 @@ __device__ __noinline__ void flag_nonfinite(const KParams &P, int bin, int ra, i
 // Add one binned pair: weight from the queue (product of the grid weights)
 // or, for the inverse-p kinds, formed here; fixed-point shared add.
 template <bool UNITW, int WK>
-__device__ __forceinline__ void add_binned(const KParams &P, uint32_t *s_lo, uint32_t *s_hi, int bin, float w,
-                                           int ia, int jb, int ra, int rb) {
+__device__ __forceinline__ void add_binned(const KParams &P, const Shm &S, int bin, float wa, float wb, int ia,
+                                           int jb, int ka, int jl, int ra, int rb) {
+    if constexpr (WK == W_ADJ) {
+        // the pair adds wa * wb to its bin: dL/dwa += G wb, dL/dwb += G wa
+        const double g = S.G[bin];
+        atomicAdd(&S.ga[ka], g * (double)wb);
+        atomicAdd(&S.gb[jl], g * (double)wa);
+        return;
+    }
+    float w = UNITW ? 1.0f : __fmul_rn(wa, wb);
     if (WK != W_PLAIN) {
         w = pair_weight<WK>(P, w, P.a.idx[ia], P.b.idx[jb]);
         if (!isfinite(w)) {
@@ -384,7 +409,7 @@ __device__ __forceinline__ void add_binned(const KParams &P, uint32_t *s_lo, uin
         }
     }
     const long long q = (UNITW && WK == W_PLAIN) ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
-    dev::acc_add(s_lo, s_hi, bin, q);
+    dev::acc_add(S.lo, S.hi, bin, q);
 }
 
 // Bin one pair that passed the guard-widened range test, from its FP32
@@ -395,10 +420,9 @@ __device__ __forceinline__ void add_binned(const KParams &P, uint32_t *s_lo, uin
 // its two points.
 template <int MODE, bool UNITW, int WK>
 __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
-                                         const float *s_t1, const float *s_t2, const unsigned char *s_l1,
-                                         const unsigned char *s_l2, uint32_t *s_lo, uint32_t *s_hi,
-                                         const float4 *s_pos, const float4 *s_aux, const float4 *s_achunk,
-                                         const float4 e, int a_start, int jbase, int ra, int rb, Counters &cnt) {
+                                         const Shm &S, const float4 *s_pos, const float4 *s_aux,
+                                         const float4 *s_achunk, const float4 e, int a_start, int jbase, int ra,
+                                         int rb, Counters &cnt) {
     // queue entry: (dx, dy, dz, A chunk index << 8 | tile index)
     const int pk = __float_as_int(e.w);
     const int ka = pk >> 8, jl = pk & 0xff;
@@ -406,7 +430,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
     const float dx = e.x, dy = e.y, dz = e.z;
     const float s2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));  // as in the candidate test
     const float4 qa = s_achunk[ka];
-    const float w = UNITW ? 1.0f : __fmul_rn(qa.w, s_pos[jl].w);
+    const float wa = qa.w, wb = s_pos[jl].w;
     float pi = 0.f;
     if constexpr (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU) {
         const float4 ab = s_aux[jl];
@@ -418,18 +442,18 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
         // v = |n1 - n2|^2 / 2 approximates 1 - cos(theta) within g_ang
         const float v = 0.5f * s2;
         bool amb1;
-        const unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, v)], v, s_t1, P.g_ang, P.lut_edge1, &amb1);
+        const unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, v)], v, S.t1, P.g_ang, P.lut_edge1, &amb1);
         if (c1 == LUT_INV) return;
         if (!amb1) {
             cnt.in_range += 1;
             bin = (int)c1;
         } else {
-            const dev::AxisK ax1{s_t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
-            int b = dev::locate_exact(s_t1, P.n1, v);
+            const dev::AxisK ax1{S.t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
+            int b = dev::locate_exact(S.t1, P.n1, v);
             bool inr;
             if (dev::near_edge(ax1, v, b, P.g_ang)) {
                 cnt.guard += 1;
-                b = exact_pair<MODE_ANGULAR>(E, s_t1, s_t2, P.a.idx[ia], P.b.idx[jb], &inr);
+                b = exact_pair<MODE_ANGULAR>(E, S.t1, S.t2, P.a.idx[ia], P.b.idx[jb], &inr);
             } else {
                 inr = b >= 0 && b < P.n1;
             }
@@ -437,7 +461,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             if (!inr) return;
             bin = b;
         }
-        add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
+        add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
         return;
     } else {
         if (MODE == MODE_SIGMA_PI) {
@@ -446,7 +470,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             const float a = fmaf(-pi, pi, s2);
             const float api = fabsf(pi);
             bool amb1, amb2;
-            unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, a)], a, s_t1, P.g_a, P.lut_edge1, &amb1);
+            unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, a)], a, S.t1, P.g_a, P.lut_edge1, &amb1);
             if (a <= P.g_a) {
                 c1 = LUT_AMB;
                 amb1 = true;
@@ -455,7 +479,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
                 c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
                 amb1 = false;
             }
-            const unsigned c2 = lut_decode(s_l2[lut2_index(P.lut2_scale, api)], api, s_t2, P.g_pi, P.lut_edge2, &amb2);
+            const unsigned c2 = lut_decode(S.l2[lut2_index(P.lut2_scale, api)], api, S.t2, P.g_pi, P.lut_edge2, &amb2);
             if (!amb && ((c1 == LUT_INV && !amb1) || (c2 == LUT_INV && !amb2))) {
                 cnt.in_range += 1;
                 return;
@@ -464,7 +488,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             if (!amb) cnt.in_range += 1;
             bin = (int)(c1 * P.n2 + c2);
         } else {
-            const unsigned c1 = lut_decode(s_l1[lut1_index(P.lut1_base, s2)], s2, s_t1, P.g_s2, P.lut_edge1, &amb);
+            const unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, s2)], s2, S.t1, P.g_s2, P.lut_edge1, &amb);
             if (c1 == LUT_INV) {
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
@@ -477,7 +501,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
                 const float mu = fabsf(pi) * inv_s;
                 const float gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
                 bool amb2;
-                c2 = lut_decode(s_l2[lut2_index(P.lut2_scale, mu)], mu, s_t2, gmu, P.lut_edge2, &amb2);
+                c2 = lut_decode(S.l2[lut2_index(P.lut2_scale, mu)], mu, S.t2, gmu, P.lut_edge2, &amb2);
                 if (c2 == LUT_INV && !amb2 && !amb && s2 >= P.s2_lut_min) {
                     cnt.in_range += 1;
                     return;
@@ -489,12 +513,12 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
         }
         if (amb) {
             bool inr, guarded;
-            bin = precise_bin<MODE>(PA, E, s_t1, s_t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
+            bin = precise_bin<MODE>(PA, E, S.t1, S.t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
             cnt.in_range += inr ? 1 : 0;
             cnt.guard += guarded ? 1 : 0;
             if (bin < 0) return;
         }
-        add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
+        add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
     }
 }
 
@@ -502,12 +526,11 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
 // d2), or for angular counts from its exact (float)(1 - cos(theta)) in d0;
 // ia/jb are its positions in the sorted grids.
 template <int MODE, bool UNITW, int WK>
-__device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, const float *s_t1, const float *s_t2,
-                                          uint32_t *s_lo, uint32_t *s_hi, float d0, float d1, float d2, int ia,
-                                          int jb, int ra, int rb, Counters &cnt) {
+__device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, const Shm &S, float d0, float d1,
+                                          float d2, int ia, int jb, int ka, int jl, int ra, int rb, Counters &cnt) {
     int bin;
     if constexpr (MODE == MODE_ANGULAR) {
-        bin = dev::locate_exact(s_t1, P.n1, d0);  // in [0, n1): the candidate test checked it
+        bin = dev::locate_exact(S.t1, P.n1, d0);  // in [0, n1): the candidate test checked it
         cnt.in_range += 1;
     } else {
         double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
@@ -522,12 +545,12 @@ __device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, 
             n2z = u2.z;
         }
         bool inr;
-        bin = exact_bin<MODE>(E, s_t1, s_t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
+        bin = exact_bin<MODE>(E, S.t1, S.t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
         cnt.in_range += inr ? 1 : 0;
         if (bin < 0) return;
     }
-    const float w = UNITW ? 1.0f : __fmul_rn((float)P.a.xyz_s[ia].w, (float)P.b.xyz_s[jb].w);
-    add_binned<UNITW, WK>(P, s_lo, s_hi, bin, w, ia, jb, ra, rb);
+    const float wa = (float)P.a.xyz_s[ia].w, wb = (float)P.b.xyz_s[jb].w;
+    add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
 }
 
 // Add a 64-bit value held as two 32-bit words into another such pair (the
@@ -543,7 +566,8 @@ template <int MODE, bool UNITW, bool JK, bool EXACT, int WK>
 __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
-    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK);
+    constexpr bool ADJ = (WK == W_ADJ);
+    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
     uint32_t *s_alo = (uint32_t *)(smem + L.alo);
@@ -560,13 +584,22 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4 *s_q = (float4 *)(smem + L.queue) + warp * QCAP;
     const unsigned lt_mask = (1u << lane) - 1u;
+    const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo), (double *)(smem + L.ga),
+                (double *)(smem + L.gb)};
 
-    for (int i = tid; i < P.nb; i += NT) {
-        s_lo[i] = 0;
-        s_hi[i] = 0;
-        if (JK) {
-            s_alo[i] = 0;
-            s_ahi[i] = 0;
+    if (ADJ) {
+        // the histogram words hold dL/d(full histogram) instead
+        for (int i = tid; i < P.nb; i += NT) ((double *)(smem + L.lo))[i] = P.adj_G[i];
+        for (int i = tid; i < TA; i += NT) S.ga[i] = 0.0;
+        for (int i = tid; i < TB; i += NT) S.gb[i] = 0.0;
+    } else {
+        for (int i = tid; i < P.nb; i += NT) {
+            s_lo[i] = 0;
+            s_hi[i] = 0;
+            if (JK) {
+                s_alo[i] = 0;
+                s_ahi[i] = 0;
+            }
         }
     }
     for (int i = tid; i <= P.n1; i += NT) s_t1[i] = P.t1g[i];
@@ -751,9 +784,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 __syncwarp();
                                 const float4 e = s_q[qn - 32 + lane];
                                 const int pk = __float_as_int(e.w);
-                                bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
-                                                           it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region,
-                                                           rb, cnt);
+                                bin_exact<MODE, UNITW, WK>(P, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
+                                                           jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb,
+                                                           cnt);
                                 __syncwarp();
                                 qn -= 32;
                             }
@@ -764,9 +797,8 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         if (lane < qn) {
                             const float4 e = s_q[lane];
                             const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW, WK>(P, EA, s_t1, s_t2, s_lo, s_hi, e.x, e.y, e.z,
-                                                       it.a_start + (pk >> 8), jbase + (pk & 0xff), it.a_region, rb,
-                                                       cnt);
+                            bin_exact<MODE, UNITW, WK>(P, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
+                                                       jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb, cnt);
                         }
                         __syncwarp();
                     }
@@ -810,7 +842,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 while (qn >= 32) {
                                     __syncwarp();
                                     const float4 e = s_q[qn - 32 + lane];
-                                    bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, s_pos,
+                                    bin_fast<MODE, UNITW, WK>(P, PA, EA, S, s_pos,
                                                               s_aux, s_achunk, e, it.a_start, jbase, it.a_region, rb,
                                                               cnt);
                                     __syncwarp();
@@ -825,12 +857,22 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     if (qn > 0) {
                         __syncwarp();
                         if (lane < qn)
-                            bin_fast<MODE, UNITW, WK>(P, PA, EA, s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, s_pos, s_aux,
+                            bin_fast<MODE, UNITW, WK>(P, PA, EA, S, s_pos, s_aux,
                                                       s_achunk, s_q[lane], it.a_start, jbase, it.a_region, rb, cnt);
                         __syncwarp();
                     }
                 }
                 __syncthreads();  // everyone is done with this buffer before it is refilled
+                if constexpr (ADJ) {
+                    // this tile's B gradients to their points
+                    const int jb0 = sg.b_start + tstart;
+                    for (int t2 = tid; t2 < tlen; t2 += NT) {
+                        const double v = S.gb[t2];
+                        if (v != 0.0) atomicAdd(&P.grad_b[P.b.idx[jb0 + t2]], v);
+                        S.gb[t2] = 0.0;
+                    }
+                    __syncthreads();
+                }
                 ++tcount;
             }
             // ---- jackknife: a region's pairs (JKHists::add_pair,
@@ -865,11 +907,20 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             }
             __syncthreads();
         }
+        // ---- adjoint: the A chunk's gradients to their points
+        if constexpr (ADJ) {
+            for (int k = tid; k < it.a_len; k += NT) {
+                const double v = S.ga[k];
+                if (v != 0.0) atomicAdd(&P.grad_a[P.a.idx[it.a_start + k]], v);
+                S.ga[k] = 0.0;
+            }
+            __syncthreads();
+        }
     }
 
     // ---- merge the privatised histogram
     __syncthreads();
-    if (!JK) {
+    if (!JK && !ADJ) {
         for (int b = tid; b < P.nb; b += NT) {
             const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
             if (v) dev::acc_add_global(P.g_full, b, v);
@@ -896,15 +947,22 @@ typedef void (*KernelFn)(const KParams);
 
 template <int MODE, int WK>
 KernelFn pick_kernel(bool unitw, bool jk, bool exact) {
-    if constexpr (WK == W_PLAIN) {
-        if (unitw) {
-            if (exact)
-                return jk ? pair_count_kernel<MODE, true, true, true, WK> : pair_count_kernel<MODE, true, false, true, WK>;
-            return jk ? pair_count_kernel<MODE, true, true, false, WK> : pair_count_kernel<MODE, true, false, false, WK>;
+    if constexpr (WK == W_ADJ) {  // no regions, per-point weights
+        return exact ? pair_count_kernel<MODE, false, false, true, WK> : pair_count_kernel<MODE, false, false, false, WK>;
+    } else {
+        if constexpr (WK == W_PLAIN) {
+            if (unitw) {
+                if (exact)
+                    return jk ? pair_count_kernel<MODE, true, true, true, WK>
+                              : pair_count_kernel<MODE, true, false, true, WK>;
+                return jk ? pair_count_kernel<MODE, true, true, false, WK>
+                          : pair_count_kernel<MODE, true, false, false, WK>;
+            }
         }
+        if (exact)
+            return jk ? pair_count_kernel<MODE, false, true, true, WK> : pair_count_kernel<MODE, false, false, true, WK>;
+        return jk ? pair_count_kernel<MODE, false, true, false, WK> : pair_count_kernel<MODE, false, false, false, WK>;
     }
-    if (exact) return jk ? pair_count_kernel<MODE, false, true, true, WK> : pair_count_kernel<MODE, false, false, true, WK>;
-    return jk ? pair_count_kernel<MODE, false, true, false, WK> : pair_count_kernel<MODE, false, false, false, WK>;
 }
 
 template <int MODE>
@@ -912,6 +970,7 @@ KernelFn pick_3d(int wk, bool unitw, bool jk, bool exact) {
     switch (wk) {
     case W_INVP_DD: return pick_kernel<MODE, W_INVP_DD>(unitw, jk, exact);
     case W_INVP_DR: return pick_kernel<MODE, W_INVP_DR>(unitw, jk, exact);
+    case W_ADJ: return pick_kernel<MODE, W_ADJ>(unitw, jk, exact);
     default: return pick_kernel<MODE, W_PLAIN>(unitw, jk, exact);
     }
 }
@@ -1273,8 +1332,11 @@ double fixed_to_double(const unsigned long long *p, double inv) {
 struct CountPlan {
     const Binning *bin = nullptr;
     const UpTable *up = nullptr;
-    bool is_auto = false, jk = false, unitw = false, angular = false;
+    bool is_auto = false, jk = false, unitw = false, angular = false, adj = false;
     int nb = 0, n_jk = 1, wk = W_PLAIN;
+    int n_a = 0, n_b = 0;  // catalogue sizes (adjoint outputs)
+    const double *adj_G_host = nullptr;
+    double *grad_a_host = nullptr, *grad_b_host = nullptr;
     double inv = 1.0;  // 2^-S
     std::vector<WorkItem> items;
     std::vector<Segment> segs;
@@ -1296,6 +1358,7 @@ struct CountBuffers {
     unsigned char *l1 = nullptr, *l2 = nullptr;
     unsigned *flags = nullptr;
     double *up_bins = nullptr, *up_centre = nullptr;
+    double *adj_G = nullptr, *grad_a = nullptr, *grad_b = nullptr;
 };
 
 int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Error *err) {
@@ -1309,6 +1372,12 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     C.nb = bin->nb;
     C.n_jk = bin->n_jk;
     C.jk = C.n_jk > 1;
+    C.adj = req.adj_G != nullptr;
+    C.adj_G_host = req.adj_G;
+    C.grad_a_host = req.grad_a;
+    C.grad_b_host = req.grad_b;
+    C.n_a = (int)A->n_all;
+    C.n_b = (int)B->n_all;
     const int wt = req.weighting;
     // Weight kind, the weight each grid point carries, and the points
     // counted: 3-D counts use the d_comov partition (GalaxyBoxes); angular
@@ -1321,6 +1390,16 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     auto wmax_of = [&](const Catalog *c) { return (double)(input_w ? c->iw_max : c->w_max); };
     auto unit_of = [&](const Catalog *c) { return input_w ? c->iw_unit : c->unit_weights; };
     C.unitw = C.wk == W_PLAIN && unit_of(A) && unit_of(B);
+    if (C.adj) {
+        if (C.angular || wt != WEIGHTS_PLAIN) {
+            err->status = 6;
+            err->msg = "the adjoint is defined for plain-weight 3-D counts";
+            return err->status;
+        }
+        C.wk = W_ADJ;
+        C.jk = false;  // dL/dw of the full histogram; regions play no part
+        C.unitw = false;
+    }
 
     // Per-axis bound on the separation of every counted pair: the maximum
     // separation (3-D), or the chord of the largest binned 1 - cos(theta),
@@ -1370,7 +1449,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     build_work_items(*ga, *gb, C.is_auto, m, side, rb, C.items, C.segs);
 
     float wscale = 1.0f;
-    if (!C.unitw) {
+    if (!C.unitw && !C.adj) {
         double wmax = wmax_of(A) * wmax_of(B);
         const double up_max = C.up ? 4.0 * C.up->abs_max : 0.0;  // interpolation stays within 4x the bins
         if (C.wk == W_INVP_DD) wmax *= up_max * std::max(req.n_runs, 1);
@@ -1380,7 +1459,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         wscale = std::ldexp(1.0f, S);
         C.inv = std::ldexp(1.0, -S);
     }
-    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk);
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk, C.adj);
     if (C.L.total + 1024 > ctx->smem_optin) {
         err->status = 6;
         err->msg = "histogram does not fit in shared memory";
@@ -1486,6 +1565,11 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     TPCF_TRY(cudaMemsetAsync(D.head, 0, sizeof(int), stm));
     TPCF_TRY(cudaMemsetAsync(D.err, 0, sizeof(int), stm));
     if (C.n_flags()) TPCF_TRY(cudaMemsetAsync(D.flags, 0, sizeof(unsigned) * C.n_flags(), stm));
+    if (C.adj) {
+        TPCF_TRY(cudaMemcpyAsync(D.adj_G, C.adj_G_host, sizeof(double) * nb, cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemsetAsync(D.grad_a, 0, sizeof(double) * std::max(C.n_a, 1), stm));
+        if (!C.is_auto) TPCF_TRY(cudaMemsetAsync(D.grad_b, 0, sizeof(double) * std::max(C.n_b, 1), stm));
+    }
 
     KParams P = C.P;
     P.items = D.items;
@@ -1503,6 +1587,9 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     P.up_thr = D.up_thr;
     P.up_bins = D.up_bins;
     P.up_centre = D.up_centre;
+    P.adj_G = D.adj_G;
+    P.grad_a = D.grad_a;
+    P.grad_b = C.is_auto ? D.grad_a : D.grad_b;
 
     TPCF_TRY(cudaFuncSetAttribute((const void *)C.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.L.total));
     int per_sm = 1;
@@ -1542,6 +1629,19 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
         err->status = 4;
         err->msg = "device wait exceeded its iteration limit; results discarded";
         return err->status;
+    }
+    if (C.adj) {
+        TPCF_TRY(cudaMemcpy(C.grad_a_host, D.grad_a, sizeof(double) * C.n_a, cudaMemcpyDeviceToHost));
+        if (!C.is_auto && C.grad_b_host)
+            TPCF_TRY(cudaMemcpy(C.grad_b_host, D.grad_b, sizeof(double) * C.n_b, cudaMemcpyDeviceToHost));
+        if (st) {
+            st->candidates += hc[0];
+            st->in_range += hc[1];
+            st->guard += hc[2];
+            st->items += C.items.size();
+            st->ms_kernel += ms;
+        }
+        return 0;
     }
     // A bin that met a non-finite pair weight holds what double
     // accumulation would: NaN, or an infinity of one sign.
@@ -1607,7 +1707,16 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
         TPCF_TRY(d_up_bins.alloc(C.n_up()));
         TPCF_TRY(d_up_centre.alloc(C.n_up()));
     }
+    DevBuf<double> d_adj_G, d_grad_a, d_grad_b;
+    if (C.adj) {
+        TPCF_TRY(d_adj_G.alloc(C.nb));
+        TPCF_TRY(d_grad_a.alloc(std::max(C.n_a, 1)));
+        if (!C.is_auto) TPCF_TRY(d_grad_b.alloc(std::max(C.n_b, 1)));
+    }
     CountBuffers D;
+    D.adj_G = d_adj_G.p;
+    D.grad_a = d_grad_a.p;
+    D.grad_b = d_grad_b.p;
     D.items = d_items.p;
     D.segs = d_segs.p;
     D.full = d_full.p;
@@ -1696,6 +1805,11 @@ struct ScratchPlan {
 int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
                      Error *err) {
     const Binning *bin = req.bin;
+    if (req.adj_G) {
+        err->status = 6;
+        err->msg = "the allocation-free count has no adjoint";
+        return err->status;
+    }
     const int nb = bin->nb, n_jk = bin->n_jk;
     // The histogram and table part of the scratch is known before the work
     // list is built; refuse an oversized binning before anything else.

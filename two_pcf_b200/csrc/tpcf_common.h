@@ -22,6 +22,7 @@ enum WeightKind {
     W_INVP_DR = 3,    // (float)((w1 * w2) * interp(1-cos))
     W_ANG_INPUT = 4,  // iw1 * iw2 (angular DD/DR: input weights)
     W_ANG_INVP = 5,   // iw1 * iw2 * (n_runs / popc)  (angular DD inverse-p)
+    W_ADJ = 6,        // adjoint of a w1 * w2 count: per-point dL/dw instead of a histogram
 };
 
 // Histogram bins are decided by comparing a float value with a float
