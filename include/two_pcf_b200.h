@@ -194,6 +194,31 @@ int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog
  * device copy and every cached cell grid.  Positions and grids are kept. */
 int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight);
 
+/* Batched counts (no single counterpart in the reference, whose driver counts
+ * one catalogue at a time): DD of each mock and/or DR of each mock against a
+ * shared random catalogue, as ONE persistent launch over the work items of
+ * every pair.  The plan (cell grids, work list, tables, device buffers) is
+ * built once by tpcf_batch_create and every tpcf_batch_run replays it as a
+ * CUDA graph (clears, the launch, the read-backs).
+ *   what: TPCF_BATCH_DD | TPCF_BATCH_DR; outputs are ordered mock by mock,
+ *         DD then DR, each as tpcf_count returns it (raw, not doubled).
+ *   refinement: cells per maximum separation 1..3, 0 automatic, or
+ *         TPCF_BATCH_AUTOTUNE: each of 1, 2, 3 is planned and timed once and
+ *         the fastest is kept (tpcf_batch_refinement reports it).
+ * The catalogues must outlive the batch, keep their weights, and keep their
+ * cached grids (no tpcf_catalog_release_cache) while it exists. */
+typedef struct tpcf_batch tpcf_batch;
+#define TPCF_BATCH_DD 1
+#define TPCF_BATCH_DR 2
+#define TPCF_BATCH_AUTOTUNE (-1)
+int tpcf_batch_create(tpcf_ctx *ctx, const tpcf_catalog *const *mocks, int32_t n_mocks, const tpcf_catalog *randoms,
+                      const tpcf_binning *bin, int precision, int32_t what, int32_t refinement, tpcf_batch **out);
+/* full_out[n_outputs * nb]; region_out[n_outputs * n_jk * nb] or NULL. */
+int tpcf_batch_run(tpcf_batch *batch, double *full_out, double *region_out, tpcf_stats *stats);
+int tpcf_batch_n_outputs(const tpcf_batch *batch);
+int tpcf_batch_refinement(const tpcf_batch *batch);
+int tpcf_batch_destroy(tpcf_batch *batch);
+
 /* Host-side evaluation of the up-weight of a 3-D inverse-p spec at values of
  * 1 - cos(theta), with the tables and arithmetic the kernels use; replaces
  * JKHists::interp after divide_by_hist (src/hist.cpp:224-231, :369-391). */

@@ -27,14 +27,14 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from ._capi import (ANGULAR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR,
-                    WEIGHTS_PLAIN, AxisSpec, Stats, WeightSpec)
+from ._capi import (ANGULAR, BATCH_AUTOTUNE, BATCH_DD, BATCH_DR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI,
+                    WEIGHTS_INVP_DD, WEIGHTS_INVP_DR, WEIGHTS_PLAIN, AxisSpec, Stats, WeightSpec)
 
 __all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "auto_pair_count", "cross_pair_count",
            "count_weighted", "pair_count_weighted", "upweight_eval", "count_backward", "normalise_auto",
            "normalise_cross",
            "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
-           "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR"]
+           "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR", "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE"]
 
 
 class TpcfError(RuntimeError):
@@ -297,3 +297,42 @@ def count_backward(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning
                                          _ptr(G), _ptr(ga), _ptr(gb), C.byref(st))
     _check(rc, ctx)
     return ga, gb, st.as_dict()
+
+
+class Batch:
+    """DD and/or DR counts of many mock catalogues (DR against one shared random
+    catalogue) in one persistent launch, planned once and replayed as a CUDA
+    graph by run().  refinement: 1..3, 0 automatic, BATCH_AUTOTUNE to time
+    1, 2 and 3 and keep the fastest."""
+
+    def __init__(self, ctx: Context, mocks, randoms: Catalog | None, binning: Binning, precision: int = FP32_GUARD,
+                 what: int = BATCH_DD | BATCH_DR, refinement: int = 0):
+        arr = (C.c_void_p * len(mocks))(*[m._h.value for m in mocks])
+        h = C.c_void_p()
+        rc = _capi.lib().tpcf_batch_create(ctx._h, arr, len(mocks), randoms._h if randoms is not None else None,
+                                           binning._h, int(precision), int(what), int(refinement), C.byref(h))
+        _check(rc, ctx)
+        self._h, self.ctx, self.binning = h, ctx, binning
+        self._keep = (list(mocks), randoms)
+        self.n_outputs = int(_capi.lib().tpcf_batch_n_outputs(h))
+        self.refinement = int(_capi.lib().tpcf_batch_refinement(h))
+
+    def run(self, with_regions: bool = True):
+        """(full[n_outputs, nb], regions[n_outputs, n_jk, nb] or None, stats)."""
+        nb, nj = self.binning.nb, self.binning.n_jk
+        full = np.zeros((self.n_outputs, nb))
+        reg = np.zeros((self.n_outputs, nj, nb)) if with_regions else None
+        st = Stats()
+        _check(_capi.lib().tpcf_batch_run(self._h, _ptr(full), _ptr(reg), C.byref(st)), self.ctx)
+        return full, reg, st.as_dict()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _capi.lib().tpcf_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -37,6 +37,7 @@ class Stats(C.Structure):
 
 
 WEIGHTS_PLAIN, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR = 0, 1, 2
+BATCH_DD, BATCH_DR, BATCH_AUTOTUNE = 1, 2, -1
 
 
 class WeightSpec(C.Structure):
@@ -74,6 +75,11 @@ _PROTOTYPES = {
     "tpcf_upweight_eval": (C.c_int, [C.POINTER(WeightSpec), _vp, C.c_int64, _vp]),
     "tpcf_count_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_catalog_set_weights": (C.c_int, [_vp, _vp]),
+    "tpcf_batch_create": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp, C.c_int, C.c_int32, C.c_int32, C.POINTER(_vp)]),
+    "tpcf_batch_run": (C.c_int, [_vp, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_batch_n_outputs": (C.c_int, [_vp]),
+    "tpcf_batch_refinement": (C.c_int, [_vp]),
+    "tpcf_batch_destroy": (C.c_int, [_vp]),
     "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_normalise_auto": (C.c_int, [_vp, C.c_int32, _vp, _vp]),

@@ -7,6 +7,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <new>
 #include <vector>
 
@@ -20,6 +21,13 @@ struct tpcf_catalog {
 };
 struct tpcf_binning {
     tpcf::Binning b;
+};
+struct tpcf_batch {
+    tpcf_ctx *ctx = nullptr;
+    tpcf::Batch *b = nullptr;
+    ~tpcf_batch() {
+        if (b) tpcf::batch_destroy(b);
+    }
 };
 
 namespace {
@@ -570,6 +578,68 @@ int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight) {
         ctx->last_error = std::string("set weights: ") + cudaGetErrorString(e);
         return TPCF_E_CUDA;
     }
+    return TPCF_OK;
+}
+
+int tpcf_batch_create(tpcf_ctx *ctx, const tpcf_catalog *const *mocks, int32_t n_mocks, const tpcf_catalog *randoms,
+                      const tpcf_binning *bin, int precision, int32_t what, int32_t refinement, tpcf_batch **out) {
+    if (!ctx || !mocks || n_mocks < 1 || !bin || !out) return TPCF_E_INVALID_ARG;
+    *out = nullptr;
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
+    if ((what & ~(TPCF_BATCH_DD | TPCF_BATCH_DR)) || !what) return fail(ctx, TPCF_E_INVALID_ARG, "bad batch outputs");
+    if ((what & TPCF_BATCH_DR) && !randoms) return fail(ctx, TPCF_E_INVALID_ARG, "DR needs the random catalogue");
+    if (refinement < -1 || refinement > 3) return fail(ctx, TPCF_E_INVALID_ARG, "bad refinement");
+    if (bin->b.mode == TPCF_ANGULAR) return fail(ctx, TPCF_E_UNSUPPORTED, "batched counts are 3-D counts");
+    std::vector<tpcf::BatchJobSpec> jobs;
+    for (int i = 0; i < n_mocks; ++i) {
+        if (!mocks[i] || mocks[i]->c.n_jk != bin->b.n_jk)
+            return fail(ctx, TPCF_E_INVALID_ARG, "mock " + std::to_string(i) + " missing or with other n_jk_regions");
+        if (what & TPCF_BATCH_DD) jobs.push_back({&mocks[i]->c, nullptr});
+        if (what & TPCF_BATCH_DR) jobs.push_back({&mocks[i]->c, &randoms->c});
+    }
+    if (randoms && randoms->c.n_jk != bin->b.n_jk)
+        return fail(ctx, TPCF_E_INVALID_ARG, "randoms and binning disagree on n_jk_regions");
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    std::unique_ptr<tpcf_batch> B(new (std::nothrow) tpcf_batch());
+    if (!B) return TPCF_E_OOM;
+    B->ctx = ctx;
+    tpcf::Error err{0, ""};
+    if (tpcf::batch_create(&ctx->c, jobs, &bin->b, precision == TPCF_FP64, refinement, &B->b, &err))
+        return fail(ctx, err.status, err.msg);
+    *out = B.release();
+    return TPCF_OK;
+}
+
+int tpcf_batch_run(tpcf_batch *batch, double *full_out, double *region_out, tpcf_stats *stats) {
+    if (!batch || !full_out) return TPCF_E_INVALID_ARG;
+    tpcf_ctx *ctx = batch->ctx;
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    auto t0 = std::chrono::steady_clock::now();
+    tpcf::Stats st;
+    tpcf::Error err{0, ""};
+    if (tpcf::batch_run(batch->b, full_out, region_out, &st, &err)) return fail(ctx, err.status, err.msg);
+    if (stats) {
+        stats->candidates = st.candidates;
+        stats->in_range = st.in_range;
+        stats->guard_evals = st.guard;
+        stats->overflow_updates = st.overflow;
+        stats->work_items = st.items;
+        stats->ms_kernel = st.ms_kernel;
+        stats->ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return TPCF_OK;
+}
+
+int tpcf_batch_n_outputs(const tpcf_batch *batch) { return batch ? tpcf::batch_jobs(batch->b) : -TPCF_E_INVALID_ARG; }
+int tpcf_batch_refinement(const tpcf_batch *batch) {
+    return batch ? tpcf::batch_refinement(batch->b) : -TPCF_E_INVALID_ARG;
+}
+int tpcf_batch_destroy(tpcf_batch *batch) {
+    if (!batch) return TPCF_E_INVALID_ARG;
+    cudaSetDevice(batch->ctx->c.device);
+    delete batch;
     return TPCF_OK;
 }
 

@@ -188,6 +188,24 @@ constexpr size_t kStaticScratchBytes = size_t(32) << 20;
 int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
                      Error *err);
 
+// pair_count.cu: batched counts — the work items of many catalogue pairs in
+// one persistent launch, planned once and replayed as a CUDA graph.
+struct Batch;
+struct BatchJobSpec {
+    const Catalog *a = nullptr;
+    const Catalog *b = nullptr;  // nullptr: auto count of a
+};
+// refinement: cells per maximum separation (1..3), 0 automatic, -1 timed
+// choice among 1, 2 and 3.
+int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *bin, bool exact_fp64, int refinement,
+                 Batch **out, Error *err);
+// full_out[n_jobs * nb], region_out[n_jobs * n_jk * nb] (may be null): raw
+// sums as tpcf_count returns them, job after job.
+int batch_run(Batch *b, double *full_out, double *region_out, Stats *st, Error *err);
+int batch_refinement(const Batch *b);
+int batch_jobs(const Batch *b);
+void batch_destroy(Batch *b);
+
 // diag.cu
 int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err);
 

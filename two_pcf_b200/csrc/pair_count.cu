@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <limits>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <type_traits>
@@ -72,8 +73,17 @@ struct GridK {
     const double *unit;
 };
 
-struct KParams {
+// One (catalogue A, catalogue B, output histogram) of a launch; a batched
+// launch runs the work items of many jobs.
+struct JobK {
     GridK a, b;
+    int out;  // output slot: histograms at g_full + 2 nb out, g_sub + 2 nb n_jk out
+    int pad[3];
+};
+
+struct KParams {
+    const JobK *jobs;  // jackknife kernels: the job of each work item (batched launches)
+    JobK job0;         // kernels without jackknife regions: the launch's only job
     const WorkItem *items;
     const Segment *segs;
     int n_items;
@@ -162,8 +172,8 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     L.tile1 = o;
     o += tile_bytes(exact);
     o = (o + 15) / 16 * 16;
-    L.misc = o;
-    o += 64;
+    L.misc = o;  // item index, mbarriers, the item's job
+    o += 64 + sizeof(JobK);
     L.total = o;
     return L;
 }
@@ -360,9 +370,9 @@ __device__ __forceinline__ double upweight(const KParams &P, double v) {
 //   W_ANG_INVP (iw1 iw2) (n_runs / popc), float division (:742-764)
 // popc = float sum of the popcounts of mask1 & mask2, plus 1 when zero.
 template <int WK>
-__device__ __forceinline__ float pair_weight(const KParams &P, float wprod, int i, int j) {
+__device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, float wprod, int i, int j) {
     auto omct = [&]() {
-        const double *u1 = P.a.unit + 3 * (size_t)i, *u2 = P.b.unit + 3 * (size_t)j;
+        const double *u1 = J.a.unit + 3 * (size_t)i, *u2 = J.b.unit + 3 * (size_t)j;
         return omct_exact(u1[0], u1[1], u1[2], u2[0], u2[1], u2[2]);
     };
     if (WK == W_INVP_DR) return __double2float_rn(__dmul_rn((double)wprod, upweight(P, omct())));
@@ -391,8 +401,8 @@ __device__ __noinline__ void flag_nonfinite(const KParams &P, int bin, int ra, i
 // Add one binned pair: weight from the queue (product of the grid weights)
 // or, for the inverse-p kinds, formed here; fixed-point shared add.
 template <bool UNITW, int WK>
-__device__ __forceinline__ void add_binned(const KParams &P, const Shm &S, int bin, float wa, float wb, int ia,
-                                           int jb, int ka, int jl, int ra, int rb) {
+__device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, const Shm &S, int bin, float wa, float wb,
+                                           int ia, int jb, int ka, int jl, int ra, int rb) {
     if constexpr (WK == W_ADJ) {
         // the pair adds wa * wb to its bin: dL/dwa += G wb, dL/dwb += G wa
         const double g = S.G[bin];
@@ -402,7 +412,7 @@ __device__ __forceinline__ void add_binned(const KParams &P, const Shm &S, int b
     }
     float w = UNITW ? 1.0f : __fmul_rn(wa, wb);
     if (WK != W_PLAIN) {
-        w = pair_weight<WK>(P, w, P.a.idx[ia], P.b.idx[jb]);
+        w = pair_weight<WK>(P, J, w, J.a.idx[ia], J.b.idx[jb]);
         if (!isfinite(w)) {
             flag_nonfinite(P, bin, ra, rb, w);
             return;
@@ -419,7 +429,7 @@ __device__ __forceinline__ void add_binned(const KParams &P, const Shm &S, int b
 // the original arrays) come from the queue entry; ra/rb are the regions of
 // its two points.
 template <int MODE, bool UNITW, int WK>
-__device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA, const ExactArgs &E,
+__device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const PreciseArgs &PA, const ExactArgs &E,
                                          const Shm &S, const float4 *s_pos, const float4 *s_aux,
                                          const float4 *s_achunk, const float4 e, int a_start, int jbase, int ra,
                                          int rb, Counters &cnt) {
@@ -453,7 +463,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             bool inr;
             if (dev::near_edge(ax1, v, b, P.g_ang)) {
                 cnt.guard += 1;
-                b = exact_pair<MODE_ANGULAR>(E, S.t1, S.t2, P.a.idx[ia], P.b.idx[jb], &inr);
+                b = exact_pair<MODE_ANGULAR>(E, S.t1, S.t2, J.a.idx[ia], J.b.idx[jb], &inr);
             } else {
                 inr = b >= 0 && b < P.n1;
             }
@@ -461,7 +471,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
             if (!inr) return;
             bin = b;
         }
-        add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+        add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
         return;
     } else {
         if (MODE == MODE_SIGMA_PI) {
@@ -513,12 +523,12 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
         }
         if (amb) {
             bool inr, guarded;
-            bin = precise_bin<MODE>(PA, E, S.t1, S.t2, s2, pi, P.a.idx[ia], P.b.idx[jb], &inr, &guarded);
+            bin = precise_bin<MODE>(PA, E, S.t1, S.t2, s2, pi, J.a.idx[ia], J.b.idx[jb], &inr, &guarded);
             cnt.in_range += inr ? 1 : 0;
             cnt.guard += guarded ? 1 : 0;
             if (bin < 0) return;
         }
-        add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+        add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
     }
 }
 
@@ -526,7 +536,8 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const PreciseArgs &PA
 // d2), or for angular counts from its exact (float)(1 - cos(theta)) in d0;
 // ia/jb are its positions in the sorted grids.
 template <int MODE, bool UNITW, int WK>
-__device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, const Shm &S, float d0, float d1,
+__device__ __forceinline__ void bin_exact(const KParams &P, const JobK &J, const ExactArgs &E, const Shm &S, float d0,
+                                          float d1,
                                           float d2, int ia, int jb, int ka, int jl, int ra, int rb, Counters &cnt) {
     int bin;
     if constexpr (MODE == MODE_ANGULAR) {
@@ -535,8 +546,8 @@ __device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, 
     } else {
         double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
         if (MODE != MODE_MONOPOLE) {
-            const double4 u1 = P.a.unit_s[ia];
-            const double4 u2 = P.b.unit_s[jb];
+            const double4 u1 = J.a.unit_s[ia];
+            const double4 u2 = J.b.unit_s[jb];
             n1x = u1.x;
             n1y = u1.y;
             n1z = u1.z;
@@ -549,8 +560,8 @@ __device__ __forceinline__ void bin_exact(const KParams &P, const ExactArgs &E, 
         cnt.in_range += inr ? 1 : 0;
         if (bin < 0) return;
     }
-    const float wa = (float)P.a.xyz_s[ia].w, wb = (float)P.b.xyz_s[jb].w;
-    add_binned<UNITW, WK>(P, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+    const float wa = (float)J.a.xyz_s[ia].w, wb = (float)J.b.xyz_s[jb].w;
+    add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
 }
 
 // Add a 64-bit value held as two 32-bit words into another such pair (the
@@ -581,6 +592,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     float4 *s_achunk = (float4 *)(smem + L.achunk);
     int *s_item = (int *)(smem + L.misc);
     uint64_t *bar = (uint64_t *)(smem + L.misc + 16);
+    JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4 *s_q = (float4 *)(smem + L.queue) + warp * QCAP;
     const unsigned lt_mask = (1u << lane) - 1u;
@@ -613,26 +625,10 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     }
     __syncthreads();
 
-    const ExactArgs EA{P.a.xyz, P.a.unit, P.b.xyz, P.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2};
     const PreciseArgs PA{P.n1, P.n2, P.min_r_sq, P.max_r_sq, P.g_s2, P.g_pi, P.g_a, P.c1_mu, P.c2_mu, P.g_mu0};
     Counters cnt;
     unsigned long long n_cand = 0, n_flush = 0, tot_in = 0, tot_guard = 0;
     unsigned tcount = 0;  // tiles staged so far by this CTA (selects buffer and phase)
-
-    auto issue = [&](unsigned tc, int start, int len) {
-        unsigned char *dst = tile_base + (tc & 1) * tile_stride;
-        dev::fence_proxy_async();
-        if (EXACT) {
-            const uint32_t by = (uint32_t)len * 32u;
-            dev::mbar_expect_tx(&bar[tc & 1], by);
-            dev::bulk_g2s(dst, P.b.xyz_s + start, by, &bar[tc & 1]);
-        } else {
-            const uint32_t by = (uint32_t)len * 16u;
-            dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
-            dev::bulk_g2s(dst, P.b.pos + start, by, &bar[tc & 1]);
-            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TB * 16, P.b.aux + start, by, &bar[tc & 1]);
-        }
-    };
 
     for (;;) {
         if (tid == 0) {
@@ -644,6 +640,30 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         const int item = s_item[0];
         if (item >= P.n_items) break;
         const WorkItem it = P.items[item];
+        if constexpr (JK) {
+            // the item's job (grids and output slot), staged for every thread
+            const int *src = (const int *)(P.jobs + it.job);
+            int *dst = (int *)s_job;
+            for (int k = tid; k < (int)(sizeof(JobK) / 4); k += NT) dst[k] = src[k];
+            __syncthreads();
+        }
+        const JobK &J = JK ? *s_job : P.job0;
+        const ExactArgs EA{J.a.xyz, J.a.unit, J.b.xyz, J.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2};
+    auto issue = [&](unsigned tc, int start, int len) {
+        unsigned char *dst = tile_base + (tc & 1) * tile_stride;
+        dev::fence_proxy_async();
+        if (EXACT) {
+            const uint32_t by = (uint32_t)len * 32u;
+            dev::mbar_expect_tx(&bar[tc & 1], by);
+            dev::bulk_g2s(dst, J.b.xyz_s + start, by, &bar[tc & 1]);
+        } else {
+            const uint32_t by = (uint32_t)len * 16u;
+            dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
+            dev::bulk_g2s(dst, J.b.pos + start, by, &bar[tc & 1]);
+            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TB * 16, J.b.aux + start, by, &bar[tc & 1]);
+        }
+    };
+
         tot_in += cnt.in_range;
         tot_guard += cnt.guard;
         cnt.in_range = cnt.guard = 0;
@@ -659,7 +679,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
 
         // ---- A points: validity and indices; FP32 coordinates are
         // (re)loaded per segment in that segment's cell frame
-        const int3 ca = P.a.coord[it.a_cell];
+        const int3 ca = J.a.coord[it.a_cell];
         double dax[R], day[R], daz[R];
         int ai[R], apack[R];
 #pragma unroll
@@ -671,7 +691,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             ai[r] = valid ? gi : 0x7fffffff;
             dax[r] = day[r] = daz[r] = 1e300;
             if (EXACT && valid) {
-                const double4 p = P.a.xyz_s[gi];
+                const double4 p = J.a.xyz_s[gi];
                 dax[r] = p.x;
                 day[r] = p.y;
                 daz[r] = p.z;
@@ -683,9 +703,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             // consume step (pi, pair weight) at full warp occupancy
             for (int k = tid; k < it.a_len; k += NT) {
                 const int gi = it.a_start + k;
-                const float wk = P.a.pos[gi].w;
+                const float wk = J.a.pos[gi].w;
                 if (kNeedAux) {
-                    const float4 q = P.a.aux[gi];
+                    const float4 q = J.a.aux[gi];
                     s_achunk[k] = make_float4(q.x, q.y, q.z, wk);
                 } else {
                     s_achunk[k] = make_float4(0.f, 0.f, 0.f, wk);
@@ -706,10 +726,10 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                 n_cand += self ? (unsigned long long)(al * bl - al * (al + 1) / 2) : (unsigned long long)(al * bl);
             }
             // A coordinates in the frame of this segment's cell
-            const int3 cb = P.b.coord[sg.b_cell];
-            const float offx = (float)((double)((P.a.kmin0 + ca.x) - (P.b.kmin0 + cb.x)) * P.side);
-            const float offy = (float)((double)((P.a.kmin1 + ca.y) - (P.b.kmin1 + cb.y)) * P.side);
-            const float offz = (float)((double)((P.a.kmin2 + ca.z) - (P.b.kmin2 + cb.z)) * P.side);
+            const int3 cb = J.b.coord[sg.b_cell];
+            const float offx = (float)((double)((J.a.kmin0 + ca.x) - (J.b.kmin0 + cb.x)) * P.side);
+            const float offy = (float)((double)((J.a.kmin1 + ca.y) - (J.b.kmin1 + cb.y)) * P.side);
+            const float offz = (float)((double)((J.a.kmin2 + ca.z) - (J.b.kmin2 + cb.z)) * P.side);
             float ax[R], ay[R], az[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
@@ -717,7 +737,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                 // +inf and never passes the candidate test
                 ax[r] = ay[r] = az[r] = 1e30f;
                 if (!EXACT && ai[r] != 0x7fffffff) {
-                    const float4 p = P.a.pos[ai[r]];
+                    const float4 p = J.a.pos[ai[r]];
                     ax[r] = p.x + offx;
                     ay[r] = p.y + offy;
                     az[r] = p.z + offz;
@@ -784,7 +804,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 __syncwarp();
                                 const float4 e = s_q[qn - 32 + lane];
                                 const int pk = __float_as_int(e.w);
-                                bin_exact<MODE, UNITW, WK>(P, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
+                                bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
                                                            jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb,
                                                            cnt);
                                 __syncwarp();
@@ -797,7 +817,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         if (lane < qn) {
                             const float4 e = s_q[lane];
                             const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW, WK>(P, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
+                            bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
                                                        jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb, cnt);
                         }
                         __syncwarp();
@@ -842,7 +862,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 while (qn >= 32) {
                                     __syncwarp();
                                     const float4 e = s_q[qn - 32 + lane];
-                                    bin_fast<MODE, UNITW, WK>(P, PA, EA, S, s_pos,
+                                    bin_fast<MODE, UNITW, WK>(P, J, PA, EA, S, s_pos,
                                                               s_aux, s_achunk, e, it.a_start, jbase, it.a_region, rb,
                                                               cnt);
                                     __syncwarp();
@@ -857,7 +877,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     if (qn > 0) {
                         __syncwarp();
                         if (lane < qn)
-                            bin_fast<MODE, UNITW, WK>(P, PA, EA, S, s_pos, s_aux,
+                            bin_fast<MODE, UNITW, WK>(P, J, PA, EA, S, s_pos, s_aux,
                                                       s_achunk, s_q[lane], it.a_start, jbase, it.a_region, rb, cnt);
                         __syncwarp();
                     }
@@ -868,7 +888,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     const int jb0 = sg.b_start + tstart;
                     for (int t2 = tid; t2 < tlen; t2 += NT) {
                         const double v = S.gb[t2];
-                        if (v != 0.0) atomicAdd(&P.grad_b[P.b.idx[jb0 + t2]], v);
+                        if (v != 0.0) atomicAdd(&P.grad_b[J.b.idx[jb0 + t2]], v);
                         S.gb[t2] = 0.0;
                     }
                     __syncthreads();
@@ -885,7 +905,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
                         if (!v) continue;
                         add64_owned(s_alo, s_ahi, b, v);
-                        if (rb != it.a_region) dev::acc_add_global(P.g_sub, (size_t)rb * P.nb + b, v);
+                        if (rb != it.a_region) dev::acc_add_global(P.g_sub, ((size_t)J.out * P.n_jk + rb) * P.nb + b, v);
                         s_lo[b] = 0;
                         s_hi[b] = 0;
                     }
@@ -900,8 +920,8 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             for (int b = tid; b < P.nb; b += NT) {
                 const unsigned long long v = ((unsigned long long)s_ahi[b] << 32) | s_alo[b];
                 if (!v) continue;
-                dev::acc_add_global(P.g_full, b, v);
-                dev::acc_add_global(P.g_sub, (size_t)it.a_region * P.nb + b, v);
+                dev::acc_add_global(P.g_full, (size_t)J.out * P.nb + b, v);
+                dev::acc_add_global(P.g_sub, ((size_t)J.out * P.n_jk + it.a_region) * P.nb + b, v);
                 s_alo[b] = 0;
                 s_ahi[b] = 0;
             }
@@ -911,7 +931,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         if constexpr (ADJ) {
             for (int k = tid; k < it.a_len; k += NT) {
                 const double v = S.ga[k];
-                if (v != 0.0) atomicAdd(&P.grad_a[P.a.idx[it.a_start + k]], v);
+                if (v != 0.0) atomicAdd(&P.grad_a[J.a.idx[it.a_start + k]], v);
                 S.ga[k] = 0.0;
             }
             __syncthreads();
@@ -1340,6 +1360,7 @@ struct CountPlan {
     double inv = 1.0;  // 2^-S
     std::vector<WorkItem> items;
     std::vector<Segment> segs;
+    std::vector<JobK> jobs;  // one for a single count
     SmemLayout L;
     Luts luts;
     KParams P;
@@ -1359,7 +1380,72 @@ struct CountBuffers {
     unsigned *flags = nullptr;
     double *up_bins = nullptr, *up_centre = nullptr;
     double *adj_G = nullptr, *grad_a = nullptr, *grad_b = nullptr;
+    JobK *jobs = nullptr;
 };
+
+// Device view of one catalogue's grid.
+void fill_grid(GridK &k, const Grid &gr, const Catalog &c) {
+    k.pos = gr.pos.p;
+    k.aux = gr.aux.p;
+    k.idx = gr.idx.p;
+    k.xyz_s = gr.xyz_s.p;
+    k.unit_s = gr.unit_s.p;
+    k.coord = gr.cell_coord.p;
+    k.kmin0 = gr.kmin[0];
+    k.kmin1 = gr.kmin[1];
+    k.kmin2 = gr.kmin[2];
+    k.xyz = c.xyz.p;
+    k.unit = c.unit.p;
+}
+
+// Kernel parameters that depend on the binning, guards and tables only (not
+// on the catalogues or the work list).
+void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side, double tn, float wscale,
+                 int n_runs) {
+    KParams &P = C.P;
+    std::memset(&P, 0, sizeof(P));
+    P.n_items = (int)C.items.size();
+    P.side = side;
+    P.n1 = bin->nb1;
+    P.n2 = (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) ? bin->nb2 : 0;
+    P.nb = C.nb;
+    P.min_r_sq = bin->min_r_sq;
+    P.max_r_sq = bin->max_r_sq;
+    P.g_s2 = g.g_s2;
+    P.g_pi = g.g_pi;
+    P.g_a = g.g_a;
+    P.c1_mu = g.c1_mu;
+    P.c2_mu = g.c2_mu;
+    P.g_mu0 = g.g_mu0;
+    P.g_ang = g.g_ang;
+    P.s2_lut_min = C.luts.s2_lut_min;
+    if (C.angular) {
+        // candidate test on the squared chord: v = chord^2 / 2 < T[n] + g_ang
+        P.lo_cut = -1.0f;
+        P.hi_cut = (float)(2.0 * (tn + g.g_ang) * (1.0 + 1e-6));
+    } else {
+        P.lo_cut = bin->min_r_sq - g.g_s2;
+        P.hi_cut = bin->max_r_sq + g.g_s2;
+    }
+    // One compare: |s^2 - mid| < half, widened to cover the float rounding of
+    // mid, half and the subtraction.
+    P.cut_mid = (float)(0.5 * ((double)P.lo_cut + (double)P.hi_cut));
+    P.cut_half = (float)(0.5 * ((double)P.hi_cut - (double)P.lo_cut) * (1.0 + 1e-5) +
+                         1e-6 * std::fabs((double)P.cut_mid));
+    P.lut1_base = C.luts.base1;
+    P.lut_edge1 = C.luts.edge1 ? 1 : 0;
+    P.lut_edge2 = C.luts.edge2 ? 1 : 0;
+    P.lut2_scale = C.luts.scale2;
+    P.n_jk = C.n_jk;
+    P.wscale = wscale;
+    P.n_runs_f = (float)n_runs;
+    P.n_runs_d = (double)n_runs;
+    if (C.up) {
+        P.n_up = C.up->ax.n_bins;
+        P.up_min = (double)C.up->ax.min;
+        P.up_max = (double)C.up->ax.max;
+    }
+}
 
 int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Error *err) {
     const Binning *bin = req.bin;
@@ -1469,67 +1555,17 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     if (C.angular) g.g_ang = (float)((0.5 * g.g_s2 + 2.0 * norm_dev + 2e-15) * (1.0 + 1e-6));
     C.luts = build_luts(*bin, g);
 
+    fill_params(C, bin, g, side, tn, wscale, req.n_runs);
     KParams &P = C.P;
-    std::memset(&P, 0, sizeof(P));
-    auto fill = [&](GridK &k, const Grid &gr, const Catalog &c) {
-        k.pos = gr.pos.p;
-        k.aux = gr.aux.p;
-        k.idx = gr.idx.p;
-        k.xyz_s = gr.xyz_s.p;
-        k.unit_s = gr.unit_s.p;
-        k.coord = gr.cell_coord.p;
-        k.kmin0 = gr.kmin[0];
-        k.kmin1 = gr.kmin[1];
-        k.kmin2 = gr.kmin[2];
-        k.xyz = c.xyz.p;
-        k.unit = c.unit.p;
-    };
-    fill(P.a, *ga, *A);
-    fill(P.b, *gb, *B);
-    P.n_items = (int)C.items.size();
-    P.side = side;
-    P.n1 = bin->nb1;
-    P.n2 = (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) ? bin->nb2 : 0;
-    P.nb = C.nb;
-    P.min_r_sq = bin->min_r_sq;
-    P.max_r_sq = bin->max_r_sq;
-    P.g_s2 = g.g_s2;
-    P.g_pi = g.g_pi;
-    P.g_a = g.g_a;
-    P.c1_mu = g.c1_mu;
-    P.c2_mu = g.c2_mu;
-    P.g_mu0 = g.g_mu0;
-    P.g_ang = g.g_ang;
-    P.s2_lut_min = C.luts.s2_lut_min;
-    if (C.angular) {
-        // candidate test on the squared chord: v = chord^2 / 2 < T[n] + g_ang
-        P.lo_cut = -1.0f;
-        P.hi_cut = (float)(2.0 * (tn + g.g_ang) * (1.0 + 1e-6));
-    } else {
-        P.lo_cut = bin->min_r_sq - g.g_s2;
-        P.hi_cut = bin->max_r_sq + g.g_s2;
-    }
-    // One compare: |s^2 - mid| < half, widened to cover the float rounding of
-    // mid, half and the subtraction.
-    P.cut_mid = (float)(0.5 * ((double)P.lo_cut + (double)P.hi_cut));
-    P.cut_half = (float)(0.5 * ((double)P.hi_cut - (double)P.lo_cut) * (1.0 + 1e-5) +
-                         1e-6 * std::fabs((double)P.cut_mid));
-    P.lut1_base = C.luts.base1;
-    P.lut_edge1 = C.luts.edge1 ? 1 : 0;
-    P.lut_edge2 = C.luts.edge2 ? 1 : 0;
-    P.lut2_scale = C.luts.scale2;
-    P.n_jk = C.n_jk;
-    P.wscale = wscale;
+    JobK job;
+    std::memset(&job, 0, sizeof(job));
+    fill_grid(job.a, *ga, *A);
+    fill_grid(job.b, *gb, *B);
+    job.out = 0;
+    C.jobs.assign(1, job);
     P.a_masks = A->masks.p;
     P.b_masks = B->masks.p;
     P.n_mask = A->n_mask;
-    P.n_runs_f = (float)req.n_runs;
-    P.n_runs_d = (double)req.n_runs;
-    if (C.up) {
-        P.n_up = C.up->ax.n_bins;
-        P.up_min = (double)C.up->ax.min;
-        P.up_max = (double)C.up->ax.max;
-    }
     C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
     return 0;
 }
@@ -1547,6 +1583,7 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
                                  stm));
         TPCF_TRY(cudaMemcpyAsync(D.segs, C.segs.data(), sizeof(Segment) * C.segs.size(), cudaMemcpyHostToDevice, stm));
     }
+    TPCF_TRY(cudaMemcpyAsync(D.jobs, C.jobs.data(), sizeof(JobK) * C.jobs.size(), cudaMemcpyHostToDevice, stm));
     TPCF_TRY(cudaMemcpyAsync(D.t1, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
     if (!bin->t2.empty())
         TPCF_TRY(cudaMemcpyAsync(D.t2, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
@@ -1572,6 +1609,8 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     }
 
     KParams P = C.P;
+    P.jobs = D.jobs;
+    P.job0 = C.jobs[0];
     P.items = D.items;
     P.segs = D.segs;
     P.head = D.head;
@@ -1707,6 +1746,8 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
         TPCF_TRY(d_up_bins.alloc(C.n_up()));
         TPCF_TRY(d_up_centre.alloc(C.n_up()));
     }
+    DevBuf<JobK> d_jobs;
+    TPCF_TRY(d_jobs.alloc(C.jobs.size()));
     DevBuf<double> d_adj_G, d_grad_a, d_grad_b;
     if (C.adj) {
         TPCF_TRY(d_adj_G.alloc(C.nb));
@@ -1714,6 +1755,7 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
         if (!C.is_auto) TPCF_TRY(d_grad_b.alloc(std::max(C.n_b, 1)));
     }
     CountBuffers D;
+    D.jobs = d_jobs.p;
     D.adj_G = d_adj_G.p;
     D.grad_a = d_grad_a.p;
     D.grad_b = d_grad_b.p;
@@ -1734,6 +1776,300 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     D.up_centre = d_up_centre.p;
     return execute(ctx, C, D, full_out, region_out, st, err, true);
 }
+
+// ---------------------------------------------------------------------------
+// Batched counts.
+
+namespace {
+
+int plan_batch(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *bin, bool exact, int m, CountPlan &C,
+               Error *err) {
+    if (bin->mode == MODE_ANGULAR) {
+        err->status = 6;
+        err->msg = "batched counts are 3-D counts";
+        return err->status;
+    }
+    C.bin = bin;
+    C.nb = bin->nb;
+    C.n_jk = bin->n_jk;
+    C.jk = true;  // per-item flushes to each job's own histograms
+    C.wk = W_PLAIN;
+    bool unitw = true;
+    double wmax = 0;
+    for (const BatchJobSpec &j : jobs) {
+        const Catalog *A = j.a, *B = j.b ? j.b : j.a;
+        unitw = unitw && A->unit_weights && B->unit_weights;
+        wmax = std::max(wmax, (double)A->w_max * (double)B->w_max);
+    }
+    C.unitw = unitw;
+    const double rb = bin->rmax_bound;
+    const double side = rb / m * (1.0 + 1e-9);
+    GridSpec gs;
+    gs.side = side;
+    std::vector<long long> cost;
+    for (size_t j = 0; j < jobs.size(); ++j) {
+        Catalog *A = const_cast<Catalog *>(jobs[j].a);
+        Catalog *B = const_cast<Catalog *>(jobs[j].b ? jobs[j].b : jobs[j].a);
+        const bool is_auto = jobs[j].b == nullptr;
+        Grid *ga = nullptr, *gb = nullptr;
+        if (build_grid(ctx, A, gs, exact, &ga, err)) return err->status;
+        if (is_auto) gb = ga;
+        else if (build_grid(ctx, B, gs, exact, &gb, err)) return err->status;
+        JobK jk;
+        std::memset(&jk, 0, sizeof(jk));
+        fill_grid(jk.a, *ga, *A);
+        fill_grid(jk.b, *gb, *B);
+        jk.out = (int)j;
+        C.jobs.push_back(jk);
+        if (A->n_kept == 0 || B->n_kept == 0) continue;
+        std::vector<WorkItem> it;
+        std::vector<Segment> sg;
+        build_work_items(*ga, *gb, is_auto, m, side, rb, it, sg);
+        const int off = (int)C.segs.size();
+        for (WorkItem w : it) {
+            long long bl = 0;
+            for (int k = w.seg_begin; k < w.seg_end; ++k) bl += sg[k].b_len;
+            w.seg_begin += off;
+            w.seg_end += off;
+            w.job = (int)j;
+            C.items.push_back(w);
+            cost.push_back((long long)w.a_len * bl);
+        }
+        C.segs.insert(C.segs.end(), sg.begin(), sg.end());
+    }
+    // one longest-first order over every job's items
+    std::vector<int> order(C.items.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::vector<WorkItem> sorted(C.items.size());
+    for (size_t k = 0; k < order.size(); ++k) sorted[k] = C.items[order[k]];
+    C.items.swap(sorted);
+
+    float wscale = 1.0f;
+    if (!unitw) {
+        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
+        wscale = std::ldexp(1.0f, S);
+        C.inv = std::ldexp(1.0, -S);
+    }
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, exact, true);
+    if (C.L.total + 1024 > ctx->smem_optin) {
+        err->status = 6;
+        err->msg = "histogram does not fit in shared memory";
+        return err->status;
+    }
+    const Guards g = compute_guards(side, m, rb);
+    C.luts = build_luts(*bin, g);
+    fill_params(C, bin, g, side, 2.0, wscale, 0);
+    C.P.job0 = C.jobs[0];
+    C.fn = pick(bin->mode, W_PLAIN, unitw, true, exact);
+    return 0;
+}
+
+}  // namespace
+
+struct Batch {
+    Ctx *ctx = nullptr;
+    CountPlan C;
+    int m = 0, grid = 0;
+    size_t n_out = 0;
+    DevBuf<WorkItem> items;
+    DevBuf<Segment> segs;
+    DevBuf<JobK> jobs;
+    DevBuf<unsigned long long> full, sub, cnt;
+    DevBuf<int> head, err;
+    DevBuf<float> t1, t2;
+    DevBuf<unsigned char> l1, l2;
+    unsigned long long *h_full = nullptr, *h_sub = nullptr, *h_cnt = nullptr;  // pinned
+    int *h_err = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    ~Batch() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        if (h_full) cudaFreeHost(h_full);
+        if (h_sub) cudaFreeHost(h_sub);
+        if (h_cnt) cudaFreeHost(h_cnt);
+        if (h_err) cudaFreeHost(h_err);
+    }
+};
+
+namespace {
+
+// Plan, allocate and upload a batch for one refinement, then capture its
+// run (clears, the launch, the read-backs) as a CUDA graph.
+int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *bin, bool exact, int m,
+                std::unique_ptr<Batch> &out, Error *err) {
+    std::unique_ptr<Batch> B(new Batch());
+    B->ctx = ctx;
+    B->m = m;
+    CountPlan &C = B->C;
+    if (plan_batch(ctx, jobs, bin, exact, m, C, err)) return err->status;
+    B->n_out = C.jobs.size();
+    const size_t nb = C.nb, nj = C.n_jk;
+    cudaStream_t stm = ctx->stream;
+    TPCF_TRY(B->items.alloc(C.items.size()));
+    TPCF_TRY(B->segs.alloc(C.segs.size()));
+    TPCF_TRY(B->jobs.alloc(C.jobs.size()));
+    TPCF_TRY(B->full.alloc(2 * nb * B->n_out));
+    TPCF_TRY(B->sub.alloc(2 * nb * nj * B->n_out));
+    TPCF_TRY(B->cnt.alloc(4));
+    TPCF_TRY(B->head.alloc(1));
+    TPCF_TRY(B->err.alloc(1));
+    TPCF_TRY(B->t1.alloc(bin->t1.size()));
+    TPCF_TRY(B->t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
+    TPCF_TRY(B->l1.alloc(LUT1_N));
+    TPCF_TRY(B->l2.alloc(LUT2_N));
+    TPCF_TRY(cudaMallocHost((void **)&B->h_full, sizeof(unsigned long long) * 2 * nb * B->n_out));
+    TPCF_TRY(cudaMallocHost((void **)&B->h_sub, sizeof(unsigned long long) * 2 * nb * nj * B->n_out));
+    TPCF_TRY(cudaMallocHost((void **)&B->h_cnt, sizeof(unsigned long long) * 4));
+    TPCF_TRY(cudaMallocHost((void **)&B->h_err, sizeof(int)));
+    if (!C.items.empty()) {
+        TPCF_TRY(cudaMemcpyAsync(B->items.p, C.items.data(), sizeof(WorkItem) * C.items.size(),
+                                 cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(cudaMemcpyAsync(B->segs.p, C.segs.data(), sizeof(Segment) * C.segs.size(), cudaMemcpyHostToDevice,
+                                 stm));
+    }
+    TPCF_TRY(cudaMemcpyAsync(B->jobs.p, C.jobs.data(), sizeof(JobK) * C.jobs.size(), cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(B->t1.p, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
+    if (!bin->t2.empty())
+        TPCF_TRY(cudaMemcpyAsync(B->t2.p, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(B->l1.p, C.luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaMemcpyAsync(B->l2.p, C.luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(cudaStreamSynchronize(stm));
+
+    KParams P = C.P;
+    P.jobs = B->jobs.p;
+    P.items = B->items.p;
+    P.segs = B->segs.p;
+    P.head = B->head.p;
+    P.t1g = B->t1.p;
+    P.t2g = B->t2.p;
+    P.lut1g = B->l1.p;
+    P.lut2g = B->l2.p;
+    P.g_full = B->full.p;
+    P.g_sub = B->sub.p;
+    P.counters = B->cnt.p;
+    P.err = B->err.p;
+    TPCF_TRY(cudaFuncSetAttribute((const void *)C.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)C.L.total));
+    int per_sm = 1;
+    TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, C.fn, NT, C.L.total));
+    per_sm = std::max(per_sm, 1);
+    B->grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, std::max<long long>(C.items.size(), 1));
+
+    TPCF_TRY(cudaStreamBeginCapture(stm, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(B->full.p, 0, sizeof(unsigned long long) * 2 * nb * B->n_out, stm);
+    cudaMemsetAsync(B->sub.p, 0, sizeof(unsigned long long) * 2 * nb * nj * B->n_out, stm);
+    cudaMemsetAsync(B->cnt.p, 0, sizeof(unsigned long long) * 4, stm);
+    cudaMemsetAsync(B->head.p, 0, sizeof(int), stm);
+    cudaMemsetAsync(B->err.p, 0, sizeof(int), stm);
+    if (!C.items.empty()) C.fn<<<B->grid, NT, C.L.total, stm>>>(P);
+    cudaMemcpyAsync(B->h_full, B->full.p, sizeof(unsigned long long) * 2 * nb * B->n_out, cudaMemcpyDeviceToHost, stm);
+    cudaMemcpyAsync(B->h_sub, B->sub.p, sizeof(unsigned long long) * 2 * nb * nj * B->n_out, cudaMemcpyDeviceToHost,
+                    stm);
+    cudaMemcpyAsync(B->h_cnt, B->cnt.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm);
+    cudaMemcpyAsync(B->h_err, B->err.p, sizeof(int), cudaMemcpyDeviceToHost, stm);
+    TPCF_TRY(cudaStreamEndCapture(stm, &B->graph));
+    TPCF_TRY(cudaGraphInstantiate(&B->exec, B->graph, 0));
+    out = std::move(B);
+    return 0;
+}
+
+}  // namespace
+
+int batch_run(Batch *B, double *full_out, double *region_out, Stats *st, Error *err) {
+    Ctx *ctx = B->ctx;
+    const CountPlan &C = B->C;
+    cudaStream_t stm = ctx->stream;
+    cudaEvent_t e0, e1;
+    TPCF_TRY(cudaEventCreate(&e0));
+    TPCF_TRY(cudaEventCreate(&e1));
+    TPCF_TRY(cudaEventRecord(e0, stm));
+    TPCF_TRY(cudaGraphLaunch(B->exec, stm));
+    TPCF_TRY(cudaEventRecord(e1, stm));
+    TPCF_TRY(cudaStreamSynchronize(stm));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (!C.items.empty()) ++ctx->launches;
+    if (*B->h_err) {
+        err->status = 4;
+        err->msg = "device wait exceeded its iteration limit; results discarded";
+        return err->status;
+    }
+    const size_t nb = C.nb, nj = C.n_jk;
+    for (size_t k = 0; k < nb * B->n_out; ++k) full_out[k] = fixed_to_double(&B->h_full[2 * k], C.inv);
+    if (region_out)
+        for (size_t k = 0; k < nb * nj * B->n_out; ++k) region_out[k] = fixed_to_double(&B->h_sub[2 * k], C.inv);
+    if (st) {
+        st->candidates += B->h_cnt[0];
+        st->in_range += B->h_cnt[1];
+        st->guard += B->h_cnt[2];
+        st->overflow += B->h_cnt[3];
+        st->items += C.items.size();
+        st->ms_kernel += ms;
+    }
+    return 0;
+}
+
+int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *bin, bool exact_fp64, int refinement,
+                 Batch **out, Error *err) {
+    *out = nullptr;
+    if (jobs.empty()) {
+        err->status = 1;
+        err->msg = "empty batch";
+        return err->status;
+    }
+    std::vector<int> choices;
+    if (refinement > 0) {
+        choices.push_back(refinement);
+    } else if (refinement == 0) {
+        // as run_count: from the largest catalogue's mean density
+        const Catalog *big = jobs[0].a;
+        for (const BatchJobSpec &j : jobs) {
+            if (j.a->n_kept > big->n_kept) big = j.a;
+            if (j.b && j.b->n_kept > big->n_kept) big = j.b;
+        }
+        const double rb = bin->rmax_bound;
+        double vol = 1;
+        for (int k = 0; k < 3; ++k) vol *= std::max(big->hi_kept[k] - big->lo_kept[k], rb);
+        choices.push_back(big->n_kept * (rb / 2) * (rb / 2) * (rb / 2) / vol >= 256 ? 2 : 1);
+    } else {
+        choices = {1, 2, 3};
+    }
+    std::unique_ptr<Batch> best;
+    double best_ms = 0;
+    for (int m : choices) {
+        std::unique_ptr<Batch> b;
+        if (batch_build(ctx, jobs, bin, exact_fp64, m, b, err)) {
+            if (choices.size() > 1 && err->status == 6) continue;  // e.g. a grid too fine for this refinement
+            return err->status;
+        }
+        if (choices.size() > 1) {
+            // autotune: time one replay of each candidate refinement
+            std::vector<double> f(b->C.nb * b->n_out);
+            Stats st;
+            if (batch_run(b.get(), f.data(), nullptr, &st, err)) return err->status;
+            if (!best || st.ms_kernel < best_ms) {
+                best_ms = st.ms_kernel;
+                best = std::move(b);
+            }
+        } else {
+            best = std::move(b);
+        }
+    }
+    if (!best) {
+        err->status = 6;
+        err->msg = "no refinement could be planned";
+        return err->status;
+    }
+    *out = best.release();
+    return 0;
+}
+
+int batch_refinement(const Batch *b) { return b->m; }
+int batch_jobs(const Batch *b) { return (int)b->n_out; }
+void batch_destroy(Batch *b) { delete b; }
 
 // ---------------------------------------------------------------------------
 // Counting without device allocation.
@@ -1829,6 +2165,7 @@ int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double
     const size_t o_up_thr = sp.take(sizeof(float) * n_up);
     const size_t o_up_bins = sp.take(sizeof(double) * n_up);
     const size_t o_up_centre = sp.take(sizeof(double) * n_up);
+    const size_t o_jobs = sp.take(sizeof(JobK));
     auto too_big = [&](size_t n_items, size_t n_segs) {
         err->status = 6;
         err->msg = "count needs " + std::to_string(sp.total) + " bytes of scratch (" + std::to_string(nb) +
@@ -1864,6 +2201,7 @@ int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double
     D.up_thr = reinterpret_cast<float *>(p + o_up_thr);
     D.up_bins = reinterpret_cast<double *>(p + o_up_bins);
     D.up_centre = reinterpret_cast<double *>(p + o_up_centre);
+    D.jobs = reinterpret_cast<JobK *>(p + o_jobs);
     return execute(ctx, C, D, full_out, region_out, st, err, false);
 }
 

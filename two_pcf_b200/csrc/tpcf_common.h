@@ -47,7 +47,8 @@ struct WorkItem {
     int a_region;   // jackknife region of every A point of the item
     int seg_begin;  // segments [seg_begin, seg_end) in the segment array
     int seg_end;
-    int pad[2];
+    int job;     // which (catalogue A, catalogue B, output) of a batched launch
+    int pad;
 };
 
 struct Segment {
