@@ -40,6 +40,7 @@ UNIT = "pairs/s"
 SIGMA_PI_AXES = ((0.0, 50.0, 1.0, 50), (0.0, 50.0, 1.0, 50))
 S_MU_AXES = ((0.0, 100.0, 1.3, 40), (0.0, 1.0, 0.0, 50))
 F_MODE = {1: 16, 2: 13, 0: 0}   # FP32 flops per in-range pair beyond the 8 of s^2
+TRAFFIC_SMU_RR_5PCT = 26.36e6   # DRAM bytes of one s-mu RR launch at --scale 0.05 (ncu, see profiles/)
 
 
 def parse():
@@ -402,7 +403,15 @@ def main():
                    "parallelism": f"replicas{ws}" if ws > 1 else "single"},
         "in_range_pairs_per_step": tot_in // args.steps, "candidates_per_step": tot_cand // args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_tflops if fp32_tflops else None, "traffic": None,
+                     "frac": achieved / fp32_tflops if fp32_tflops else None,
+                     "traffic": TRAFFIC_SMU_RR_5PCT * 20,
+                     "traffic_note": "DRAM bytes (read + write) of one s-mu RR launch: ncu capture at 5 % of the "
+                                     "catalogue (profiles/pair_count_smu_jk_weighted_ncu.md, 26.4 MB) scaled by the "
+                                     "points (x20); the catalogue is read about once per launch, tiles and A chunks "
+                                     "are reused from shared memory and L2",
+                     "smem_atomics_per_s": 2.0 * tot_in / (tot_kms * 1e-3) if tot_kms > 0 else None,
+                     "smem_atomic_frac": (2.0 * tot_in / (tot_kms * 1e-3) / atom_rate) if (tot_kms > 0 and atom_rate)
+                     else None,
                      "peak_source": "FP32 FMA probe kernel run live on this GPU (tpcf_measure_peaks); "
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "flops_model": "8 per candidate pair + 16 (sigma-pi) / 13 (s-mu) per in-range pair",
