@@ -26,7 +26,7 @@ CXX = os.environ.get("TPCF_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["grid.cu", "pair_count.cu", "diag.cu"]
-CPP_SOURCES = ["axis.cpp", "capi.cpp"]
+CPP_SOURCES = ["axis.cpp", "capi.cpp", "worklist.cpp"]
 
 
 def _run(cmd):
@@ -64,7 +64,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         obj = os.path.join(BUILD_DIR, f + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
-            jobs.append([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-I", CSRC,
+            jobs.append([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp", "-I", CSRC,
                          "-I", os.path.join(CUDA_HOME, "include"), "-c", src, "-o", obj])
     with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
         outs = list(ex.map(_run, jobs))
@@ -73,7 +73,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
             sys.stdout.write(o)
     if jobs or not os.path.exists(LIB_PATH):
         tmp = LIB_PATH + ".tmp"
-        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static"])
+        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static", "-lgomp"])
         shutil.move(tmp, LIB_PATH)
     return LIB_PATH
 

@@ -206,6 +206,11 @@ int batch_refinement(const Batch *b);
 int batch_jobs(const Batch *b);
 void batch_destroy(Batch *b);
 
+// worklist.cpp: the work items of one (A, B) count with cells of `side`
+// (m cells per maximum separation rb), longest first.
+void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, double side, double rb,
+                      std::vector<WorkItem> &items, std::vector<Segment> &segs);
+
 // diag.cu
 int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err);
 

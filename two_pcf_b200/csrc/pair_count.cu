@@ -59,7 +59,7 @@ constexpr unsigned char LUT_AMB = 255;  // bucket within the guard of an edge
 constexpr unsigned char LUT_EDGE = 128;
 constexpr int kLutEdgeMaxBins = 126;
 constexpr uint32_t kWaitLimit = 1u << 22;
-constexpr long long kItemMaxB = 16384;  // B points per work item (load balance)
+static_assert(TA == kChunkA, "work items are built for chunks of kChunkA points");
 
 struct GridK {
     const float4 *pos;
@@ -498,20 +498,27 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
             if (!amb) cnt.in_range += 1;
             bin = (int)(c1 * P.n2 + c2);
         } else {
-            const unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, s2)], s2, S.t1, P.g_s2, P.lut_edge1, &amb);
+            // both table lookups first: the two load chains overlap
+            const unsigned raw1 = S.l1[lut1_index(P.lut1_base, s2)];
+            unsigned raw2 = 0;
+            float mu = 0.f, gmu = 0.f;
+            if (MODE == MODE_S_MU) {
+                const float inv_s = rsqrtf(s2);
+                mu = fabsf(pi) * inv_s;
+                gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
+                raw2 = S.l2[lut2_index(P.lut2_scale, mu)];
+            }
+            const unsigned c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
+            bool amb2 = false;
+            unsigned c2 = 0;
+            if (MODE == MODE_S_MU) c2 = lut_decode(raw2, mu, S.t2, gmu, P.lut_edge2, &amb2);
             if (c1 == LUT_INV) {
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
                 cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
                 return;
             }
-            unsigned c2 = 0;
             if (MODE == MODE_S_MU) {
-                const float inv_s = rsqrtf(s2);
-                const float mu = fabsf(pi) * inv_s;
-                const float gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
-                bool amb2;
-                c2 = lut_decode(S.l2[lut2_index(P.lut2_scale, mu)], mu, S.t2, gmu, P.lut_edge2, &amb2);
                 if (c2 == LUT_INV && !amb2 && !amb && s2 >= P.s2_lut_min) {
                     cnt.in_range += 1;
                     return;
@@ -1008,42 +1015,6 @@ KernelFn pick(int mode, int wk, bool unitw, bool jk, bool exact) {
     }
 }
 
-void decode_cell(const Grid &g, int id, int c[3]) {
-    if (g.morton) {
-        unsigned v = (unsigned)id;
-        for (int m = 0; m < 3; ++m) {
-            unsigned x = (v >> m) & 0x09249249u;
-            x = (x | (x >> 2)) & 0x030C30C3u;
-            x = (x | (x >> 4)) & 0x0300F00Fu;
-            x = (x | (x >> 8)) & 0x030000FFu;
-            x = (x | (x >> 16)) & 0x3ffu;
-            c[m] = (int)x;
-        }
-    } else {
-        c[0] = id / (g.dim[1] * g.dim[2]);
-        c[1] = (id / g.dim[2]) % g.dim[1];
-        c[2] = id % g.dim[2];
-    }
-}
-
-int encode_cell(const Grid &g, const int c[3]) {
-    for (int m = 0; m < 3; ++m)
-        if (c[m] < 0 || c[m] >= g.dim[m]) return -1;
-    if (g.morton) {
-        unsigned id = 0;
-        for (int m = 0; m < 3; ++m) {
-            unsigned x = (unsigned)c[m] & 0x3ffu;
-            x = (x | (x << 16)) & 0x030000FFu;
-            x = (x | (x << 8)) & 0x0300F00Fu;
-            x = (x | (x << 4)) & 0x030C30C3u;
-            x = (x | (x << 2)) & 0x09249249u;
-            id |= x << m;
-        }
-        return (int)id;
-    }
-    return (c[0] * g.dim[1] + c[1]) * g.dim[2] + c[2];
-}
-
 inline float f_from_bits(uint32_t u) {
     float f;
     std::memcpy(&f, &u, 4);
@@ -1101,109 +1072,6 @@ unsigned char lut_entry(const Category &cat, const std::vector<double> &edges, d
 
 }  // namespace
 
-// Work list.  For every (cell, region) run of A, the segments are the runs
-// of B in the cells whose boxes are closer than the maximum separation,
-// sorted by region; long A runs are split into chunks of TA points.  For an
-// auto count every unordered pair of points is visited once: a B run is a
-// segment of an A run when it starts after it in the sorted order, and the A
-// run's own segment starts at the chunk and keeps only j > i.
-void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, double side, double rb,
-                      std::vector<WorkItem> &items, std::vector<Segment> &segs) {
-    std::vector<int> offs;
-    for (int ox = -m; ox <= m; ++ox)
-        for (int oy = -m; oy <= m; ++oy)
-            for (int oz = -m; oz <= m; ++oz) {
-                double g2 = 0;
-                for (int o : {ox, oy, oz}) {
-                    double gap = std::max(std::abs(o) - 1, 0) * side * (1.0 - 1e-12);
-                    g2 += gap * gap;
-                }
-                if (g2 < rb * rb) {
-                    offs.push_back(ox);
-                    offs.push_back(oy);
-                    offs.push_back(oz);
-                }
-            }
-    items.clear();
-    segs.clear();
-    std::vector<Segment> cand;
-    std::vector<std::pair<long long, int>> cost;  // (cost, item)
-    for (int ca = 0; ca < ga.ncell; ++ca) {
-        const int a0 = ga.h_cell_start[ca], a1 = ga.h_cell_start[ca + 1];
-        if (a1 == a0) continue;
-        int c[3];
-        decode_cell(ga, ca, c);
-        const int ra0 = ga.h_region_start[ca], ra1 = ga.h_region_start[ca + 1];
-        for (int ra = ra0; ra < ra1; ++ra) {
-            const int s0 = ga.h_run_start[ra];
-            const int s1 = (ra + 1 < ra1) ? ga.h_run_start[ra + 1] : a1;
-            cand.clear();
-            for (size_t k = 0; k < offs.size(); k += 3) {
-                int cbv[3];
-                for (int mm = 0; mm < 3; ++mm) cbv[mm] = ga.kmin[mm] + c[mm] + offs[k + mm] - gb.kmin[mm];
-                const int cb = encode_cell(gb, cbv);
-                if (cb < 0) continue;
-                const int b0 = gb.h_cell_start[cb], b1 = gb.h_cell_start[cb + 1];
-                if (b1 == b0) continue;
-                if (is_auto && cb < ca) continue;
-                const int rb0 = gb.h_region_start[cb], rb1 = gb.h_region_start[cb + 1];
-                for (int rbk = rb0; rbk < rb1; ++rbk) {
-                    const int t0 = gb.h_run_start[rbk];
-                    const int t1 = (rbk + 1 < rb1) ? gb.h_run_start[rbk + 1] : b1;
-                    if (is_auto && t0 < s0) continue;
-                    Segment sg;
-                    sg.b_start = t0;
-                    sg.b_len = t1 - t0;
-                    sg.b_cell = cb;
-                    sg.meta = gb.h_regions[rbk] | ((is_auto && t0 == s0) ? (1 << 16) : 0);
-                    cand.push_back(sg);
-                }
-            }
-            if (cand.empty()) continue;
-            std::stable_sort(cand.begin(), cand.end(),
-                             [](const Segment &x, const Segment &y) { return (x.meta & 0xffff) < (y.meta & 0xffff); });
-            for (int s = s0; s < s1; s += TA) {
-                WorkItem w;
-                std::memset(&w, 0, sizeof(w));
-                w.a_start = s;
-                w.a_len = std::min(TA, s1 - s);
-                w.a_cell = ca;
-                w.a_region = ga.h_regions[ra];
-                w.seg_begin = (int)segs.size();
-                long long bl = 0;
-                for (Segment sg : cand) {
-                    if (sg.meta >> 16) {
-                        // the A run itself: j > i, starting at this chunk
-                        sg.b_len = sg.b_start + sg.b_len - s;
-                        sg.b_start = s;
-                    }
-                    // Close the item when it holds enough B points, so that a
-                    // count always splits into many more items than CTAs.
-                    if (bl > 0 && bl + sg.b_len > kItemMaxB) {
-                        w.seg_end = (int)segs.size();
-                        cost.push_back({(long long)w.a_len * bl, (int)items.size()});
-                        items.push_back(w);
-                        w.seg_begin = (int)segs.size();
-                        bl = 0;
-                    }
-                    bl += sg.b_len;
-                    segs.push_back(sg);
-                }
-                w.seg_end = (int)segs.size();
-                cost.push_back({(long long)w.a_len * bl, (int)items.size()});
-                items.push_back(w);
-            }
-        }
-    }
-    // Largest items first, so the dynamic queue ends balanced.
-    std::stable_sort(cost.begin(), cost.end(),
-                     [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
-                         return x.first > y.first;
-                     });
-    std::vector<WorkItem> sorted(items.size());
-    for (size_t k = 0; k < cost.size(); ++k) sorted[k] = items[cost[k].second];
-    items.swap(sorted);
-}
 
 #define TPCF_TRY(expr)                                                                        \
     do {                                                                                      \

@@ -33,6 +33,8 @@ constexpr int kMaxBins1D = 256;      // per axis
 constexpr int kMaxBinsTotal = 8192;  // per histogram
 constexpr int kMaxMaskInts = 32;     // 64-bit masks per object for inverse-p weights
 constexpr int kMaxRegions = 4096;    // jackknife regions
+constexpr int kChunkA = 1024;        // A points per work item (256 threads x 4)
+constexpr long long kItemMaxB = 16384;  // B points per work item (load balance)
 
 // One unit of device work: a chunk of one (cell, jackknife region) run of
 // catalogue A against a list of runs of catalogue B (its segments) from the
