@@ -281,6 +281,93 @@ double tpcf_ls_estimator(double dd, double dr, double rr);
 uint64_t tpcf_kernel_launches(const tpcf_ctx *ctx);
 int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s);
 
+/* ---------------------------------------------------------------------------
+ * The command-line flow around the counts (src/main.cpp:11-84): parameter
+ * file, redshift -> comoving distance, catalogue reader, result writers.
+ * Host-only; these calls need no device.  A failed call leaves its message in
+ * tpcf_host_last_error() of the calling thread.
+ * ------------------------------------------------------------------------- */
+typedef struct tpcf_params tpcf_params;
+typedef struct tpcf_cosmology tpcf_cosmology;
+typedef struct tpcf_host_catalog tpcf_host_catalog;
+
+const char *tpcf_host_last_error(void);
+
+/* Params(file) (src/io.cpp:16-237): a line that does not start with '#' and
+ * holds '=' is cut at its first '#' and split at its first '=', and every
+ * space is removed from key and value.  Numbers convert as std::stoi /
+ * std::stod do; a value they would reject fails the call
+ * (TPCF_E_INVALID_ARG).  Keys the file does not set read as 0 / "" (the
+ * reference leaves them uninitialised); n_jk_regions <= 1 reads as 1. */
+int tpcf_params_load(const char *path, tpcf_params **out);
+int tpcf_params_parse(const char *text, tpcf_params **out);
+int tpcf_params_destroy(tpcf_params *params);
+/* Fields by their parameter-file key.  get_int also reads the boolean keys
+ * (0/1).  get_string copies at most cap bytes including the terminator and
+ * returns the string's length, or a negative status. */
+int tpcf_params_get_double(const tpcf_params *params, const char *key, double *out);
+int tpcf_params_get_int(const tpcf_params *params, const char *key, int32_t *out);
+int tpcf_params_get_string(const tpcf_params *params, const char *key, char *out, int32_t cap);
+
+/* Cosmology(omega_m, h, z_min, z_max, z_save_step, z_oversample) and
+ * comov_dist (src/cosmology.cpp:11-100, src/dataset.cpp:110-126); the
+ * reference's program uses z_save_step = 1e-4, z_oversample = 100
+ * (src/main.cpp:40).  Outside [z_min, z_max'] comov_dist returns z_min or
+ * z_max' (the table's last z), as the reference does. */
+int tpcf_cosmology_create(double omega_m, double h, double z_min, double z_max, double z_save_step,
+                          int32_t z_oversample, tpcf_cosmology **out);
+int tpcf_cosmology_destroy(tpcf_cosmology *cosmo);
+int tpcf_cosmology_comov_dist(const tpcf_cosmology *cosmo, const double *z, int64_t n, double *out);
+
+/* Galaxy::set (src/galaxy.cpp:8-27) over n points: x_norm from ra/dec in
+ * degrees, xyz = d_comov * x_norm, or 0 where d_comov < 0. */
+int tpcf_galaxy_set(int64_t n, const double *ra_deg, const double *dec_deg, const double *d_comov, double *xyz,
+                    double *x_norm);
+/* The cartesian reader's transform (src/io.cpp:393-399): d_comov = |x|,
+ * x_norm = x / d_comov. */
+int tpcf_cartesian_set(int64_t n, const double *xyz, double *d_comov, double *x_norm);
+
+typedef enum { TPCF_CARTESIAN = 0, TPCF_EQUATORIAL = 1 } tpcf_coord_system;
+
+/* read_data_ascii (src/io.cpp:240-414), parsed in parallel.  Data lines are
+ * the non-empty lines not starting with '#'; fields are split at ',' if the
+ * line holds one, else at tabs if it holds one, else at spaces, empty pieces
+ * skipped.  Columns: x y z or ra dec z, then the weight if use_weights, then
+ * the jackknife region if n_jk_regions > 1.  A missing or unparsable field
+ * fails the call with its line number (the reference aborts or loops
+ * forever there).  cosmo is required for TPCF_EQUATORIAL. */
+int tpcf_read_ascii(const char *path, int coord_system, int use_weights, int32_t n_jk_regions,
+                    const tpcf_cosmology *cosmo, tpcf_host_catalog **out);
+int64_t tpcf_host_catalog_size(const tpcf_host_catalog *cat);
+/* Borrowed views, valid until the catalogue is destroyed: xyz[3n], x_norm[3n],
+ * d_comov[n], weight[n], jk_region[n] — the arguments tpcf_catalog_create takes. */
+int tpcf_host_catalog_arrays(const tpcf_host_catalog *cat, const double **xyz, const double **x_norm,
+                             const double **d_comov, const float **weight, const int32_t **jk_region);
+int tpcf_host_catalog_destroy(tpcf_host_catalog *cat);
+
+/* generate_sub_filename (src/io.cpp:628-641): the region number goes before
+ * the last '.' of the name.  Returns the length, or a negative status. */
+int tpcf_sub_filename(const char *filename, int64_t sub, char *out, int32_t cap);
+
+/* output_xi_1D / output_xi_2D with output type "ascii" (src/io.cpp:724-756,
+ * :832-853): writes filename with the full histograms and, when the region
+ * arrays are given, one file per jackknife region named by
+ * tpcf_sub_filename.  Columns as the reference writes them (bin index(es),
+ * centre(s), width(s), Landy-Szalay xi, DD, DR, RR; numbers as std::ostream
+ * prints a double by default).  dd/dr/rr are normalised histograms of
+ * tpcf_binning_total_bins(bin) values, the *_sub arrays n_jk * nb values.
+ * TPCF_ANGULAR binnings are refused (the reference writes those as HDF5). */
+int tpcf_write_xi_ascii(const char *filename, const tpcf_binning *bin, const double *dd, const double *dr,
+                        const double *rr, const double *dd_sub, const double *dr_sub, const double *rr_sub);
+
+/* The reference's program (src/main.cpp:11-84, plain build) on a parameter
+ * file: read both catalogues, then for each of plot_monopole, plot_sigma_pi,
+ * plot_s_mu count DD, DR and RR on the device, normalise and write the ASCII
+ * outputs (auto_correlate_*, src/correlators.cpp:127-459).  HDF5 catalogues
+ * and outputs are refused with TPCF_E_UNSUPPORTED (this build has no HDF5
+ * library).  log: 0 quiet, 1 one line per step on stderr. */
+int tpcf_run_param_file(const char *path, int device, int precision, int log);
+
 #ifdef __cplusplus
 }
 #endif

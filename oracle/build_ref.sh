@@ -11,6 +11,9 @@
 #                           -D_N_MASK_INTS=32, linked against the in-memory
 #                           HDF5 stand-in in oracle/hdf5_stub/ (libhdf5 is not
 #                           installed here)
+#   twopcf_ref              the reference's own command-line program (plain
+#                           build, src/main.cpp included), for end-to-end
+#                           comparisons of parameter file -> ASCII outputs
 #
 # Flags follow the reference makefile (makefile:3-7) with g++ in place of icc
 # (icc is not available): -O3 -std=c++11 -fopenmp.  -ffp-contract=off keeps
@@ -47,4 +50,7 @@ $CXX $FLAGS -D_HAVE_HDF5 -D_USE_INV_WEIGHTS -D_N_MASK_INTS=32 -I"$HERE/hdf5_stub
     -I"$REF/src/healpix" "$HERE/ref_harness.cpp" "$HERE/hdf5_stub/hdf5_stub.cpp" $SRCS \
     -o "$OUT/libtwopcf_ref_invp.so.tmp"
 mv "$OUT/libtwopcf_ref_invp.so.tmp" "$OUT/libtwopcf_ref_invp.so"
-echo "built $OUT/libtwopcf_ref_plain.so $OUT/libtwopcf_ref_invp.so"
+$CXX -O3 -std=c++11 -fopenmp -ffp-contract=off -w -D_ANGULAR_PI_DEFN -D_N_MASK_INTS=1 -I"$REF/src" \
+    -I"$REF/src/healpix" "$REF/src/main.cpp" $SRCS -o "$OUT/twopcf_ref.tmp"
+mv "$OUT/twopcf_ref.tmp" "$OUT/twopcf_ref"
+echo "built $OUT/libtwopcf_ref_plain.so $OUT/libtwopcf_ref_invp.so $OUT/twopcf_ref"

@@ -154,7 +154,7 @@ void ref_galaxy_set(const double *ra, const double *dec, const double *dcom, lon
 }
 
 // Params(file) (src/io.cpp:16-237) on the given text; returns the numeric
-// fields in a fixed order (see tests/test_host_params.py) — doubles first,
+// fields in a fixed order (see tests/test_ingest_cpu.py) — doubles first,
 // then ints.
 int ref_params_parse(const char *text, double *dbl, int *ints) {
     std::string path = write_temp_params(text);
@@ -171,6 +171,70 @@ int ref_params_parse(const char *text, double *dbl, int *ints) {
                p.calculate_angular_dr_invpweights, p.theta_n_bins, p.healpix_order, p.n_bitwise_runs};
     std::memcpy(dbl, d, sizeof(d));
     std::memcpy(ints, k, sizeof(k));
+    return 0;
+}
+
+// read_file(path, "ascii", cosmo, params) (src/io.cpp:597-626) with the
+// Params of the given text (coord_system, use_weights, n_jk_regions and the
+// cosmology as src/main.cpp:39-45 sets them up).  Returns the number of
+// points; the outputs are written only when cap >= that number.
+long long ref_read_ascii(const char *param_text, const char *path, long long cap, double *x_out,
+                         double *xnorm_out, double *dcom_out, float *weight_out, int *jk_out) {
+    std::string ppath = write_temp_params(param_text);
+    if (ppath.empty()) return -1;
+    Quiet q;
+    Params p(ppath);
+    std::remove(ppath.c_str());
+    Cosmology *cosmo = NULL;
+    if (p.coord_system == "equatorial") cosmo = new Cosmology(p.omega_m, p.h, p.z_min, p.z_max, 0.0001, 100);
+    GalaxyCatalogue *cat = read_file(path, "ascii", cosmo, p);
+    delete cosmo;
+    long long n = cat ? cat->n_gals : -1;
+    if (cat && cap >= n) {
+        for (long long i = 0; i < n; ++i) {
+            const Galaxy &g = cat->gals[i];
+            for (int m = 0; m < 3; ++m) { x_out[3 * i + m] = g.x[m]; xnorm_out[3 * i + m] = g.x_norm[m]; }
+            dcom_out[i] = g.d_comov;
+            weight_out[i] = g.weight;
+            jk_out[i] = g.jk_region;
+        }
+    }
+    delete cat;
+    return n;
+}
+
+// output_xi_1D (mode 0) / output_xi_2D (mode 1 sigma-pi, 2 s-mu) with file
+// type "ascii" (src/io.cpp:724-756, :832-853) on histograms given as arrays;
+// axp = {min1, max1, base1, min2, max2, base2} as the Params doubles, the
+// histograms built as the auto_correlate_* drivers build them
+// (src/correlators.cpp:131, :284-285, :436-437).
+int ref_write_xi(const char *filename, int mode, const double *axp, int nb1, int nb2, int n_jk, const double *dd,
+                 const double *dr, const double *rr, const double *dd_sub, const double *dr_sub,
+                 const double *rr_sub) {
+    Quiet q;
+    const double *src[3][2] = {{dd, dd_sub}, {dr, dr_sub}, {rr, rr_sub}};
+    if (mode == 0) {
+        Hist tmp(axp[0], axp[1], nb1, axp[2]);
+        JKHists h0(n_jk, tmp), h1(n_jk, tmp), h2(n_jk, tmp);
+        JKHists *h[3] = {&h0, &h1, &h2};
+        for (int k = 0; k < 3; ++k) {
+            std::memcpy(h[k]->full_hist.bins, src[k][0], sizeof(double) * nb1);
+            std::memcpy(h[k]->sub_hist, src[k][1], sizeof(double) * nb1 * n_jk);
+        }
+        output_xi_1D(filename, "ascii", &h0, &h1, &h2, NULL, NULL);
+    } else {
+        Hist2D tmp = (mode == 1) ? Hist2D(axp[0], axp[1], nb1, axp[2], axp[3], axp[4], nb2, axp[5])
+                                 : Hist2D(axp[0], axp[1], nb1, axp[2], 0.0, 1.0, nb2, 0);
+        JKHists2D h0(n_jk, tmp), h1(n_jk, tmp), h2(n_jk, tmp);
+        JKHists2D *h[3] = {&h0, &h1, &h2};
+        const int nb = nb1 * nb2;
+        for (int k = 0; k < 3; ++k) {
+            std::memcpy(h[k]->full_hist.bins, src[k][0], sizeof(double) * nb);
+            std::memcpy(h[k]->sub_hist, src[k][1], sizeof(double) * nb * n_jk);
+        }
+        output_xi_2D(filename, "ascii", mode == 1 ? "sigma" : "s", mode == 1 ? "pi" : "mu", &h0, &h1, &h2, NULL,
+                     NULL);
+    }
     return 0;
 }
 

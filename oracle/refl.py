@@ -72,6 +72,10 @@ def plain():
         vp = C.c_void_p
         lib.ref_count_3d.argtypes = [C.c_int, C.c_int, vp, vp, vp, vp, vp, C.c_int, vp, vp, vp, vp, vp,
                                      C.c_int, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _ip]
+        lib.ref_read_ascii.argtypes = [C.c_char_p, C.c_char_p, C.c_longlong, vp, vp, vp, vp, vp]
+        lib.ref_read_ascii.restype = C.c_longlong
+        lib.ref_write_xi.argtypes = [C.c_char_p, C.c_int, _dp, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, _dp,
+                                     _dp]
         _PLAIN = lib
     return _PLAIN
 
@@ -140,6 +144,26 @@ def params_parse(text: str):
     if rc != 0:
         raise RuntimeError("ref_params_parse failed")
     return d, k
+
+
+def read_ascii(param_text: str, path: str) -> dict:
+    """read_file(path, "ascii", cosmo, Params(param_text)): the Galaxy fields."""
+    L = plain()
+    n = L.ref_read_ascii(param_text.encode(), str(path).encode(), -1, None, None, None, None, None)
+    if n < 0:
+        raise RuntimeError("ref_read_ascii failed")
+    out = {"xyz": np.empty((n, 3)), "x_norm": np.empty((n, 3)), "d_comov": np.empty(n),
+           "weight": np.empty(n, np.float32), "jk": np.empty(n, np.int32)}
+    L.ref_read_ascii(param_text.encode(), str(path).encode(), n, *[_ptr(out[k]) for k in
+                                                                  ("xyz", "x_norm", "d_comov", "weight", "jk")])
+    return out
+
+
+def write_xi(filename: str, mode: int, axp, nb1: int, nb2: int, n_jk: int, dd, dr, rr, dd_sub, dr_sub, rr_sub):
+    """output_xi_1D (mode 0) / output_xi_2D (1 sigma-pi, 2 s-mu), file type "ascii"."""
+    arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (dd, dr, rr, dd_sub, dr_sub, rr_sub)]
+    plain().ref_write_xi(str(filename).encode(), int(mode), np.ascontiguousarray(axp, dtype=np.float64), nb1, nb2,
+                         n_jk, *arrs)
 
 
 def normalise(is_auto, w1, jk1, w2, jk2, n_jk, full, sub):

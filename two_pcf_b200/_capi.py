@@ -87,7 +87,31 @@ _PROTOTYPES = {
     "tpcf_ls_estimator": (C.c_double, [C.c_double, C.c_double, C.c_double]),
     "tpcf_kernel_launches": (C.c_uint64, [_vp]),
     "tpcf_measure_peaks": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+    # command-line flow (host only)
+    "tpcf_host_last_error": (C.c_char_p, []),
+    "tpcf_params_load": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "tpcf_params_parse": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),
+    "tpcf_params_destroy": (C.c_int, [_vp]),
+    "tpcf_params_get_double": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_double)]),
+    "tpcf_params_get_int": (C.c_int, [_vp, C.c_char_p, C.POINTER(C.c_int32)]),
+    "tpcf_params_get_string": (C.c_int, [_vp, C.c_char_p, C.c_char_p, C.c_int32]),
+    "tpcf_cosmology_create": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32,
+                                        C.POINTER(_vp)]),
+    "tpcf_cosmology_destroy": (C.c_int, [_vp]),
+    "tpcf_cosmology_comov_dist": (C.c_int, [_vp, _vp, C.c_int64, _vp]),
+    "tpcf_galaxy_set": (C.c_int, [C.c_int64, _vp, _vp, _vp, _vp, _vp]),
+    "tpcf_cartesian_set": (C.c_int, [C.c_int64, _vp, _vp, _vp]),
+    "tpcf_read_ascii": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int32, _vp, C.POINTER(_vp)]),
+    "tpcf_host_catalog_size": (C.c_int64, [_vp]),
+    "tpcf_host_catalog_arrays": (C.c_int, [_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                                           C.POINTER(_vp)]),
+    "tpcf_host_catalog_destroy": (C.c_int, [_vp]),
+    "tpcf_sub_filename": (C.c_int, [C.c_char_p, C.c_int64, C.c_char_p, C.c_int32]),
+    "tpcf_write_xi_ascii": (C.c_int, [C.c_char_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "tpcf_run_param_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int]),
 }
+
+CARTESIAN, EQUATORIAL = 0, 1
 
 _LIB = None
 

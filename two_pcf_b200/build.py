@@ -26,7 +26,9 @@ CXX = os.environ.get("TPCF_CXX", "g++")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_SOURCES = ["grid.cu", "pair_count.cu", "diag.cu"]
-CPP_SOURCES = ["axis.cpp", "capi.cpp", "worklist.cpp"]
+CPP_SOURCES = ["axis.cpp", "capi.cpp", "worklist.cpp", "ingest.cpp", "capi_host.cpp", "driver.cpp"]
+CLI_SOURCE = "two_pcf_main.cpp"
+CLI_PATH = os.path.join(LIB_DIR, "two_pcf")
 
 
 def _run(cmd):
@@ -75,6 +77,11 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         tmp = LIB_PATH + ".tmp"
         _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static", "-lgomp"])
         shutil.move(tmp, LIB_PATH)
+    cli_src = os.path.join(CSRC, CLI_SOURCE)
+    if _stale(CLI_PATH, [cli_src, LIB_PATH] + headers):
+        tmp = CLI_PATH + ".tmp"
+        _run([CXX, "-O2", "-std=c++17", cli_src, "-o", tmp, "-L", LIB_DIR, "-ltpcf_b200", "-Wl,-rpath,$ORIGIN"])
+        shutil.move(tmp, CLI_PATH)
     return LIB_PATH
 
 

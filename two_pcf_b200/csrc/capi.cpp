@@ -11,24 +11,7 @@
 #include <new>
 #include <vector>
 
-#include "engine.h"
-
-struct tpcf_ctx {
-    tpcf::Ctx c;
-};
-struct tpcf_catalog {
-    tpcf::Catalog c;
-};
-struct tpcf_binning {
-    tpcf::Binning b;
-};
-struct tpcf_batch {
-    tpcf_ctx *ctx = nullptr;
-    tpcf::Batch *b = nullptr;
-    ~tpcf_batch() {
-        if (b) tpcf::batch_destroy(b);
-    }
-};
+#include "capi_types.h"
 
 namespace {
 

@@ -1,0 +1,213 @@
+// The reference's program on a parameter file (src/main.cpp:11-84, plain
+// build), with the pair counts on the device: tpcf_run_param_file.
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <memory>
+#include <string>
+#include <vector>
+
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "capi_types.h"
+#include "ingest.h"
+
+namespace {
+
+struct Log {
+    int level;
+    std::chrono::steady_clock::time_point t0 = std::chrono::steady_clock::now();
+    void operator()(const char *fmt, ...) const {
+        if (!level) return;
+        double s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        std::fprintf(stderr, "[two_pcf %8.3f s] ", s);
+        va_list ap;
+        va_start(ap, fmt);
+        std::vfprintf(stderr, fmt, ap);
+        va_end(ap);
+        std::fputc('\n', stderr);
+    }
+};
+
+struct Err {
+    int status = TPCF_OK;
+    std::string msg;
+    bool set(int st, const std::string &m) {
+        status = st;
+        msg = m;
+        return false;
+    }
+};
+
+struct CtxDel {
+    void operator()(tpcf_ctx *c) const { tpcf_destroy(c); }
+};
+struct CatDel {
+    void operator()(tpcf_catalog *c) const { tpcf_catalog_destroy(c); }
+};
+struct BinDel {
+    void operator()(tpcf_binning *b) const { tpcf_binning_destroy(b); }
+};
+using CtxPtr = std::unique_ptr<tpcf_ctx, CtxDel>;
+using CatPtr = std::unique_ptr<tpcf_catalog, CatDel>;
+using BinPtr = std::unique_ptr<tpcf_binning, BinDel>;
+
+// read_file (src/io.cpp:597-626) for the file types this build reads.
+bool read_catalogue(const tpcf::Params &p, const std::string &name, const std::string &type,
+                    const tpcf::CosmologyTable *cosmo, tpcf::HostCatalogue &out, Err &e) {
+    if (type == "hdf5")
+        return e.set(TPCF_E_UNSUPPORTED, name + ": HDF5 catalogues need the HDF5 library, which this build lacks");
+    if (type != "ascii") return e.set(TPCF_E_INVALID_ARG, "unknown file type '" + type + "' for " + name);
+    tpcf::Coords c;
+    if (p.coord_system == "cartesian") c = tpcf::Coords::Cartesian;
+    else if (p.coord_system == "equatorial") c = tpcf::Coords::Equatorial;
+    else return e.set(TPCF_E_INVALID_ARG, "unknown coord_system '" + p.coord_system + "'");
+    std::string err;
+    if (!tpcf::read_ascii(name, c, p.use_weights, p.n_jk_regions, cosmo, out, err))
+        return e.set(TPCF_E_INVALID_ARG, err);
+    return true;
+}
+
+bool upload(tpcf_ctx *ctx, const tpcf::HostCatalogue &h, int n_jk, CatPtr &out, Err &e) {
+    tpcf_catalog *c = nullptr;
+    int rc = tpcf_catalog_create(ctx, h.size(), h.xyz.data(), h.x_norm.data(), h.d_comov.data(), h.weight.data(),
+                                 nullptr, n_jk > 1 ? h.jk_region.data() : nullptr, n_jk, nullptr, 0, &c);
+    if (rc) return e.set(rc, std::string("catalogue upload: ") + tpcf_last_error(ctx));
+    out.reset(c);
+    return true;
+}
+
+// One auto_correlate_* (src/correlators.cpp:127-153, :280-307, :432-459):
+// DD, DR, RR in the reference's convention (jackknife-inverted, auto counts
+// doubled), each normalised, then the ASCII outputs.
+bool correlate(tpcf_ctx *ctx, const char *what, int mode, const tpcf_axis_spec &a1, const tpcf_axis_spec *a2,
+               int n_jk, tpcf_catalog *data, tpcf_catalog *rand, int precision, const std::string &filename,
+               const std::string &output_type, const Log &log, Err &e) {
+    if (output_type == "hdf5")
+        return e.set(TPCF_E_UNSUPPORTED, std::string(what) + ": HDF5 output needs the HDF5 library, which this build lacks");
+    if (output_type != "ascii")
+        return e.set(TPCF_E_INVALID_ARG, std::string(what) + ": unknown output type '" + output_type + "'");
+    tpcf_binning *b = nullptr;
+    int rc = tpcf_binning_create(ctx, mode, &a1, a2, n_jk, &b);
+    if (rc) return e.set(rc, std::string(what) + " binning: " + tpcf_last_error(ctx));
+    BinPtr bin(b);
+    const int nb = tpcf_binning_total_bins(b);
+    std::vector<double> full[3], sub[3];
+    for (int k = 0; k < 3; ++k) {
+        full[k].assign(nb, 0.0);
+        sub[k].assign((size_t)n_jk * nb, 0.0);
+    }
+    tpcf_stats st[3];
+    log("%s: DD", what);
+    rc = tpcf_auto_pair_count(ctx, data, b, precision, full[0].data(), sub[0].data(), &st[0]);
+    if (!rc) rc = tpcf_normalise_auto(data, nb, full[0].data(), sub[0].data());
+    if (!rc) {
+        log("%s: DR", what);
+        rc = tpcf_cross_pair_count(ctx, data, rand, b, precision, full[1].data(), sub[1].data(), &st[1]);
+    }
+    if (!rc) rc = tpcf_normalise_cross(data, rand, nb, full[1].data(), sub[1].data());
+    if (!rc) {
+        log("%s: RR", what);
+        rc = tpcf_auto_pair_count(ctx, rand, b, precision, full[2].data(), sub[2].data(), &st[2]);
+    }
+    if (!rc) rc = tpcf_normalise_auto(rand, nb, full[2].data(), sub[2].data());
+    if (rc) return e.set(rc, std::string(what) + ": " + tpcf_last_error(ctx));
+    log("%s: %.3e + %.3e + %.3e pairs in range, kernels %.1f + %.1f + %.1f ms", what, (double)st[0].in_range,
+        (double)st[1].in_range, (double)st[2].in_range, st[0].ms_kernel, st[1].ms_kernel, st[2].ms_kernel);
+    rc = tpcf_write_xi_ascii(filename.c_str(), b, full[0].data(), full[1].data(), full[2].data(), sub[0].data(),
+                             sub[1].data(), sub[2].data());
+    if (rc) return e.set(rc, std::string(what) + ": " + tpcf_host_last_error());
+    log("%s: wrote %s and %d region files", what, filename.c_str(), n_jk);
+    return true;
+}
+
+bool run(const char *path, int device, int precision, const Log &log, Err &e) {
+    tpcf::Params p;
+    std::string err;
+    if (!tpcf::load_params(path, p, err)) return e.set(TPCF_E_INVALID_ARG, err);
+#ifdef _OPENMP
+    if (p.n_threads > 0) omp_set_num_threads(p.n_threads);
+#endif
+    std::unique_ptr<tpcf::CosmologyTable> cosmo;
+    if (p.coord_system == "equatorial") {
+        cosmo.reset(new tpcf::CosmologyTable());
+        if (!tpcf::make_cosmology(p.omega_m, p.h, p.z_min, p.z_max, 0.0001, 100, *cosmo, err))
+            return e.set(TPCF_E_INVALID_ARG, err);
+    }
+    tpcf::HostCatalogue hd, hr;
+    if (!read_catalogue(p, p.data_filename, p.data_file_type, cosmo.get(), hd, e)) return false;
+    log("read %lld data points from %s", (long long)hd.size(), p.data_filename.c_str());
+    if (!read_catalogue(p, p.random_filename, p.random_file_type, cosmo.get(), hr, e)) return false;
+    log("read %lld random points from %s", (long long)hr.size(), p.random_filename.c_str());
+
+    // Each auto_correlate_* re-partitions the catalogues that the previous
+    // one's GalaxyBoxes left permuted in place; with points at d_comov < 0 the
+    // partition's early stop can then keep a different set, which is not
+    // reproduced here.
+    const int n_modes = (int)p.plot_monopole + (int)p.plot_sigma_pi + (int)p.plot_s_mu;
+    auto has_negative = [](const tpcf::HostCatalogue &h) {
+        for (double d : h.d_comov)
+            if (d < 0.0) return true;
+        return false;
+    };
+    if (n_modes > 1 && (has_negative(hd) || has_negative(hr)))
+        return e.set(TPCF_E_UNSUPPORTED,
+                     "catalogue points with d_comov < 0 and more than one of plot_monopole / plot_sigma_pi / "
+                     "plot_s_mu: run the modes one per parameter file");
+
+    tpcf_ctx *c = nullptr;
+    int rc = tpcf_create(device, &c);
+    if (rc) return e.set(rc, "device context: " + std::string(c ? tpcf_last_error(c) : tpcf_status_string(rc)));
+    CtxPtr ctx(c);
+    CatPtr data, rand;
+    if (!upload(c, hd, p.n_jk_regions, data, e) || !upload(c, hr, p.n_jk_regions, rand, e)) return false;
+    log("catalogues on device %d: %lld + %lld points kept", device, (long long)tpcf_catalog_n_used(data.get()),
+        (long long)tpcf_catalog_n_used(rand.get()));
+
+    if (p.plot_monopole) {
+        tpcf_axis_spec a{p.monopole_min, p.monopole_max, p.monopole_log_base, p.monopole_n_bins};
+        if (!correlate(c, "monopole", TPCF_MONOPOLE, a, nullptr, p.n_jk_regions, data.get(), rand.get(), precision,
+                       p.monopole_filename, p.monopole_output_type, log, e))
+            return false;
+    }
+    if (p.plot_sigma_pi) {
+        tpcf_axis_spec a{p.sigma_min, p.sigma_max, p.sigma_log_base, p.sigma_n_bins};
+        tpcf_axis_spec b{p.pi_min, p.pi_max, p.pi_log_base, p.pi_n_bins};
+        if (!correlate(c, "sigma-pi", TPCF_SIGMA_PI, a, &b, p.n_jk_regions, data.get(), rand.get(), precision,
+                       p.sigma_pi_filename, p.sigma_pi_output_type, log, e))
+            return false;
+    }
+    if (p.plot_s_mu) {
+        tpcf_axis_spec a{p.s_min, p.s_max, p.s_log_base, p.s_n_bins};
+        tpcf_axis_spec b{0.0, 1.0, 0.0, p.mu_n_bins};
+        if (!correlate(c, "s-mu", TPCF_S_MU, a, &b, p.n_jk_regions, data.get(), rand.get(), precision,
+                       p.s_mu_filename, p.s_mu_output_type, log, e))
+            return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+extern "C" int tpcf_run_param_file(const char *path, int device, int precision, int log_level) {
+    if (!path) {
+        tpcf::set_host_error("NULL parameter file path");
+        return TPCF_E_INVALID_ARG;
+    }
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) {
+        tpcf::set_host_error("bad precision");
+        return TPCF_E_INVALID_ARG;
+    }
+    Log log{log_level};
+    Err e;
+    try {
+        if (run(path, device, precision, log, e)) return TPCF_OK;
+    } catch (const std::bad_alloc &) {
+        e.status = TPCF_E_OOM;
+        e.msg = "out of host memory";
+    }
+    tpcf::set_host_error(e.msg);
+    return e.status ? e.status : TPCF_E_INVALID_ARG;
+}
