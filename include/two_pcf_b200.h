@@ -146,7 +146,12 @@ typedef enum {
     /* Inverse-p DR: 3-D weight1 * weight2 * angular up-weight
      * (cross_pair_count_*_invpweights); angular weight1 * weight2 over points
      * with d_comov >= 0 (cross_pair_count_angular_invpweights). */
-    TPCF_WEIGHTS_INVP_DR = 2
+    TPCF_WEIGHTS_INVP_DR = 2,
+    /* TPCF_WEIGHTS_INVP_DD of the build with _USE_DITHER_WEIGHTS
+     * (src/correlators_invpweight.cpp:62-71, :749-757): n_bitwise_runs is
+     * replaced per pair by the popcount of dither_mask1 & dither_mask2 (1 when
+     * none).  Both catalogues need dither masks (tpcf_catalog_set_dither_masks). */
+    TPCF_WEIGHTS_INVP_DD_DITHER = 3
 } tpcf_weighting;
 
 typedef struct {
@@ -193,6 +198,29 @@ int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog
 /* Replace a catalogue's weights (n floats, Galaxy::weight) in place: the
  * device copy and every cached cell grid.  Positions and grids are kept. */
 int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight);
+
+/* Galaxy::dither_mask of the _USE_DITHER_WEIGHTS build (src/galaxy.h:28-30):
+ * n * n_mask_ints int64 words, object-major, the width of the catalogue's
+ * bitmasks. */
+int tpcf_catalog_set_dither_masks(tpcf_catalog *cat, const int64_t *dither_mask);
+
+/* Line of sight of pi in TPCF_SIGMA_PI and TPCF_S_MU binnings.
+ * TPCF_LOS_ANGULAR (default): pi = (x1 - x2) . (x_norm1 + x_norm2) / 2, the
+ * reference's default build (_ANGULAR_PI_DEFN, src/correlators.cpp:166-170).
+ * TPCF_LOS_MIDPOINT: pi = (x1 - x2) . (x1 + x2) / |x1 + x2|, its build
+ * without that flag (:172-182); counted with the exact sequence for every
+ * candidate in either precision. */
+typedef enum { TPCF_LOS_ANGULAR = 0, TPCF_LOS_MIDPOINT = 1 } tpcf_line_of_sight;
+int tpcf_binning_set_line_of_sight(tpcf_binning *bin, int line_of_sight);
+
+/* The inverse-p build's reading of the bitwise weights
+ * (read_data_hdf5, src/io.cpp:519-586), on arrays: input_weight = weight;
+ * total = popcount of the object's n_mask_ints mask words (1 when 0); where
+ * total != n_bitwise_runs, weight *= n_bitwise_runs / total in double
+ * (with dither_mask, not NULL: weight *= popcount(dither) / total).
+ * weight[n] is updated in place; input_weight[n] receives the old values. */
+int tpcf_iip_weights(int64_t n, int32_t n_mask_ints, const int64_t *bitmask, const int64_t *dither_mask,
+                     int32_t n_bitwise_runs, float *weight, float *input_weight);
 
 /* Batched counts (no single counterpart in the reference, whose driver counts
  * one catalogue at a time): DD of each mock and/or DR of each mock against a
@@ -367,6 +395,25 @@ int tpcf_write_xi_ascii(const char *filename, const tpcf_binning *bin, const dou
  * and outputs are refused with TPCF_E_UNSUPPORTED (this build has no HDF5
  * library).  log: 0 quiet, 1 one line per step on stderr. */
 int tpcf_run_param_file(const char *path, int device, int precision, int log);
+
+/* The inverse-p program after its catalogues are read (src/main.cpp:51-60):
+ * the angular stage of calc_angular_upweight
+ * (src/correlators_invpweight.cpp:985-1033) — angular DD (every point,
+ * input-weight products), DD with inverse-p weights, DR, DR with inverse-p
+ * weights on Hist(0, 1 - cos(theta_max), theta_n_bins, theta_log_base) —
+ * then, for each plot_* flag, auto_correlate_*_invpweights
+ * (:210-237, :445-474, :682-711): DD with inverse-p weights and the
+ * DD / DD-inverse-p up-weight, DR with the DR / DR-inverse-p up-weight, plain
+ * RR, normalised and written as ASCII where the parameters name the files.
+ * The angular histograms stay in memory instead of going through HDF5 files,
+ * so the calculate_angular_* flags and file names are not used: all four are
+ * always computed.  data and randoms carry bitmasks (and input weights, e.g.
+ * from tpcf_iip_weights); dither = 1 is the _USE_DITHER_WEIGHTS build (both
+ * need dither masks).  angular_out: NULL or 4 * (1 + n_jk) * theta_n_bins
+ * doubles receiving DD, DD-inverse-p, DR, DR-inverse-p, each as its full
+ * histogram then its n_jk region rows, in the reference's convention. */
+int tpcf_run_invp(tpcf_ctx *ctx, const tpcf_params *params, const tpcf_catalog *data, const tpcf_catalog *randoms,
+                  int precision, int dither, double *angular_out, int log);
 
 #ifdef __cplusplus
 }

@@ -11,6 +11,10 @@
 #                           -D_N_MASK_INTS=32, linked against the in-memory
 #                           HDF5 stand-in in oracle/hdf5_stub/ (libhdf5 is not
 #                           installed here)
+#   libtwopcf_ref_midpoint.so        plain build without -D_ANGULAR_PI_DEFN (pi
+#                                    along x1 + x2, src/correlators.cpp:172-182)
+#   libtwopcf_ref_invp_dither.so     inverse-p build with -D_USE_DITHER_WEIGHTS
+#   libtwopcf_ref_invp4.so           inverse-p build with -D_N_MASK_INTS=4
 #   twopcf_ref              the reference's own command-line program (plain
 #                           build, src/main.cpp included), for end-to-end
 #                           comparisons of parameter file -> ASCII outputs
@@ -40,17 +44,31 @@ SRCS="$REF/src/boxes.cpp $REF/src/correlators.cpp $REF/src/correlators_invpweigh
       $REF/src/io.cpp $REF/src/healpix/error_handling.cpp $REF/src/healpix/healpix_base.cpp \
       $REF/src/healpix/pointing.cpp $REF/src/healpix/geom_utils.cpp \
       $REF/src/healpix/healpix_tables.cpp $REF/src/healpix/string_utils.cpp"
-FLAGS="-O3 -std=c++11 -fopenmp -ffp-contract=off -fPIC -shared -w -D_ANGULAR_PI_DEFN"
+BASE="-O3 -std=c++11 -fopenmp -ffp-contract=off -fPIC -shared -w"
+INVP="-D_HAVE_HDF5 -D_USE_INV_WEIGHTS -I$HERE/hdf5_stub"
+INC="-I$REF/src -I$REF/src/healpix"
 
-$CXX $FLAGS -D_N_MASK_INTS=1 -I"$REF/src" -I"$REF/src/healpix" \
-    "$HERE/ref_harness.cpp" $SRCS -o "$OUT/libtwopcf_ref_plain.so.tmp"
-mv "$OUT/libtwopcf_ref_plain.so.tmp" "$OUT/libtwopcf_ref_plain.so"
+# build <output name> <flags...>: one shared library of the harness and the
+# reference sources; the builds run in parallel and each is checked.
+build() {
+    name=$1
+    shift
+    stub=""
+    case "$*" in *_USE_INV_WEIGHTS*) stub="$HERE/hdf5_stub/hdf5_stub.cpp" ;; esac
+    $CXX $BASE "$@" $INC "$HERE/ref_harness.cpp" $stub $SRCS -o "$OUT/$name.tmp" && mv "$OUT/$name.tmp" "$OUT/$name"
+}
 
-$CXX $FLAGS -D_HAVE_HDF5 -D_USE_INV_WEIGHTS -D_N_MASK_INTS=32 -I"$HERE/hdf5_stub" -I"$REF/src" \
-    -I"$REF/src/healpix" "$HERE/ref_harness.cpp" "$HERE/hdf5_stub/hdf5_stub.cpp" $SRCS \
-    -o "$OUT/libtwopcf_ref_invp.so.tmp"
-mv "$OUT/libtwopcf_ref_invp.so.tmp" "$OUT/libtwopcf_ref_invp.so"
-$CXX -O3 -std=c++11 -fopenmp -ffp-contract=off -w -D_ANGULAR_PI_DEFN -D_N_MASK_INTS=1 -I"$REF/src" \
-    -I"$REF/src/healpix" "$REF/src/main.cpp" $SRCS -o "$OUT/twopcf_ref.tmp"
-mv "$OUT/twopcf_ref.tmp" "$OUT/twopcf_ref"
-echo "built $OUT/libtwopcf_ref_plain.so $OUT/libtwopcf_ref_invp.so $OUT/twopcf_ref"
+build libtwopcf_ref_plain.so -D_ANGULAR_PI_DEFN -D_N_MASK_INTS=1 & p1=$!
+build libtwopcf_ref_invp.so -D_ANGULAR_PI_DEFN $INVP -D_N_MASK_INTS=32 & p2=$!
+build libtwopcf_ref_midpoint.so -D_N_MASK_INTS=1 & p3=$!
+build libtwopcf_ref_invp_dither.so -D_ANGULAR_PI_DEFN $INVP -D_USE_DITHER_WEIGHTS -D_N_MASK_INTS=32 & p4=$!
+build libtwopcf_ref_invp4.so -D_ANGULAR_PI_DEFN $INVP -D_N_MASK_INTS=4 & p5=$!
+$CXX -O3 -std=c++11 -fopenmp -ffp-contract=off -w -D_ANGULAR_PI_DEFN -D_N_MASK_INTS=1 $INC \
+    "$REF/src/main.cpp" $SRCS -o "$OUT/twopcf_ref.tmp" && mv "$OUT/twopcf_ref.tmp" "$OUT/twopcf_ref" & p6=$!
+rc=0
+for p in $p1 $p2 $p3 $p4 $p5 $p6; do wait $p || rc=1; done
+if [ $rc -ne 0 ]; then
+    echo "build_ref.sh: a reference build failed" >&2
+    exit 1
+fi
+echo "built $(ls "$OUT" | tr '\n' ' ')"

@@ -31,7 +31,7 @@ class OrcAxis(C.Structure):
 class OrcCat(C.Structure):
     _fields_ = [("n", C.c_int), ("xyz", C.c_void_p), ("unit", C.c_void_p), ("dcom", C.c_void_p),
                 ("w", C.c_void_p), ("iw", C.c_void_p), ("jk", C.c_void_p), ("masks", C.c_void_p),
-                ("n_mask", C.c_int)]
+                ("n_mask", C.c_int), ("dmasks", C.c_void_p)]
 
 
 class OrcUpweight(C.Structure):
@@ -70,6 +70,7 @@ def lib():
         L.orc_ls.restype = C.c_double
         L.orc_partition.argtypes = [C.c_void_p, C.c_int, C.c_void_p]
         L.orc_partition.restype = C.c_int
+        L.orc_set_variant.argtypes = [C.c_int, C.c_int]
         _LIB = L
     return _LIB
 
@@ -85,7 +86,7 @@ def _p(a):
 class Cat:
     """Holds a catalogue's arrays alive and exposes the OrcCat view."""
 
-    def __init__(self, xyz, unit=None, dcom=None, w=None, iw=None, jk=None, masks=None):
+    def __init__(self, xyz, unit=None, dcom=None, w=None, iw=None, jk=None, masks=None, dmasks=None):
         self.xyz = _arr(xyz, np.float64)
         n = self.xyz.shape[0]
         if unit is None:
@@ -97,9 +98,27 @@ class Cat:
         self.iw = _arr(iw, np.float32)
         self.jk = _arr(jk, np.int32)
         self.masks = _arr(masks, np.int64)
+        self.dmasks = _arr(dmasks, np.int64)
         n_mask = 0 if self.masks is None else self.masks.reshape(n, -1).shape[1]
         self.c = OrcCat(n, _p(self.xyz), _p(self.unit), _p(self.dcom), _p(self.w), _p(self.iw), _p(self.jk),
-                        _p(self.masks), n_mask)
+                        _p(self.masks), n_mask, _p(self.dmasks))
+
+
+class variant:
+    """Context manager selecting a build variant of the reference for the
+    oracle's counts: los_midpoint (pi without _ANGULAR_PI_DEFN) and/or
+    dither (_USE_DITHER_WEIGHTS)."""
+
+    def __init__(self, los_midpoint=False, dither=False):
+        self.args = (int(los_midpoint), int(dither))
+
+    def __enter__(self):
+        lib().orc_set_variant(*self.args)
+        return self
+
+    def __exit__(self, *exc):
+        lib().orc_set_variant(0, 0)
+        return False
 
 
 def axis(vmin, vmax, n_bins, base) -> OrcAxis:

@@ -85,6 +85,10 @@ std::string write_temp_params(const char *text) {
     return path;
 }
 
+// Dither masks (the _USE_DITHER_WEIGHTS build) of the first and second
+// catalogue of the next calls, object-major; set by ref_invp_set_dither.
+const long long *g_dither[2] = {nullptr, nullptr};
+
 }  // namespace
 
 extern "C" {
@@ -367,6 +371,15 @@ int ref_invp_read(const char *param_text, const double *c1, const double *c2, co
         ss << p.bitwise_weight_dataset_name << m;
         put(ss.str(), H5T_NATIVE_LONG, tmp.data());
     }
+#ifdef _USE_DITHER_WEIGHTS
+    // dither masks from ref_invp_set_dither (first catalogue), object-major
+    for (int m = 0; m < _N_MASK_INTS; ++m) {
+        for (int i = 0; i < n; ++i) tmp[i] = g_dither[0] ? (long)g_dither[0][(size_t)i * _N_MASK_INTS + m] : -1L;
+        std::stringstream ss;
+        ss << p.dither_weight_dataset_name << m;
+        put(ss.str(), H5T_NATIVE_LONG, tmp.data());
+    }
+#endif
     H5Fclose(f);
     Cosmology *cosmo = NULL;
     if (p.coord_system == "equatorial") cosmo = new Cosmology(p.omega_m, p.h, p.z_min, p.z_max, 0.0001, 100);
@@ -387,14 +400,33 @@ int ref_invp_read(const char *param_text, const double *c1, const double *c2, co
 
 namespace {
 void fill_cat_invp(GalaxyCatalogue *cat, const double *xyz, const double *unit, const double *dcom,
-                   const float *w, const float *iw, const int *jk, const long long *masks) {
+                   const float *w, const float *iw, const int *jk, const long long *masks, int which) {
     fill_cat(cat, xyz, unit, dcom, w, jk);
     for (int i = 0; i < cat->n_gals; ++i) {
         cat->gals[i].input_weight = iw ? iw[i] : cat->gals[i].weight;
         for (int m = 0; m < _N_MASK_INTS; ++m) cat->gals[i].bitmask[m] = masks ? masks[(size_t)i * _N_MASK_INTS + m] : -1LL;
+#ifdef _USE_DITHER_WEIGHTS
+        const long long *d = g_dither[which];
+        for (int m = 0; m < _N_MASK_INTS; ++m) cat->gals[i].dither_mask[m] = d ? d[(size_t)i * _N_MASK_INTS + m] : -1LL;
+#else
+        (void)which;
+#endif
     }
 }
 }  // namespace
+
+int ref_has_dither(void) {
+#ifdef _USE_DITHER_WEIGHTS
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+void ref_invp_set_dither(const long long *d1, const long long *d2) {
+    g_dither[0] = d1;
+    g_dither[1] = d2;
+}
 
 // Angular stage (src/correlators_invpweight.cpp:713-982 via the stages of
 // calc_angular_upweight, :985-1033).  kind: 0 = angular DD
@@ -415,7 +447,7 @@ int ref_invp_angular(const char *param_text, int kind, const double *xyz1, const
     Params p(path);
     std::remove(path.c_str());
     GalaxyCatalogue c1(n1, p.n_jk_regions);
-    fill_cat_invp(&c1, xyz1, unit1, dcom1, w1, iw1, jk1, m1);
+    fill_cat_invp(&c1, xyz1, unit1, dcom1, w1, iw1, jk1, m1, 0);
     Hist tmp(0.0, 1.0 - cos(p.theta_max), p.theta_n_bins, p.theta_log_base);
     JKHists h(p.n_jk_regions, tmp);
     bool req = (kind == 1 || kind == 3);
@@ -424,7 +456,7 @@ int ref_invp_angular(const char *param_text, int kind, const double *xyz1, const
     else if (kind == 1) auto_pair_count_angular_invpweights(&px1, &h, p);
     else {
         GalaxyCatalogue c2(n2, p.n_jk_regions);
-        fill_cat_invp(&c2, xyz2, unit2, dcom2, w2, iw2, jk2, m2);
+        fill_cat_invp(&c2, xyz2, unit2, dcom2, w2, iw2, jk2, m2, 1);
         GalaxyPixels px2(c2.gals, n2, p.healpix_order, p.theta_max, req);
         if (kind == 2) cross_pair_count_angular(&px1, &px2, &h);
         else cross_pair_count_angular_invpweights(&px1, &px2, &h);
@@ -487,10 +519,10 @@ int ref_invp_count_3d(const char *param_text, int mode, int is_auto, const doubl
     std::remove(path.c_str());
     int n_jk = p.n_jk_regions;
     GalaxyCatalogue c1(n1, n_jk);
-    fill_cat_invp(&c1, xyz1, unit1, dcom1, w1, iw1, jk1, m1);
+    fill_cat_invp(&c1, xyz1, unit1, dcom1, w1, iw1, jk1, m1, 0);
     GalaxyCatalogue c2(n2 > 0 ? n2 : 1, n_jk);
     c2.n_gals = n2;
-    if (n2 > 0) fill_cat_invp(&c2, xyz2, unit2, dcom2, w2, iw2, jk2, m2);
+    if (n2 > 0) fill_cat_invp(&c2, xyz2, unit2, dcom2, w2, iw2, jk2, m2, 1);
     double rmax = mode == 0 ? p.monopole_max
                 : mode == 1 ? std::sqrt(p.sigma_max * p.sigma_max + p.pi_max * p.pi_max) : p.s_max;
     GalaxyBoxes b1(c1.gals, n1, c2.gals, n2, rmax);
@@ -528,6 +560,32 @@ int ref_invp_count_3d(const char *param_text, int mode, int is_auto, const doubl
         std::memcpy(sub_out, h.sub_hist, sizeof(double) * nb * n_jk);
     }
     c2.n_gals = n2 > 0 ? n2 : 1;
+    return 0;
+}
+
+// The inverse-p program after its catalogues are read (src/main.cpp:51-60):
+// calc_angular_upweight (src/correlators_invpweight.cpp:985-1033), whose
+// angular histograms go through the HDF5 stand-in under the params' file
+// names, then auto_correlate_{monopole,sigma_pi,s_mu}_invpweights as the
+// plot_* flags select, each writing its outputs (type "ascii") where the
+// params name them.  Catalogue 1 is the data, catalogue 2 the randoms.
+int ref_invp_correlate(const char *param_text, const double *xyz1, const double *unit1, const double *dcom1,
+                       const float *w1, const float *iw1, const int *jk1, const long long *m1, int n1,
+                       const double *xyz2, const double *unit2, const double *dcom2, const float *w2,
+                       const float *iw2, const int *jk2, const long long *m2, int n2, int n_threads) {
+    std::string path = write_temp_params(param_text);
+    if (path.empty()) return -1;
+    Quiet q;
+    set_threads(n_threads);
+    Params p(path);
+    std::remove(path.c_str());
+    GalaxyCatalogue data(n1, p.n_jk_regions), randoms(n2, p.n_jk_regions);
+    fill_cat_invp(&data, xyz1, unit1, dcom1, w1, iw1, jk1, m1, 0);
+    fill_cat_invp(&randoms, xyz2, unit2, dcom2, w2, iw2, jk2, m2, 1);
+    calc_angular_upweight(&data, &randoms, p);
+    if (p.plot_monopole) auto_correlate_monopole_invpweights(&data, &randoms, p);
+    if (p.plot_sigma_pi) auto_correlate_sigma_pi_invpweights(&data, &randoms, p);
+    if (p.plot_s_mu) auto_correlate_s_mu_invpweights(&data, &randoms, p);
     return 0;
 }
 

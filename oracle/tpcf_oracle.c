@@ -49,7 +49,20 @@ typedef struct {
     const int *jk;          /* n or NULL (0) */
     const long long *masks; /* n x n_mask or NULL (all bits set) */
     int n_mask;
+    const long long *dmasks; /* n x n_mask dither masks (Galaxy::dither_mask) or NULL */
 } orc_cat;
+
+/* Build variants of the reference, selected at run time here:
+ *   los_midpoint — pi without _ANGULAR_PI_DEFN (src/correlators.cpp:172-182);
+ *   dither       — _USE_DITHER_WEIGHTS: the popcount of the two dither masks
+ *                  replaces n_bitwise_runs in the inverse-p DD weights
+ *                  (src/correlators_invpweight.cpp:62-71, :749-757). */
+static int g_los_midpoint = 0, g_dither = 0;
+
+void orc_set_variant(int los_midpoint, int dither) {
+    g_los_midpoint = los_midpoint;
+    g_dither = dither;
+}
 
 /* Angular up-weight table for JKHists::interp: the ratio histogram's full
  * bins, its axis, and the bin centres the reference computes with exp(). */
@@ -247,7 +260,12 @@ static inline int pair_bin_3d(const orc_setup *s, const orc_cat *a, int i, const
         /* src/correlators_invpweight.cpp:51-77 */
         double omct = one_minus_cos(n1, n2);
         float pw = popc_weight(a->masks + (size_t)i * a->n_mask, b->masks + (size_t)j * b->n_mask, a->n_mask);
-        pw = (float)(orc_interp(s->up, omct) * s->n_runs / pw);
+        if (g_dither) {
+            float dw = popc_weight(a->dmasks + (size_t)i * a->n_mask, b->dmasks + (size_t)j * b->n_mask, a->n_mask);
+            pw = (float)(orc_interp(s->up, omct) * dw / pw);
+        } else {
+            pw = (float)(orc_interp(s->up, omct) * s->n_runs / pw);
+        }
         float iw1 = a->iw ? a->iw[i] : w1, iw2 = b->iw ? b->iw[j] : w2;
         weight = iw1 * iw2 * pw;
     } else {
@@ -261,11 +279,25 @@ static inline int pair_bin_3d(const orc_setup *s, const orc_cat *a, int i, const
         int bin = orc_to_int(orc_axis_bin_num(&s->ax1, sqrtf(s2)));
         return (bin < s->ax1.n_bins && bin >= 0) ? bin : -1;
     }
-    /* pi, _ANGULAR_PI_DEFN (src/correlators.cpp:166-170) */
-    float pi = (float)((double)d[0] * (n1[0] + n2[0]));
-    pi = (float)((double)pi + (double)d[1] * (n1[1] + n2[1]));
-    pi = (float)((double)pi + (double)d[2] * (n1[2] + n2[2]));
-    pi = (float)((double)pi * 0.5);
+    float pi;
+    if (g_los_midpoint) {
+        /* src/correlators.cpp:172-182 */
+        float sum[3], inv = 0.0f;
+        for (int m = 0; m < 3; ++m) {
+            sum[m] = (float)(x1[m] + x2[m]);
+            inv += sum[m] * sum[m];
+        }
+        inv = (float)(1.0 / (double)sqrtf(inv));
+        pi = d[0] * sum[0] * inv;
+        pi += d[1] * sum[1] * inv;
+        pi += d[2] * sum[2] * inv;
+    } else {
+        /* pi, _ANGULAR_PI_DEFN (src/correlators.cpp:166-170) */
+        pi = (float)((double)d[0] * (n1[0] + n2[0]));
+        pi = (float)((double)pi + (double)d[1] * (n1[1] + n2[1]));
+        pi = (float)((double)pi + (double)d[2] * (n1[2] + n2[2]));
+        pi = (float)((double)pi * 0.5);
+    }
     float v1, v2;
     if (s->mode == ORC_SIGMA_PI) {
         v1 = sqrtf(s2 - pi * pi);
@@ -515,7 +547,10 @@ static void eval_angular(const orc_setup *s, const orc_cat *a, int i, const orc_
         break;
     case 1: { /* auto_pair_count_angular_invpweights (:743-764) */
         float pw = popc_weight(a->masks + (size_t)i * a->n_mask, b->masks + (size_t)j * b->n_mask, a->n_mask);
-        pw = (float)s->n_runs / pw;
+        if (g_dither)
+            pw = popc_weight(a->dmasks + (size_t)i * a->n_mask, b->dmasks + (size_t)j * b->n_mask, a->n_mask) / pw;
+        else
+            pw = (float)s->n_runs / pw;
         weight = iw1 * iw2 * pw;
         break;
     }

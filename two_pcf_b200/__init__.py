@@ -27,14 +27,16 @@ import ctypes as C
 import numpy as np
 
 from . import _capi
-from ._capi import (ANGULAR, BATCH_AUTOTUNE, BATCH_DD, BATCH_DR, FP32_GUARD, FP64, MONOPOLE, S_MU, SIGMA_PI,
-                    WEIGHTS_INVP_DD, WEIGHTS_INVP_DR, WEIGHTS_PLAIN, AxisSpec, Stats, WeightSpec)
+from ._capi import (ANGULAR, BATCH_AUTOTUNE, BATCH_DD, BATCH_DR, FP32_GUARD, FP64, LOS_ANGULAR, LOS_MIDPOINT,
+                    MONOPOLE, S_MU, SIGMA_PI, WEIGHTS_INVP_DD, WEIGHTS_INVP_DD_DITHER, WEIGHTS_INVP_DR, WEIGHTS_PLAIN,
+                    AxisSpec, Stats, WeightSpec)
 
 __all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "auto_pair_count", "cross_pair_count",
            "count_weighted", "pair_count_weighted", "upweight_eval", "count_backward", "normalise_auto",
            "normalise_cross",
            "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
-           "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR", "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE"]
+           "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR", "WEIGHTS_INVP_DD_DITHER", "LOS_ANGULAR", "LOS_MIDPOINT", "iip_weights",
+           "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE"]
 
 
 class TpcfError(RuntimeError):
@@ -123,6 +125,11 @@ class Catalog:
         w = np.ascontiguousarray(weight, np.float32).reshape(self.n)
         _check(_capi.lib().tpcf_catalog_set_weights(self._h, _ptr(w)), self.ctx)
 
+    def set_dither_masks(self, dither_mask):
+        """Galaxy::dither_mask (the _USE_DITHER_WEIGHTS build): n x n_mask_ints int64."""
+        m = np.ascontiguousarray(dither_mask, np.int64).reshape(self.n, -1)
+        _check(_capi.lib().tpcf_catalog_set_dither_masks(self._h, _ptr(m)), self.ctx)
+
     def close(self):
         if getattr(self, "_h", None):
             _capi.lib().tpcf_catalog_destroy(self._h)
@@ -158,6 +165,11 @@ class Binning:
         self.n_jk = int(n_jk_regions)
         self.nb = int(_capi.lib().tpcf_binning_total_bins(h))
         self.shape = (a1.n_bins,) if mode in (MONOPOLE, ANGULAR) else (a1.n_bins, a2.n_bins)
+
+    def set_line_of_sight(self, line_of_sight: int):
+        """LOS_ANGULAR (the reference's default _ANGULAR_PI_DEFN build) or
+        LOS_MIDPOINT (its build without it, src/correlators.cpp:172-182)."""
+        _check(_capi.lib().tpcf_binning_set_line_of_sight(self._h, int(line_of_sight)), self.ctx)
 
     def thresholds(self, axis: int = 1) -> np.ndarray:
         n = _capi.lib().tpcf_binning_thresholds(self._h, axis, None, 0)
@@ -275,6 +287,19 @@ def pair_count_weighted(ctx: Context, a: Catalog, b: Catalog | None, binning: Bi
                                               int(precision), _ptr(full), _ptr(sub), C.byref(st))
     _check(rc, ctx)
     return full, sub, st.as_dict()
+
+
+def iip_weights(bitmask, weight, n_bitwise_runs: int, dither_mask=None):
+    """The inverse-p build's reading of bitwise weights (src/io.cpp:519-586):
+    returns (weight, input_weight) as float32."""
+    m = np.ascontiguousarray(bitmask, np.int64)
+    n = m.shape[0]
+    m = m.reshape(n, -1)
+    d = None if dither_mask is None else np.ascontiguousarray(dither_mask, np.int64).reshape(n, m.shape[1])
+    w = np.array(weight, dtype=np.float32, copy=True).reshape(n)
+    iw = np.empty(n, np.float32)
+    _check(_capi.lib().tpcf_iip_weights(n, m.shape[1], _ptr(m), _ptr(d), int(n_bitwise_runs), _ptr(w), _ptr(iw)))
+    return w, iw
 
 
 def upweight_eval(weights: Weights, values) -> np.ndarray:

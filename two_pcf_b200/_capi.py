@@ -36,7 +36,8 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
-WEIGHTS_PLAIN, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR = 0, 1, 2
+WEIGHTS_PLAIN, WEIGHTS_INVP_DD, WEIGHTS_INVP_DR, WEIGHTS_INVP_DD_DITHER = 0, 1, 2, 3
+LOS_ANGULAR, LOS_MIDPOINT = 0, 1
 BATCH_DD, BATCH_DR, BATCH_AUTOTUNE = 1, 2, -1
 
 
@@ -75,6 +76,9 @@ _PROTOTYPES = {
     "tpcf_upweight_eval": (C.c_int, [C.POINTER(WeightSpec), _vp, C.c_int64, _vp]),
     "tpcf_count_backward": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_catalog_set_weights": (C.c_int, [_vp, _vp]),
+    "tpcf_catalog_set_dither_masks": (C.c_int, [_vp, _vp]),
+    "tpcf_binning_set_line_of_sight": (C.c_int, [_vp, C.c_int]),
+    "tpcf_iip_weights": (C.c_int, [C.c_int64, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp]),
     "tpcf_batch_create": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp, C.c_int, C.c_int32, C.c_int32, C.POINTER(_vp)]),
     "tpcf_batch_run": (C.c_int, [_vp, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_batch_n_outputs": (C.c_int, [_vp]),
@@ -109,6 +113,7 @@ _PROTOTYPES = {
     "tpcf_sub_filename": (C.c_int, [C.c_char_p, C.c_int64, C.c_char_p, C.c_int32]),
     "tpcf_write_xi_ascii": (C.c_int, [C.c_char_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "tpcf_run_param_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    "tpcf_run_invp": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, C.c_int]),
 }
 
 CARTESIAN, EQUATORIAL = 0, 1

@@ -378,14 +378,20 @@ namespace {
 int prepare_weights(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                     const tpcf_weight_spec *spec, tpcf::CountRequest &req, tpcf::UpTable &up) {
     req.weighting = spec ? spec->weighting : TPCF_WEIGHTS_PLAIN;
-    if (req.weighting < TPCF_WEIGHTS_PLAIN || req.weighting > TPCF_WEIGHTS_INVP_DR)
+    if (req.weighting < TPCF_WEIGHTS_PLAIN || req.weighting > TPCF_WEIGHTS_INVP_DD_DITHER)
         return fail(ctx, TPCF_E_INVALID_ARG, "bad weighting");
     if (req.weighting == TPCF_WEIGHTS_PLAIN) return TPCF_OK;
+    if (req.weighting == TPCF_WEIGHTS_INVP_DD_DITHER) {
+        req.weighting = TPCF_WEIGHTS_INVP_DD;
+        req.dither = true;
+    }
     req.n_runs = spec->n_bitwise_runs;
     if (req.weighting == TPCF_WEIGHTS_INVP_DD) {
         const tpcf::Catalog &ca = a->c, &cb = b ? b->c : a->c;
         if (ca.n_mask < 1 || ca.n_mask != cb.n_mask)
             return fail(ctx, TPCF_E_INVALID_ARG, "inverse-p DD weights need bitmasks of one width on both catalogues");
+        if (req.dither && (!ca.dmasks.p || !cb.dmasks.p))
+            return fail(ctx, TPCF_E_INVALID_ARG, "dither weights need dither masks on both catalogues");
     }
     if (bin->b.mode != TPCF_ANGULAR) {
         const tpcf_axis_spec &t = spec->theta_axis;
@@ -416,7 +422,7 @@ int count_impl(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, cons
     req.a = &a->c;
     req.b = b ? &b->c : nullptr;
     req.bin = &bin->b;
-    req.exact_fp64 = precision == TPCF_FP64;
+    req.exact_fp64 = precision == TPCF_FP64 || bin->b.los_midpoint;
     const int nb = bin->b.nb;
     // Points a count uses: every point for plain angular counts, the d_comov
     // partition otherwise.
@@ -506,7 +512,7 @@ int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog
     req.a = &a->c;
     req.b = b ? &b->c : nullptr;
     req.bin = &bin->b;
-    req.exact_fp64 = precision == TPCF_FP64;
+    req.exact_fp64 = precision == TPCF_FP64 || bin->b.los_midpoint;
     req.adj_G = dL_dfull;
     req.grad_a = dL_dw_a;
     req.grad_b = dL_dw_b;
@@ -564,6 +570,54 @@ int tpcf_catalog_set_weights(tpcf_catalog *cat, const float *weight) {
     return TPCF_OK;
 }
 
+int tpcf_catalog_set_dither_masks(tpcf_catalog *cat, const int64_t *dither_mask) {
+    if (!cat || !dither_mask) return TPCF_E_INVALID_ARG;
+    tpcf::Catalog &c = cat->c;
+    tpcf::Ctx *ctx = c.ctx;
+    if (c.n_mask < 1) {
+        ctx->last_error = "dither masks need the catalogue's bitmasks (their width sets the dither masks' width)";
+        return TPCF_E_INVALID_ARG;
+    }
+    const size_t words = (size_t)c.n_all * c.n_mask;
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e == cudaSuccess) e = c.dmasks.alloc(words);
+    if (e == cudaSuccess && words > 0)
+        e = cudaMemcpyAsync(c.dmasks.p, dither_mask, sizeof(long long) * words, cudaMemcpyHostToDevice, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        c.dmasks.release();
+        ctx->last_error = std::string("dither masks: ") + cudaGetErrorString(e);
+        return e == cudaErrorMemoryAllocation ? TPCF_E_OOM : TPCF_E_CUDA;
+    }
+    return TPCF_OK;
+}
+
+int tpcf_binning_set_line_of_sight(tpcf_binning *bin, int line_of_sight) {
+    if (!bin || (line_of_sight != TPCF_LOS_ANGULAR && line_of_sight != TPCF_LOS_MIDPOINT)) return TPCF_E_INVALID_ARG;
+    bin->b.los_midpoint = line_of_sight == TPCF_LOS_MIDPOINT;
+    return TPCF_OK;
+}
+
+int tpcf_iip_weights(int64_t n, int32_t n_mask_ints, const int64_t *bitmask, const int64_t *dither_mask,
+                     int32_t n_bitwise_runs, float *weight, float *input_weight) {
+    if (n < 0 || n_mask_ints < 1 || (n > 0 && (!bitmask || !weight || !input_weight))) return TPCF_E_INVALID_ARG;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) {
+        int total = 0, dtotal = 0;
+        for (int k = 0; k < n_mask_ints; ++k) {
+            total += __builtin_popcountll((unsigned long long)bitmask[(size_t)i * n_mask_ints + k]);
+            if (dither_mask) dtotal += __builtin_popcountll((unsigned long long)dither_mask[(size_t)i * n_mask_ints + k]);
+        }
+        input_weight[i] = weight[i];
+        if (total == 0) total = 1;
+        if (total != n_bitwise_runs) {
+            const double ratio = dither_mask ? (double)dtotal / (double)total : (double)n_bitwise_runs / (double)total;
+            weight[i] = (float)((double)weight[i] * ratio);
+        }
+    }
+    return TPCF_OK;
+}
+
 int tpcf_batch_create(tpcf_ctx *ctx, const tpcf_catalog *const *mocks, int32_t n_mocks, const tpcf_catalog *randoms,
                       const tpcf_binning *bin, int precision, int32_t what, int32_t refinement, tpcf_batch **out) {
     if (!ctx || !mocks || n_mocks < 1 || !bin || !out) return TPCF_E_INVALID_ARG;
@@ -588,7 +642,7 @@ int tpcf_batch_create(tpcf_ctx *ctx, const tpcf_catalog *const *mocks, int32_t n
     if (!B) return TPCF_E_OOM;
     B->ctx = ctx;
     tpcf::Error err{0, ""};
-    if (tpcf::batch_create(&ctx->c, jobs, &bin->b, precision == TPCF_FP64, refinement, &B->b, &err))
+    if (tpcf::batch_create(&ctx->c, jobs, &bin->b, precision == TPCF_FP64 || bin->b.los_midpoint, refinement, &B->b, &err))
         return fail(ctx, err.status, err.msg);
     *out = B.release();
     return TPCF_OK;

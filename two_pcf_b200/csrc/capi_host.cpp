@@ -17,16 +17,6 @@
 #include "capi_types.h"
 #include "ingest.h"
 
-struct tpcf_params {
-    tpcf::Params p;
-};
-struct tpcf_cosmology {
-    tpcf::CosmologyTable t;
-};
-struct tpcf_host_catalog {
-    tpcf::HostCatalogue c;
-};
-
 namespace {
 
 thread_local std::string g_host_error;

@@ -3,6 +3,7 @@
 #pragma once
 #include "../../include/two_pcf_b200.h"
 #include "engine.h"
+#include "ingest.h"
 
 struct tpcf_ctx {
     tpcf::Ctx c;
@@ -19,4 +20,13 @@ struct tpcf_batch {
     ~tpcf_batch() {
         if (b) tpcf::batch_destroy(b);
     }
+};
+struct tpcf_params {
+    tpcf::Params p;
+};
+struct tpcf_cosmology {
+    tpcf::CosmologyTable t;
+};
+struct tpcf_host_catalog {
+    tpcf::HostCatalogue c;
 };

@@ -1,6 +1,7 @@
 // The reference's program on a parameter file (src/main.cpp:11-84, plain
 // build), with the pair counts on the device: tpcf_run_param_file.
 #include <chrono>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <memory>
@@ -79,12 +80,15 @@ bool upload(tpcf_ctx *ctx, const tpcf::HostCatalogue &h, int n_jk, CatPtr &out, 
     return true;
 }
 
-// One auto_correlate_* (src/correlators.cpp:127-153, :280-307, :432-459):
-// DD, DR, RR in the reference's convention (jackknife-inverted, auto counts
-// doubled), each normalised, then the ASCII outputs.
+// One auto_correlate_* (src/correlators.cpp:127-153, :280-307, :432-459), or
+// with weight specs auto_correlate_*_invpweights
+// (src/correlators_invpweight.cpp:210-237, :445-474, :682-711): DD, DR, RR in
+// the reference's convention (jackknife-inverted, auto counts doubled), each
+// normalised, then the ASCII outputs.  RR is always a plain count.
 bool correlate(tpcf_ctx *ctx, const char *what, int mode, const tpcf_axis_spec &a1, const tpcf_axis_spec *a2,
-               int n_jk, tpcf_catalog *data, tpcf_catalog *rand, int precision, const std::string &filename,
-               const std::string &output_type, const Log &log, Err &e) {
+               int n_jk, const tpcf_catalog *data, const tpcf_catalog *rand, int precision,
+               const std::string &filename, const std::string &output_type, const tpcf_weight_spec *dd_spec,
+               const tpcf_weight_spec *dr_spec, const Log &log, Err &e) {
     if (output_type == "hdf5")
         return e.set(TPCF_E_UNSUPPORTED, std::string(what) + ": HDF5 output needs the HDF5 library, which this build lacks");
     if (output_type != "ascii")
@@ -101,11 +105,12 @@ bool correlate(tpcf_ctx *ctx, const char *what, int mode, const tpcf_axis_spec &
     }
     tpcf_stats st[3];
     log("%s: DD", what);
-    rc = tpcf_auto_pair_count(ctx, data, b, precision, full[0].data(), sub[0].data(), &st[0]);
+    rc = tpcf_pair_count_weighted(ctx, data, nullptr, b, dd_spec, precision, full[0].data(), sub[0].data(), &st[0]);
     if (!rc) rc = tpcf_normalise_auto(data, nb, full[0].data(), sub[0].data());
     if (!rc) {
         log("%s: DR", what);
-        rc = tpcf_cross_pair_count(ctx, data, rand, b, precision, full[1].data(), sub[1].data(), &st[1]);
+        rc = tpcf_pair_count_weighted(ctx, data, rand, b, dr_spec, precision, full[1].data(), sub[1].data(),
+                                      &st[1]);
     }
     if (!rc) rc = tpcf_normalise_cross(data, rand, nb, full[1].data(), sub[1].data());
     if (!rc) {
@@ -121,6 +126,78 @@ bool correlate(tpcf_ctx *ctx, const char *what, int mode, const tpcf_axis_spec &
     if (rc) return e.set(rc, std::string(what) + ": " + tpcf_host_last_error());
     log("%s: wrote %s and %d region files", what, filename.c_str(), n_jk);
     return true;
+}
+
+// The plot_monopole / plot_sigma_pi / plot_s_mu sequence of main
+// (src/main.cpp:53-70) with the given DD and DR weightings.
+bool correlate_modes(tpcf_ctx *c, const tpcf::Params &p, const tpcf_catalog *data, const tpcf_catalog *rand,
+                     int precision, const tpcf_weight_spec *dd, const tpcf_weight_spec *dr, const Log &log, Err &e) {
+    if (p.plot_monopole) {
+        tpcf_axis_spec a{p.monopole_min, p.monopole_max, p.monopole_log_base, p.monopole_n_bins};
+        if (!correlate(c, "monopole", TPCF_MONOPOLE, a, nullptr, p.n_jk_regions, data, rand, precision,
+                       p.monopole_filename, p.monopole_output_type, dd, dr, log, e))
+            return false;
+    }
+    if (p.plot_sigma_pi) {
+        tpcf_axis_spec a{p.sigma_min, p.sigma_max, p.sigma_log_base, p.sigma_n_bins};
+        tpcf_axis_spec b{p.pi_min, p.pi_max, p.pi_log_base, p.pi_n_bins};
+        if (!correlate(c, "sigma-pi", TPCF_SIGMA_PI, a, &b, p.n_jk_regions, data, rand, precision,
+                       p.sigma_pi_filename, p.sigma_pi_output_type, dd, dr, log, e))
+            return false;
+    }
+    if (p.plot_s_mu) {
+        tpcf_axis_spec a{p.s_min, p.s_max, p.s_log_base, p.s_n_bins};
+        tpcf_axis_spec b{0.0, 1.0, 0.0, p.mu_n_bins};
+        if (!correlate(c, "s-mu", TPCF_S_MU, a, &b, p.n_jk_regions, data, rand, precision, p.s_mu_filename,
+                       p.s_mu_output_type, dd, dr, log, e))
+            return false;
+    }
+    return true;
+}
+
+// The inverse-p program after reading (src/main.cpp:51-60).  The angular
+// stage of calc_angular_upweight (src/correlators_invpweight.cpp:985-1033)
+// runs on the device and its four histograms stay in memory: the 3-D stage
+// takes DD / DD-inverse-p and DR / DR-inverse-p as the up-weight ratios that
+// the reference reads back from its HDF5 files (read_hdf5_hist +
+// divide_by_hist, :20-24).
+bool run_invp(tpcf_ctx *c, const tpcf::Params &p, const tpcf_catalog *data, const tpcf_catalog *rand,
+              int precision, bool dither, double *angular_out, const Log &log, Err &e) {
+    const int nt = p.theta_n_bins, n_jk = p.n_jk_regions;
+    // Hist(0.0, 1.0 - cos(theta_max), theta_n_bins, theta_log_base) (:990-991)
+    const tpcf_axis_spec th{0.0, 1.0 - std::cos(p.theta_max), p.theta_log_base, nt};
+    tpcf_binning *b = nullptr;
+    int rc = tpcf_binning_create(c, TPCF_ANGULAR, &th, nullptr, n_jk, &b);
+    if (rc) return e.set(rc, std::string("angular binning: ") + tpcf_last_error(c));
+    BinPtr bin(b);
+    // kind 0 DD (plain, every point), 1 DD inverse-p, 2 DR, 3 DR inverse-p
+    std::vector<double> ang[4];
+    const char *names[4] = {"angular DD", "angular DD inverse-p", "angular DR", "angular DR inverse-p"};
+    for (int k = 0; k < 4; ++k) {
+        ang[k].assign((size_t)(1 + n_jk) * nt, 0.0);
+        tpcf_weight_spec ws{};
+        ws.weighting = k == 1 ? (dither ? TPCF_WEIGHTS_INVP_DD_DITHER : TPCF_WEIGHTS_INVP_DD)
+                     : k == 3 ? TPCF_WEIGHTS_INVP_DR : TPCF_WEIGHTS_PLAIN;
+        ws.n_bitwise_runs = p.n_bitwise_runs;
+        tpcf_stats st;
+        rc = tpcf_pair_count_weighted(c, data, k < 2 ? nullptr : rand, b, &ws, precision, ang[k].data(),
+                                      ang[k].data() + nt, &st);
+        if (rc) return e.set(rc, std::string(names[k]) + ": " + tpcf_last_error(c));
+        log("%s: %.3e pairs binned, kernel %.1f ms", names[k], (double)st.in_range, st.ms_kernel);
+        if (angular_out) std::copy(ang[k].begin(), ang[k].end(), angular_out + (size_t)k * (1 + n_jk) * nt);
+    }
+    tpcf_weight_spec dd{}, dr{};
+    dd.weighting = dither ? TPCF_WEIGHTS_INVP_DD_DITHER : TPCF_WEIGHTS_INVP_DD;
+    dd.n_bitwise_runs = p.n_bitwise_runs;
+    dd.theta_axis = th;
+    dd.up_numerator = ang[0].data();
+    dd.up_denominator = ang[1].data();
+    dr.weighting = TPCF_WEIGHTS_INVP_DR;
+    dr.n_bitwise_runs = p.n_bitwise_runs;
+    dr.theta_axis = th;
+    dr.up_numerator = ang[2].data();
+    dr.up_denominator = ang[3].data();
+    return correlate_modes(c, p, data, rand, precision, &dd, &dr, log, e);
 }
 
 bool run(const char *path, int device, int precision, const Log &log, Err &e) {
@@ -166,27 +243,7 @@ bool run(const char *path, int device, int precision, const Log &log, Err &e) {
     log("catalogues on device %d: %lld + %lld points kept", device, (long long)tpcf_catalog_n_used(data.get()),
         (long long)tpcf_catalog_n_used(rand.get()));
 
-    if (p.plot_monopole) {
-        tpcf_axis_spec a{p.monopole_min, p.monopole_max, p.monopole_log_base, p.monopole_n_bins};
-        if (!correlate(c, "monopole", TPCF_MONOPOLE, a, nullptr, p.n_jk_regions, data.get(), rand.get(), precision,
-                       p.monopole_filename, p.monopole_output_type, log, e))
-            return false;
-    }
-    if (p.plot_sigma_pi) {
-        tpcf_axis_spec a{p.sigma_min, p.sigma_max, p.sigma_log_base, p.sigma_n_bins};
-        tpcf_axis_spec b{p.pi_min, p.pi_max, p.pi_log_base, p.pi_n_bins};
-        if (!correlate(c, "sigma-pi", TPCF_SIGMA_PI, a, &b, p.n_jk_regions, data.get(), rand.get(), precision,
-                       p.sigma_pi_filename, p.sigma_pi_output_type, log, e))
-            return false;
-    }
-    if (p.plot_s_mu) {
-        tpcf_axis_spec a{p.s_min, p.s_max, p.s_log_base, p.s_n_bins};
-        tpcf_axis_spec b{0.0, 1.0, 0.0, p.mu_n_bins};
-        if (!correlate(c, "s-mu", TPCF_S_MU, a, &b, p.n_jk_regions, data.get(), rand.get(), precision,
-                       p.s_mu_filename, p.s_mu_output_type, log, e))
-            return false;
-    }
-    return true;
+    return correlate_modes(c, p, data.get(), rand.get(), precision, nullptr, nullptr, log, e);
 }
 
 }  // namespace
@@ -204,6 +261,34 @@ extern "C" int tpcf_run_param_file(const char *path, int device, int precision, 
     Err e;
     try {
         if (run(path, device, precision, log, e)) return TPCF_OK;
+    } catch (const std::bad_alloc &) {
+        e.status = TPCF_E_OOM;
+        e.msg = "out of host memory";
+    }
+    tpcf::set_host_error(e.msg);
+    return e.status ? e.status : TPCF_E_INVALID_ARG;
+}
+
+extern "C" int tpcf_run_invp(tpcf_ctx *ctx, const tpcf_params *params, const tpcf_catalog *data,
+                             const tpcf_catalog *randoms, int precision, int dither, double *angular_out,
+                             int log_level) {
+    if (!ctx || !params || !data || !randoms) {
+        tpcf::set_host_error("NULL argument");
+        return TPCF_E_INVALID_ARG;
+    }
+    if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) {
+        tpcf::set_host_error("bad precision");
+        return TPCF_E_INVALID_ARG;
+    }
+    const tpcf::Params &p = params->p;
+    if (p.theta_n_bins < 1 || !(p.theta_max > 0)) {
+        tpcf::set_host_error("theta_max and theta_n_bins must be set for the inverse-p flow");
+        return TPCF_E_INVALID_ARG;
+    }
+    Log log{log_level};
+    Err e;
+    try {
+        if (run_invp(ctx, p, data, randoms, precision, dither != 0, angular_out, log, e)) return TPCF_OK;
     } catch (const std::bad_alloc &) {
         e.status = TPCF_E_OOM;
         e.msg = "out of host memory";

@@ -90,6 +90,7 @@ struct Catalog {
     DevBuf<float> w, iw;
     DevBuf<int> jk;
     DevBuf<long long> masks;
+    DevBuf<long long> dmasks;     // dither masks (Galaxy::dither_mask), n_mask per point, or empty
     DevBuf<int> kept;             // indices kept by the d_comov partition
     std::vector<float> h_w;       // host copies used by normalisation
     std::vector<int> h_jk;
@@ -105,6 +106,9 @@ struct Binning {
     float min_r_sq = 0, max_r_sq = 0;  // float range test of the reference
     double rmax_bound = 0;             // every in-range pair is closer than this on each axis
     std::vector<float> t1, t2;         // threshold tables (see axis.h)
+    // Line of sight for pi: false = x_norm1 + x_norm2 (_ANGULAR_PI_DEFN,
+    // src/correlators.cpp:166-170), true = x1 + x2 (:172-182).
+    bool los_midpoint = false;
     ValueSpace vs1 = ValueSpace::Direct, vs2 = ValueSpace::Direct;
 };
 
@@ -173,6 +177,7 @@ struct CountRequest {
     int weighting = WEIGHTS_PLAIN;
     const UpTable *up = nullptr; // 3-D inverse-p counts
     int n_runs = 0;              // Params::n_bitwise_runs
+    bool dither = false;         // _USE_DITHER_WEIGHTS: popc(dither masks) in place of n_runs
     int refinement = 0;
     // adjoint of a plain-weight 3-D count: with adj_G = dL/d(raw full
     // histogram) set, the count writes per-point dL/dw into grad_a (n_all of

@@ -106,7 +106,10 @@ struct KParams {
     int *err;
     // inverse-p weights and the angular up-weight
     const long long *a_masks, *b_masks;  // original catalogue bitmasks, object-major
+    const long long *a_dmasks, *b_dmasks;  // dither masks (dither != 0), same layout
     int n_mask;
+    int dither;    // _USE_DITHER_WEIGHTS: popc of the dither masks replaces n_runs
+    int los_mid;   // pi along x1 + x2 (src/correlators.cpp:172-182), exact path only
     float n_runs_f;
     double n_runs_d;
     const float *up_thr;                 // n_up + 1 interval thresholds
@@ -187,12 +190,17 @@ struct ExactArgs {
     const double *a_xyz, *a_unit, *b_xyz, *b_unit;
     float min_r_sq, max_r_sq;
     int n1, n2;
+    int los_mid;
 };
 
+// With mid set, (n1*, n2*) are the positions x1, x2 and pi follows the
+// reference's build without _ANGULAR_PI_DEFN (src/correlators.cpp:172-182):
+// sum = (float)(x1 + x2), inv = (float)(1.0 / sqrtf(|sum|^2)) in double,
+// pi = sum_m (d_m sum_m) inv, all in float.
 template <int MODE>
 __device__ __forceinline__ int exact_bin(const ExactArgs &E, const float *t1, const float *t2, float d0, float d1,
                                          float d2, double n1x, double n1y, double n1z, double n2x, double n2y,
-                                         double n2z, bool *in_range) {
+                                         double n2z, bool *in_range, bool mid = false) {
     float s2 = __fadd_rn(__fadd_rn(__fmul_rn(d0, d0), __fmul_rn(d1, d1)), __fmul_rn(d2, d2));
     *in_range = (s2 < E.max_r_sq) && (s2 > E.min_r_sq);
     if (!*in_range) return -1;
@@ -200,10 +208,22 @@ __device__ __forceinline__ int exact_bin(const ExactArgs &E, const float *t1, co
         int b = dev::locate_exact(t1, E.n1, s2);
         return (b >= 0 && b < E.n1) ? b : -1;
     }
-    float pi = __double2float_rn(__dmul_rn((double)d0, __dadd_rn(n1x, n2x)));
-    pi = __double2float_rn(__dadd_rn((double)pi, __dmul_rn((double)d1, __dadd_rn(n1y, n2y))));
-    pi = __double2float_rn(__dadd_rn((double)pi, __dmul_rn((double)d2, __dadd_rn(n1z, n2z))));
-    pi = __double2float_rn(__dmul_rn((double)pi, 0.5));
+    float pi;
+    if (mid) {
+        const float sx = __double2float_rn(__dadd_rn(n1x, n2x));
+        const float sy = __double2float_rn(__dadd_rn(n1y, n2y));
+        const float sz = __double2float_rn(__dadd_rn(n1z, n2z));
+        const float r2 = __fadd_rn(__fadd_rn(__fmul_rn(sx, sx), __fmul_rn(sy, sy)), __fmul_rn(sz, sz));
+        const float inv = __double2float_rn(__ddiv_rn(1.0, (double)__fsqrt_rn(r2)));
+        pi = __fmul_rn(__fmul_rn(d0, sx), inv);
+        pi = __fadd_rn(pi, __fmul_rn(__fmul_rn(d1, sy), inv));
+        pi = __fadd_rn(pi, __fmul_rn(__fmul_rn(d2, sz), inv));
+    } else {
+        pi = __double2float_rn(__dmul_rn((double)d0, __dadd_rn(n1x, n2x)));
+        pi = __double2float_rn(__dadd_rn((double)pi, __dmul_rn((double)d1, __dadd_rn(n1y, n2y))));
+        pi = __double2float_rn(__dadd_rn((double)pi, __dmul_rn((double)d2, __dadd_rn(n1z, n2z))));
+        pi = __double2float_rn(__dmul_rn((double)pi, 0.5));
+    }
     int b1, b2;
     if (MODE == MODE_S_MU) {
         b1 = dev::locate_exact(t1, E.n1, s2);
@@ -249,7 +269,8 @@ __device__ __forceinline__ int exact_pair(const ExactArgs E, const float *t1, co
     float d2 = __double2float_rn(__dsub_rn(x1[2], x2[2]));
     double n1x = 0, n1y = 0, n1z = 0, n2x = 0, n2y = 0, n2z = 0;
     if (MODE != MODE_MONOPOLE) {
-        const double *u1 = E.a_unit + 3 * (size_t)ia, *u2 = E.b_unit + 3 * (size_t)jb;
+        const double *u1 = E.los_mid ? x1 : E.a_unit + 3 * (size_t)ia;
+        const double *u2 = E.los_mid ? x2 : E.b_unit + 3 * (size_t)jb;
         n1x = u1[0];
         n1y = u1[1];
         n1z = u1[2];
@@ -257,7 +278,8 @@ __device__ __forceinline__ int exact_pair(const ExactArgs E, const float *t1, co
         n2y = u2[1];
         n2z = u2[2];
     }
-    return exact_bin<MODE>(E, t1, t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, in_range);
+    return exact_bin<MODE>(E, t1, t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, in_range,
+                           MODE != MODE_MONOPOLE && E.los_mid);
 }
 
 // Parameters of the threshold-search path (passed by value to the
@@ -382,8 +404,19 @@ __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, fl
     for (int k = 0; k < P.n_mask; ++k) c += __popcll((unsigned long long)(__ldg(m1 + k) & __ldg(m2 + k)));
     float pw = (float)c;  // exact: at most 64 * kMaxMaskInts
     if (pw < 0.5f) pw += 1.0f;
-    if (WK == W_ANG_INVP) return __fmul_rn(wprod, __fdiv_rn(P.n_runs_f, pw));
-    const float f = __double2float_rn(__ddiv_rn(__dmul_rn(upweight(P, omct()), P.n_runs_d), (double)pw));
+    // numerator: n_runs, or with _USE_DITHER_WEIGHTS the same float popcount
+    // of the two dither masks (src/correlators_invpweight.cpp:62-71, :749-757)
+    float num = P.n_runs_f;
+    if (P.dither) {
+        const long long *d1 = P.a_dmasks + (size_t)i * P.n_mask;
+        const long long *d2 = P.b_dmasks + (size_t)j * P.n_mask;
+        int dc = 0;
+        for (int k = 0; k < P.n_mask; ++k) dc += __popcll((unsigned long long)(__ldg(d1 + k) & __ldg(d2 + k)));
+        num = (float)dc;
+        if (num < 0.5f) num += 1.0f;
+    }
+    if (WK == W_ANG_INVP) return __fmul_rn(wprod, __fdiv_rn(num, pw));
+    const float f = __double2float_rn(__ddiv_rn(__dmul_rn(upweight(P, omct()), (double)num), (double)pw));
     return __fmul_rn(wprod, f);
 }
 
@@ -562,8 +595,19 @@ __device__ __forceinline__ void bin_exact(const KParams &P, const JobK &J, const
             n2y = u2.y;
             n2z = u2.z;
         }
+        if (MODE != MODE_MONOPOLE && P.los_mid) {
+            const double4 x1 = J.a.xyz_s[ia];
+            const double4 x2 = J.b.xyz_s[jb];
+            n1x = x1.x;
+            n1y = x1.y;
+            n1z = x1.z;
+            n2x = x2.x;
+            n2y = x2.y;
+            n2z = x2.z;
+        }
         bool inr;
-        bin = exact_bin<MODE>(E, S.t1, S.t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr);
+        bin = exact_bin<MODE>(E, S.t1, S.t2, d0, d1, d2, n1x, n1y, n1z, n2x, n2y, n2z, &inr,
+                              MODE != MODE_MONOPOLE && P.los_mid);
         cnt.in_range += inr ? 1 : 0;
         if (bin < 0) return;
     }
@@ -655,7 +699,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             __syncthreads();
         }
         const JobK &J = JK ? *s_job : P.job0;
-        const ExactArgs EA{J.a.xyz, J.a.unit, J.b.xyz, J.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2};
+        const ExactArgs EA{J.a.xyz, J.a.unit, J.b.xyz, J.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2, P.los_mid};
     auto issue = [&](unsigned tc, int start, int len) {
         unsigned char *dst = tile_base + (tc & 1) * tile_stride;
         dev::fence_proxy_async();
@@ -1308,6 +1352,7 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     P.wscale = wscale;
     P.n_runs_f = (float)n_runs;
     P.n_runs_d = (double)n_runs;
+    P.los_mid = bin->los_midpoint ? 1 : 0;
     if (C.up) {
         P.n_up = C.up->ax.n_bins;
         P.up_min = (double)C.up->ax.min;
@@ -1406,9 +1451,11 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     if (!C.unitw && !C.adj) {
         double wmax = wmax_of(A) * wmax_of(B);
         const double up_max = C.up ? 4.0 * C.up->abs_max : 0.0;  // interpolation stays within 4x the bins
-        if (C.wk == W_INVP_DD) wmax *= up_max * std::max(req.n_runs, 1);
+        // the popcount-ratio numerator: n_runs, or a dither popcount (at most 64 per mask word)
+        const double num = std::max(req.dither ? 64.0 * A->n_mask : (double)req.n_runs, 1.0);
+        if (C.wk == W_INVP_DD) wmax *= up_max * num;
         else if (C.wk == W_INVP_DR) wmax *= up_max;
-        else if (C.wk == W_ANG_INVP) wmax *= std::max(req.n_runs, 1);
+        else if (C.wk == W_ANG_INVP) wmax *= num;
         const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
         wscale = std::ldexp(1.0f, S);
         C.inv = std::ldexp(1.0, -S);
@@ -1434,6 +1481,11 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     P.a_masks = A->masks.p;
     P.b_masks = B->masks.p;
     P.n_mask = A->n_mask;
+    if (req.dither && (C.wk == W_INVP_DD || C.wk == W_ANG_INVP)) {
+        P.dither = 1;
+        P.a_dmasks = A->dmasks.p;
+        P.b_dmasks = B->dmasks.p;
+    }
     C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
     return 0;
 }
@@ -1551,9 +1603,12 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
         return 0;
     }
     // A bin that met a non-finite pair weight holds what double
-    // accumulation would: NaN, or an infinity of one sign.
+    // accumulation would: NaN, or an infinity of one sign.  The NaN is the
+    // one x86 arithmetic generates for 0/0 and inf - inf (sign bit set),
+    // which the reference's up-weights carry into its sums and which its
+    // ASCII outputs print as "-nan".
     auto flagged = [](unsigned f, double v) {
-        if ((f & 1u) || ((f & 2u) && (f & 4u))) return std::numeric_limits<double>::quiet_NaN();
+        if ((f & 1u) || ((f & 2u) && (f & 4u))) return std::copysign(std::numeric_limits<double>::quiet_NaN(), -1.0);
         if (f & 2u) return std::numeric_limits<double>::infinity();
         if (f & 4u) return -std::numeric_limits<double>::infinity();
         return v;

@@ -14,6 +14,7 @@ read_file(..., "ascii")     src/io.cpp:240     read_ascii(path, coord_system, ..
 generate_sub_filename       src/io.cpp:628     sub_filename(name, region)
 output_xi_1D / output_xi_2D src/io.cpp:724     write_xi_ascii(name, binning, DD, DR, RR, ...)
 main                        src/main.cpp:11    run_param_file(path)  /  two_pcf_b200/lib/two_pcf
+main, inverse-p build       src/main.cpp:51    run_invp(ctx, params, data, randoms)
 =============================================  ==========================================
 
 All of it runs on the host except run_param_file, whose pair counts run on
@@ -29,7 +30,7 @@ from . import _capi
 from ._capi import CARTESIAN, EQUATORIAL, FP32_GUARD
 
 __all__ = ["Params", "Cosmology", "galaxy_set", "cartesian_set", "read_ascii", "sub_filename", "write_xi_ascii",
-           "run_param_file", "CARTESIAN", "EQUATORIAL", "HostError"]
+           "run_param_file", "run_invp", "CARTESIAN", "EQUATORIAL", "HostError"]
 
 
 class HostError(RuntimeError):
@@ -213,3 +214,18 @@ def write_xi_ascii(filename: str, binning, dd, dr, rr, dd_sub=None, dr_sub=None,
 def run_param_file(path: str, device: int = 0, precision: int = FP32_GUARD, log: bool = False):
     """The reference's program on a parameter file, counts on the GPU."""
     _check(_capi.lib().tpcf_run_param_file(str(path).encode(), int(device), int(precision), int(bool(log))))
+
+
+def run_invp(ctx, params: Params, data, randoms, precision: int = FP32_GUARD, dither: bool = False,
+             log: bool = False) -> dict:
+    """The inverse-p program after reading (tpcf_run_invp): angular stage on
+    the GPU, then the 3-D inverse-p counts and ASCII outputs the parameters
+    ask for.  data / randoms are two_pcf_b200.Catalog objects with bitmasks.
+    Returns the angular histograms {"dd", "dd_invp", "dr", "dr_invp"}, each
+    (full[nt], regions[n_jk, nt]) in the reference's convention."""
+    nt = params.get_int("theta_n_bins")
+    n_jk = params.get_int("n_jk_regions")
+    out = np.zeros((4, 1 + n_jk, nt))
+    _check(_capi.lib().tpcf_run_invp(ctx._h, params._h, data._h, randoms._h, int(precision), int(bool(dither)),
+                                     _ptr(out), int(bool(log))))
+    return {k: (out[i, 0].copy(), out[i, 1:].copy()) for i, k in enumerate(("dd", "dd_invp", "dr", "dr_invp"))}
