@@ -79,7 +79,24 @@ int tpcf_create(int device, tpcf_ctx **out) {
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
     ctx->c.smem_optin = (size_t)optin;
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->c.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        // The context's own pool for per-call scratch: memory a call releases
+        // stays reserved for the next call (the pool is destroyed with the
+        // context), so counts never wait on the driver to map or unmap memory.
+        cudaMemPoolProps props;
+        std::memset(&props, 0, sizeof(props));
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        e = cudaMemPoolCreate(&ctx->c.pool, &props);
+        if (e == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            e = cudaMemPoolSetAttribute(ctx->c.pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+    }
     if (e != cudaSuccess) {
+        if (ctx->c.pool) cudaMemPoolDestroy(ctx->c.pool);
+        if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;
         return TPCF_E_CUDA;
     }
@@ -91,6 +108,8 @@ int tpcf_create(int device, tpcf_ctx **out) {
 int tpcf_destroy(tpcf_ctx *ctx) {
     if (!ctx) return TPCF_E_INVALID_ARG;
     cudaSetDevice(ctx->c.device);
+    if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    if (ctx->c.pool) cudaMemPoolDestroy(ctx->c.pool);
     if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return TPCF_OK;
@@ -146,15 +165,19 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
     c.n_jk = n_jk_regions;
     c.n_mask = bitmask ? n_mask_ints : 0;
 
+    // Host checks and bounds, in parallel over the points.  Each check
+    // reports its lowest failing index, in the order the checks are listed.
     std::vector<double> unit;
-    std::vector<double> dcom_v;
+    int64_t bad = N;
+#pragma omp parallel for schedule(static) reduction(min : bad)
     for (int i = 0; i < N; ++i)
         for (int m = 0; m < 3; ++m)
-            if (!std::isfinite(xyz[3 * (size_t)i + m]))
-                return fail(ctx, TPCF_E_INVALID_ARG, "non-finite coordinate at index " + std::to_string(i));
+            if (!std::isfinite(xyz[3 * (size_t)i + m])) bad = std::min<int64_t>(bad, i);
+    if (bad < N) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite coordinate at index " + std::to_string(bad));
     if (!x_norm) {
         // src/io.cpp:393-399: d_comov = sqrt(x.x), x_norm = x / d_comov.
         unit.resize(3 * (size_t)N);
+#pragma omp parallel for schedule(static)
         for (int i = 0; i < N; ++i) {
             const double *p = xyz + 3 * (size_t)i;
             double d = std::sqrt(p[0] * p[0] + p[1] * p[1] + p[2] * p[2]);
@@ -163,74 +186,89 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
         x_norm = unit.data();
     }
     c.h_jk.assign(N, 0);
-    if (jk_region)
+    if (jk_region) {
+#pragma omp parallel for schedule(static) reduction(min : bad)
         for (int i = 0; i < N; ++i) {
-            if (jk_region[i] < 0 || jk_region[i] >= n_jk_regions)
-                return fail(ctx, TPCF_E_INVALID_ARG, "jk_region out of range at index " + std::to_string(i));
+            if (jk_region[i] < 0 || jk_region[i] >= n_jk_regions) bad = std::min<int64_t>(bad, i);
             c.h_jk[i] = jk_region[i];
         }
+        if (bad < N) return fail(ctx, TPCF_E_INVALID_ARG, "jk_region out of range at index " + std::to_string(bad));
+    }
     c.h_w.assign(N, 1.0f);
     c.unit_weights = true;
     c.w_max = 0;
     c.w_min = 0;
     if (weight) {
+        bool unitw = true;
+#pragma omp parallel for schedule(static) reduction(min : bad) reduction(&& : unitw)
         for (int i = 0; i < N; ++i) {
-            if (!std::isfinite(weight[i])) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite weight");
+            if (!std::isfinite(weight[i])) bad = std::min<int64_t>(bad, i);
             c.h_w[i] = weight[i];
-            if (weight[i] != 1.0f) c.unit_weights = false;
+            unitw = unitw && weight[i] == 1.0f;
         }
+        if (bad < N) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite weight");
+        c.unit_weights = unitw;
     }
     c.n_kept = partition_kept(d_comov, N, c.h_kept);
-    for (int m = 0; m < 3; ++m) {
-        c.lo_kept[m] = c.lo_all[m] = 1e300;
-        c.hi_kept[m] = c.hi_all[m] = -1e300;
-    }
     std::vector<char> is_kept(N, 0);
     for (int k = 0; k < c.n_kept; ++k) is_kept[c.h_kept[k]] = 1;
+    // Bounding boxes of the positions and of the unit vectors (all points and
+    // the kept ones), the largest |weight| and the largest deviation of
+    // |x_norm|^2 from 1 (a term of the angular error bound).
+    double lo_all[3] = {1e300, 1e300, 1e300}, hi_all[3] = {-1e300, -1e300, -1e300};
+    double lo_kept[3] = {1e300, 1e300, 1e300}, hi_kept[3] = {-1e300, -1e300, -1e300};
+    double ulo_all[3] = {1e300, 1e300, 1e300}, uhi_all[3] = {-1e300, -1e300, -1e300};
+    double ulo_kept[3] = {1e300, 1e300, 1e300}, uhi_kept[3] = {-1e300, -1e300, -1e300};
+    float w_max = 0;
+    double norm_dev = 0;
+#pragma omp parallel for schedule(static) reduction(min : bad, lo_all[:3], lo_kept[:3], ulo_all[:3], ulo_kept[:3]) \
+    reduction(max : hi_all[:3], hi_kept[:3], uhi_all[:3], uhi_kept[:3], w_max, norm_dev)
     for (int i = 0; i < N; ++i) {
-        const float a = std::fabs(c.h_w[i]);
-        c.w_max = std::max(c.w_max, a);
-        for (int m = 0; m < 3; ++m) {
-            const double v = xyz[3 * (size_t)i + m];
-            c.lo_all[m] = std::min(c.lo_all[m], v);
-            c.hi_all[m] = std::max(c.hi_all[m], v);
-            if (is_kept[i]) {
-                c.lo_kept[m] = std::min(c.lo_kept[m], v);
-                c.hi_kept[m] = std::max(c.hi_kept[m], v);
-            }
-        }
-    }
-    // Unit vectors: bounding boxes (angular cells) and the largest deviation
-    // of |x_norm|^2 from 1 (a term of the angular error bound).
-    for (int m = 0; m < 3; ++m) {
-        c.ulo_kept[m] = c.ulo_all[m] = 1e300;
-        c.uhi_kept[m] = c.uhi_all[m] = -1e300;
-    }
-    c.norm_dev = 0;
-    for (int i = 0; i < N; ++i) {
+        w_max = std::max(w_max, std::fabs(c.h_w[i]));
         const double *u = x_norm + 3 * (size_t)i;
         for (int m = 0; m < 3; ++m) {
-            if (!std::isfinite(u[m]))
-                return fail(ctx, TPCF_E_INVALID_ARG, "non-finite x_norm at index " + std::to_string(i));
-            c.ulo_all[m] = std::min(c.ulo_all[m], u[m]);
-            c.uhi_all[m] = std::max(c.uhi_all[m], u[m]);
+            const double v = xyz[3 * (size_t)i + m];
+            lo_all[m] = std::min(lo_all[m], v);
+            hi_all[m] = std::max(hi_all[m], v);
+            if (!std::isfinite(u[m])) bad = std::min<int64_t>(bad, i);
+            ulo_all[m] = std::min(ulo_all[m], u[m]);
+            uhi_all[m] = std::max(uhi_all[m], u[m]);
             if (is_kept[i]) {
-                c.ulo_kept[m] = std::min(c.ulo_kept[m], u[m]);
-                c.uhi_kept[m] = std::max(c.uhi_kept[m], u[m]);
+                lo_kept[m] = std::min(lo_kept[m], v);
+                hi_kept[m] = std::max(hi_kept[m], v);
+                ulo_kept[m] = std::min(ulo_kept[m], u[m]);
+                uhi_kept[m] = std::max(uhi_kept[m], u[m]);
             }
         }
-        c.norm_dev = std::max(c.norm_dev, std::fabs(u[0] * u[0] + u[1] * u[1] + u[2] * u[2] - 1.0));
+        norm_dev = std::max(norm_dev, std::fabs(u[0] * u[0] + u[1] * u[1] + u[2] * u[2] - 1.0));
     }
+    if (bad < N) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite x_norm at index " + std::to_string(bad));
+    for (int m = 0; m < 3; ++m) {
+        c.lo_all[m] = lo_all[m];
+        c.hi_all[m] = hi_all[m];
+        c.lo_kept[m] = lo_kept[m];
+        c.hi_kept[m] = hi_kept[m];
+        c.ulo_all[m] = ulo_all[m];
+        c.uhi_all[m] = uhi_all[m];
+        c.ulo_kept[m] = ulo_kept[m];
+        c.uhi_kept[m] = uhi_kept[m];
+    }
+    c.w_max = w_max;
+    c.norm_dev = norm_dev;
     c.iw_max = c.w_max;
     c.iw_unit = c.unit_weights;
     if (input_weight) {
-        c.iw_max = 0;
-        c.iw_unit = true;
+        float iw_max = 0;
+        bool iw_unit = true;
+#pragma omp parallel for schedule(static) reduction(min : bad) reduction(max : iw_max) reduction(&& : iw_unit)
         for (int i = 0; i < N; ++i) {
-            if (!std::isfinite(input_weight[i])) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite input_weight");
-            c.iw_max = std::max(c.iw_max, std::fabs(input_weight[i]));
-            if (input_weight[i] != 1.0f) c.iw_unit = false;
+            if (!std::isfinite(input_weight[i])) bad = std::min<int64_t>(bad, i);
+            iw_max = std::max(iw_max, std::fabs(input_weight[i]));
+            iw_unit = iw_unit && input_weight[i] == 1.0f;
         }
+        if (bad < N) return fail(ctx, TPCF_E_INVALID_ARG, "non-finite input_weight");
+        c.iw_max = iw_max;
+        c.iw_unit = iw_unit;
     }
 
     cudaStream_t st = ctx->c.stream;
@@ -239,11 +277,11 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
         cudaError_t _e = (expr);                                 \
         if (_e != cudaSuccess) return cuda_fail(ctx, _e, "catalogue upload"); \
     } while (0)
-    CAT_TRY(c.xyz.alloc(3 * (size_t)N));
-    CAT_TRY(c.unit.alloc(3 * (size_t)N));
-    CAT_TRY(c.w.alloc(N));
-    CAT_TRY(c.jk.alloc(N));
-    CAT_TRY(c.kept.alloc(c.n_kept));
+    CAT_TRY(c.xyz.alloc(ctx->c, 3 * (size_t)N));
+    CAT_TRY(c.unit.alloc(ctx->c, 3 * (size_t)N));
+    CAT_TRY(c.w.alloc(ctx->c, N));
+    CAT_TRY(c.jk.alloc(ctx->c, N));
+    CAT_TRY(c.kept.alloc(ctx->c, c.n_kept));
     if (N > 0) {
         CAT_TRY(cudaMemcpyAsync(c.xyz.p, xyz, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
         CAT_TRY(cudaMemcpyAsync(c.unit.p, x_norm, sizeof(double) * 3 * N, cudaMemcpyHostToDevice, st));
@@ -253,11 +291,11 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
     if (c.n_kept > 0)
         CAT_TRY(cudaMemcpyAsync(c.kept.p, c.h_kept.data(), sizeof(int) * c.n_kept, cudaMemcpyHostToDevice, st));
     if (input_weight) {
-        CAT_TRY(c.iw.alloc(N));
+        CAT_TRY(c.iw.alloc(ctx->c, N));
         if (N > 0) CAT_TRY(cudaMemcpyAsync(c.iw.p, input_weight, sizeof(float) * N, cudaMemcpyHostToDevice, st));
     }
     if (c.n_mask > 0) {
-        CAT_TRY(c.masks.alloc((size_t)N * c.n_mask));
+        CAT_TRY(c.masks.alloc(ctx->c, (size_t)N * c.n_mask));
         if (N > 0)
             CAT_TRY(cudaMemcpyAsync(c.masks.p, bitmask, sizeof(long long) * (size_t)N * c.n_mask,
                                     cudaMemcpyHostToDevice, st));
@@ -580,7 +618,7 @@ int tpcf_catalog_set_dither_masks(tpcf_catalog *cat, const int64_t *dither_mask)
     }
     const size_t words = (size_t)c.n_all * c.n_mask;
     cudaError_t e = cudaSetDevice(ctx->device);
-    if (e == cudaSuccess) e = c.dmasks.alloc(words);
+    if (e == cudaSuccess) e = c.dmasks.alloc(*ctx, words);
     if (e == cudaSuccess && words > 0)
         e = cudaMemcpyAsync(c.dmasks.p, dither_mask, sizeof(long long) * words, cudaMemcpyHostToDevice, ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);

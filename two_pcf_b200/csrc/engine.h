@@ -42,6 +42,89 @@ struct Error {
     std::string msg;
 };
 
+struct Ctx {
+    int device = 0;
+    int num_sms = 148;
+    size_t smem_optin = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    std::string last_error;
+    int refinement = 0;  // 0 = automatic
+    unsigned long long launches = 0;  // kernels launched by this context
+    cudaMemPool_t pool = nullptr;     // stream-ordered pool for the scratch of each call
+};
+
+// Device scratch of one call, from the context's stream-ordered memory pool:
+// allocation and release are queued on the context's stream and released
+// memory stays in the pool for the next call, so a count neither
+// synchronises the device nor hands memory back to the driver (a cudaFree of
+// a large work list has been measured taking most of a second).  Only for
+// buffers that do not outlive the call.
+template <typename T>
+struct ScratchBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    ScratchBuf() = default;
+    ScratchBuf(const ScratchBuf &) = delete;
+    ScratchBuf &operator=(const ScratchBuf &) = delete;
+    ~ScratchBuf() { release(); }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(const Ctx &ctx, size_t count) {
+        release();
+        if (count == 0) count = 1;
+        s = ctx.stream;
+        cudaError_t e = ctx.pool ? cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), ctx.pool, s)
+                                 : cudaMallocAsync((void **)&p, count * sizeof(T), s);
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
+
+
+// Device memory from a context's pool that outlives the call that made it
+// (the cell grids cached on a catalogue): allocated in the context's stream
+// order, and released on the legacy stream when its owner goes.  Every
+// engine call returns with its stream drained, so nothing still reads the
+// memory by then; the release neither synchronises the device nor unmaps
+// memory, and it stays valid after the context (and its pool) is destroyed.
+template <typename T>
+struct PoolBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    int device = 0;
+    PoolBuf() = default;
+    PoolBuf(const PoolBuf &) = delete;
+    PoolBuf &operator=(const PoolBuf &) = delete;
+    ~PoolBuf() { release(); }
+    void release() {
+        if (p) {
+            int cur = device;
+            cudaGetDevice(&cur);
+            if (cur != device) cudaSetDevice(device);
+            cudaFreeAsync(p, 0);
+            if (cur != device) cudaSetDevice(cur);
+        }
+        p = nullptr;
+        n = 0;
+    }
+    cudaError_t alloc(const Ctx &ctx, size_t count) {
+        release();
+        if (count == 0) count = 1;
+        device = ctx.device;
+        cudaError_t e = ctx.pool ? cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), ctx.pool, ctx.stream)
+                                 : cudaMallocAsync((void **)&p, count * sizeof(T), ctx.stream);
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+};
+
 // The points of one catalogue sorted into cubic cells of side `side` on the
 // lattice x = k * side (k integer), with points inside a cell ordered by
 // jackknife region.  Replaces GalaxyBoxes (src/boxes.cpp:10-163).
@@ -55,24 +138,22 @@ struct Grid {
     int ncell = 0;        // size of the dense cell table
     int n = 0;            // points in the grid
     bool subset_kept = true;
-    DevBuf<float4> pos;   // (x - kx*side, y - ky*side, z - kz*side, weight), float
-    DevBuf<float4> aux;   // (x_norm as float, jk as int bits)
-    DevBuf<int> idx;      // original catalogue index
-    DevBuf<double4> xyz_s;   // sorted double coordinates (exact path, FP64 path)
-    DevBuf<double4> unit_s;  // sorted double unit vectors
-    DevBuf<int> cell_start;  // ncell + 1
-    DevBuf<int3> cell_coord; // local coords of each dense cell id (for offsets)
-    DevBuf<int> region_start;  // ncell + 1, CSR of distinct jk regions per cell
-    DevBuf<int> regions;       // region of each run
-    DevBuf<int> run_start;     // first point of each run
+    PoolBuf<float4> pos;   // (x - kx*side, y - ky*side, z - kz*side, weight), float
+    PoolBuf<float4> aux;   // (x_norm as float, jk as int bits)
+    PoolBuf<int> idx;      // original catalogue index
+    PoolBuf<double4> xyz_s;   // sorted double coordinates (exact path, FP64 path)
+    PoolBuf<double4> unit_s;  // sorted double unit vectors
+    PoolBuf<int> cell_start;  // ncell + 1
+    PoolBuf<int3> cell_coord; // local coords of each dense cell id (for offsets)
+    PoolBuf<int> region_start;  // ncell + 1, CSR of distinct jk regions per cell
+    PoolBuf<int> regions;       // region of each run
+    PoolBuf<int> run_start;     // first point of each run
     std::vector<int> h_cell_start;  // host copies for the work-list build
     std::vector<int> h_region_start;
     std::vector<int> h_regions;
     std::vector<int> h_run_start;
     bool has_fp64 = false;
 };
-
-struct Ctx;
 
 struct Catalog {
     Ctx *ctx = nullptr;
@@ -86,12 +167,12 @@ struct Catalog {
     double ulo_kept[3], uhi_kept[3], ulo_all[3], uhi_all[3];  // bounding boxes of the unit vectors
     double norm_dev = 0;          // max | x_norm . x_norm - 1 |
     bool iw_unit = true;          // every input weight == 1.0f
-    DevBuf<double> xyz, unit;
-    DevBuf<float> w, iw;
-    DevBuf<int> jk;
-    DevBuf<long long> masks;
-    DevBuf<long long> dmasks;     // dither masks (Galaxy::dither_mask), n_mask per point, or empty
-    DevBuf<int> kept;             // indices kept by the d_comov partition
+    PoolBuf<double> xyz, unit;
+    PoolBuf<float> w, iw;
+    PoolBuf<int> jk;
+    PoolBuf<long long> masks;
+    PoolBuf<long long> dmasks;    // dither masks (Galaxy::dither_mask), n_mask per point, or empty
+    PoolBuf<int> kept;            // indices kept by the d_comov partition
     std::vector<float> h_w;       // host copies used by normalisation
     std::vector<int> h_jk;
     std::vector<int> h_kept;
@@ -117,16 +198,6 @@ struct Stats {
     double ms_kernel = 0, ms_total = 0;
 };
 
-struct Ctx {
-    int device = 0;
-    int num_sms = 148;
-    size_t smem_optin = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
-    std::string last_error;
-    int refinement = 0;  // 0 = automatic
-    unsigned long long launches = 0;  // kernels launched by this context
-};
 
 // grid.cu
 // Which grid of a catalogue: cell side, the point subset (the d_comov

@@ -317,20 +317,20 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
                cat->n_jk};
 
     long long nbucket = ncell * cat->n_jk;
-    DevBuf<int> bucket, counts;
-    TPCF_CUDA_TRY(bucket.alloc(n));
-    TPCF_CUDA_TRY(counts.alloc(nbucket + 1));
-    TPCF_CUDA_TRY(g->pos.alloc(n));
-    TPCF_CUDA_TRY(g->aux.alloc(n));
-    TPCF_CUDA_TRY(g->idx.alloc(n));
+    ScratchBuf<int> bucket, counts;
+    TPCF_CUDA_TRY(bucket.alloc(*ctx, n));
+    TPCF_CUDA_TRY(counts.alloc(*ctx, nbucket + 1));
+    TPCF_CUDA_TRY(g->pos.alloc(*ctx, n));
+    TPCF_CUDA_TRY(g->aux.alloc(*ctx, n));
+    TPCF_CUDA_TRY(g->idx.alloc(*ctx, n));
     if (want_fp64) {
-        TPCF_CUDA_TRY(g->xyz_s.alloc(n));
-        TPCF_CUDA_TRY(g->unit_s.alloc(n));
+        TPCF_CUDA_TRY(g->xyz_s.alloc(*ctx, n));
+        TPCF_CUDA_TRY(g->unit_s.alloc(*ctx, n));
         g->has_fp64 = true;
     }
-    TPCF_CUDA_TRY(g->cell_start.alloc(ncell + 1));
-    TPCF_CUDA_TRY(g->cell_coord.alloc(ncell));
-    TPCF_CUDA_TRY(g->region_start.alloc(ncell + 1));
+    TPCF_CUDA_TRY(g->cell_start.alloc(*ctx, ncell + 1));
+    TPCF_CUDA_TRY(g->cell_coord.alloc(*ctx, ncell));
+    TPCF_CUDA_TRY(g->region_start.alloc(*ctx, ncell + 1));
     TPCF_CUDA_TRY(cudaMemsetAsync(counts.p, 0, sizeof(int) * (nbucket + 1), st));
     const int *subset = subset_kept ? cat->kept.p : nullptr;
     const int *jk = cat->n_jk > 1 ? cat->jk.p : nullptr;
@@ -341,8 +341,8 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
     }
     // counts -> bucket starts (exclusive); the extra element becomes n.
     TPCF_CUDA_TRY(exclusive_scan(counts.p, counts.p, nbucket + 1, st, &ctx->launches));
-    DevBuf<int> fill;
-    TPCF_CUDA_TRY(fill.alloc(nbucket));
+    ScratchBuf<int> fill;
+    TPCF_CUDA_TRY(fill.alloc(*ctx, nbucket));
     TPCF_CUDA_TRY(cudaMemsetAsync(fill.p, 0, sizeof(int) * nbucket, st));
     if (n > 0) {
         scatter_kernel<<<(n + 255) / 256, 256, 0, st>>>(gd, coords, cat->unit.p, wsrc,
@@ -352,8 +352,8 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
         ++ctx->launches;
         TPCF_CUDA_TRY(cudaGetLastError());
     }
-    DevBuf<int> nreg;
-    TPCF_CUDA_TRY(nreg.alloc(ncell + 1));
+    ScratchBuf<int> nreg;
+    TPCF_CUDA_TRY(nreg.alloc(*ctx, ncell + 1));
     TPCF_CUDA_TRY(cudaMemsetAsync(nreg.p, 0, sizeof(int) * (ncell + 1), st));
     cells_kernel<<<(unsigned)((ncell + 1 + 255) / 256), 256, 0, st>>>(gd, (int)ncell, n, counts.p, g->cell_start.p,
                                                                      g->cell_coord.p, nreg.p);
@@ -368,8 +368,8 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
                                   cudaMemcpyDeviceToHost, st));
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
     int nregions = g->h_region_start[ncell];
-    TPCF_CUDA_TRY(g->regions.alloc(nregions));
-    TPCF_CUDA_TRY(g->run_start.alloc(nregions));
+    TPCF_CUDA_TRY(g->regions.alloc(*ctx, nregions));
+    TPCF_CUDA_TRY(g->run_start.alloc(*ctx, nregions));
     regions_kernel<<<(unsigned)((ncell + 255) / 256), 256, 0, st>>>(gd, (int)ncell, counts.p, g->region_start.p,
                                                                    g->regions.p, g->run_start.p);
     ++ctx->launches;

@@ -1414,14 +1414,19 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     int m = req.refinement > 0 ? req.refinement : ctx->refinement;
     if (m <= 0) {
         // Automatic: refine to side rb/2 when cells of that size would still
-        // hold a few hundred points on average.
-        const double *lo = C.angular ? (subset ? A->ulo_kept : A->ulo_all) : A->lo_kept;
-        const double *hi = C.angular ? (subset ? A->uhi_kept : A->uhi_all) : A->hi_kept;
-        const double n = subset ? (double)A->n_kept : (double)A->n_all;
-        double vol = 1;
-        for (int k = 0; k < 3; ++k) vol *= std::max(hi[k] - lo[k], rb);
-        const double per_cell = n * (rb / 2) * (rb / 2) * (rb / 2) / vol;
-        m = per_cell >= 256 ? 2 : 1;
+        // hold a few hundred points on average in the denser catalogue (the
+        // B points a cell's stencil visits set the candidate count; measured
+        // on the survey benchmark, a cross count of sparse data against dense
+        // randoms runs ~10 % faster at side rb/2 than at rb).
+        auto per_cell = [&](const Catalog *X) {
+            const double *lo = C.angular ? (subset ? X->ulo_kept : X->ulo_all) : X->lo_kept;
+            const double *hi = C.angular ? (subset ? X->uhi_kept : X->uhi_all) : X->hi_kept;
+            const double n = subset ? (double)X->n_kept : (double)X->n_all;
+            double vol = 1;
+            for (int k = 0; k < 3; ++k) vol *= std::max(hi[k] - lo[k], rb);
+            return n * (rb / 2) * (rb / 2) * (rb / 2) / vol;
+        };
+        m = std::max(per_cell(A), per_cell(B)) >= 256 ? 2 : 1;
     }
     const double side = rb / m * (1.0 + 1e-9);
     GridSpec gs;
@@ -1644,38 +1649,39 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     CountPlan C;
     if (plan_count(ctx, req, true, C, err)) return err->status;
     const Binning *bin = req.bin;
-    DevBuf<WorkItem> d_items;
-    DevBuf<Segment> d_segs;
-    DevBuf<unsigned long long> d_full, d_sub, d_cnt;
-    DevBuf<int> d_head, d_err;
-    DevBuf<float> d_t1, d_t2, d_up_thr;
-    DevBuf<unsigned char> d_l1, d_l2;
-    DevBuf<unsigned> d_flags;
-    DevBuf<double> d_up_bins, d_up_centre;
-    TPCF_TRY(d_items.alloc(C.items.size()));
-    TPCF_TRY(d_segs.alloc(C.segs.size()));
-    TPCF_TRY(d_full.alloc(2 * (size_t)C.nb));
-    TPCF_TRY(d_sub.alloc(2 * (size_t)C.nb * C.n_jk));
-    TPCF_TRY(d_cnt.alloc(4));
-    TPCF_TRY(d_head.alloc(1));
-    TPCF_TRY(d_err.alloc(1));
-    TPCF_TRY(d_t1.alloc(bin->t1.size()));
-    TPCF_TRY(d_t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
-    TPCF_TRY(d_l1.alloc(LUT1_N));
-    TPCF_TRY(d_l2.alloc(LUT2_N));
-    if (C.n_flags()) TPCF_TRY(d_flags.alloc(C.n_flags()));
+    ScratchBuf<WorkItem> d_items;
+    ScratchBuf<Segment> d_segs;
+    ScratchBuf<unsigned long long> d_full, d_sub, d_cnt;
+    ScratchBuf<int> d_head, d_err;
+    ScratchBuf<float> d_t1, d_t2, d_up_thr;
+    ScratchBuf<unsigned char> d_l1, d_l2;
+    ScratchBuf<unsigned> d_flags;
+    ScratchBuf<double> d_up_bins, d_up_centre;
+    const Ctx &X = *ctx;
+    TPCF_TRY(d_items.alloc(X, C.items.size()));
+    TPCF_TRY(d_segs.alloc(X, C.segs.size()));
+    TPCF_TRY(d_full.alloc(X, 2 * (size_t)C.nb));
+    TPCF_TRY(d_sub.alloc(X, 2 * (size_t)C.nb * C.n_jk));
+    TPCF_TRY(d_cnt.alloc(X, 4));
+    TPCF_TRY(d_head.alloc(X, 1));
+    TPCF_TRY(d_err.alloc(X, 1));
+    TPCF_TRY(d_t1.alloc(X, bin->t1.size()));
+    TPCF_TRY(d_t2.alloc(X, std::max<size_t>(bin->t2.size(), 1)));
+    TPCF_TRY(d_l1.alloc(X, LUT1_N));
+    TPCF_TRY(d_l2.alloc(X, LUT2_N));
+    if (C.n_flags()) TPCF_TRY(d_flags.alloc(X, C.n_flags()));
     if (C.up) {
-        TPCF_TRY(d_up_thr.alloc(C.n_up()));
-        TPCF_TRY(d_up_bins.alloc(C.n_up()));
-        TPCF_TRY(d_up_centre.alloc(C.n_up()));
+        TPCF_TRY(d_up_thr.alloc(X, C.n_up()));
+        TPCF_TRY(d_up_bins.alloc(X, C.n_up()));
+        TPCF_TRY(d_up_centre.alloc(X, C.n_up()));
     }
-    DevBuf<JobK> d_jobs;
-    TPCF_TRY(d_jobs.alloc(C.jobs.size()));
-    DevBuf<double> d_adj_G, d_grad_a, d_grad_b;
+    ScratchBuf<JobK> d_jobs;
+    TPCF_TRY(d_jobs.alloc(X, C.jobs.size()));
+    ScratchBuf<double> d_adj_G, d_grad_a, d_grad_b;
     if (C.adj) {
-        TPCF_TRY(d_adj_G.alloc(C.nb));
-        TPCF_TRY(d_grad_a.alloc(std::max(C.n_a, 1)));
-        if (!C.is_auto) TPCF_TRY(d_grad_b.alloc(std::max(C.n_b, 1)));
+        TPCF_TRY(d_adj_G.alloc(X, C.nb));
+        TPCF_TRY(d_grad_a.alloc(X, std::max(C.n_a, 1)));
+        if (!C.is_auto) TPCF_TRY(d_grad_b.alloc(X, std::max(C.n_b, 1)));
     }
     CountBuffers D;
     D.jobs = d_jobs.p;
