@@ -53,6 +53,9 @@ def parse():
     p.add_argument("--no-fp64", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--strong", action="store_true",
+                   help="with --gpus N > 1: one workload, every count split over the ranks (strong scaling); "
+                        "default: one workload replica per rank (weak scaling)")
     p.add_argument("--one-count", choices=["s_mu", "sigma_pi"], default=None,
                    help="profiling case: one RR count of the workload's randoms at --scale, then exit")
     return p.parse_args()
@@ -91,6 +94,16 @@ def dist_max(x: float, ws: int) -> float:
     import torch.distributed as dist
     t = torch.tensor([x], dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_sum(x: float, ws: int) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -160,9 +173,10 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
-def count_step(tp, ctx, D, R, bins, precision, release=True):
-    """One pass: grids rebuilt, then DD, DR, RR for each binning.
-    Returns (in_range, candidates, kernel_ms, flops, hists)."""
+def count_step(tp, ctx, D, R, bins, precision, release=True, sharded=False):
+    """One pass: grids rebuilt, then DD, DR, RR for each binning; sharded:
+    each count split over the ranks (tp.count_sharded), this rank's shard.
+    Returns (in_range, candidates, kernel_ms, flops, hists) of this rank."""
     if release:
         for c in (D, R):
             tp._capi.lib().tpcf_catalog_release_cache(c._h)
@@ -172,7 +186,10 @@ def count_step(tp, ctx, D, R, bins, precision, release=True):
     hists = []
     for mode, b in bins:
         for a, bb in ((D, None), (D, R), (R, None)):
-            full, reg, st = tp.count(ctx, a, bb, b, precision)
+            if sharded:
+                full, reg, st = tp.count_sharded(ctx, a, bb, b, precision)
+            else:
+                full, reg, st = tp.count(ctx, a, bb, b, precision)
             in_range += st["in_range"]
             cand += st["candidates"]
             kms += st["ms_kernel"]
@@ -288,7 +305,8 @@ def main():
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
 
-    w = make_workload(2 + rank, args.scale)
+    sharded = args.strong and ws > 1
+    w = make_workload(2 if sharded else 2 + rank, args.scale)
     n_jk = w["n_jk"]
     d, r = w["data"], w["rand"]
     D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], n_jk)
@@ -303,7 +321,7 @@ def main():
     flush = torch.empty(256 * 1024 * 1024, dtype=torch.uint8, device=f"cuda:{local}")
 
     for _ in range(max(3, args.warmup)):
-        count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)
+        count_step(tp, ctx, D, R, bins, tp.FP32_GUARD, sharded=sharded)
     torch.cuda.synchronize()
 
     launches0 = tp._capi.lib().tpcf_kernel_launches(ctx._h)
@@ -319,7 +337,7 @@ def main():
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            n_in, n_c, kms, fl, hists = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)
+            n_in, n_c, kms, fl, hists = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD, sharded=sharded)
             e1.record(stream)
             e1.synchronize()
             step_ms.append(e0.elapsed_time(e1))
@@ -331,7 +349,8 @@ def main():
         dist_barrier(ws)
     launches = tp._capi.lib().tpcf_kernel_launches(ctx._h) - launches0
     total_ms = dist_max(sum(step_ms), ws)
-    value = tot_in * ws / (total_ms * 1e-3)   # every rank processes the same-sized workload
+    # whole job: pairs counted by all ranks (replicas, or the shards of one workload)
+    value = dist_sum(tot_in, ws) / (total_ms * 1e-3)
     clocks = clk.summary()
 
     # plain FP64 path on one step, and bit-exactness of the two paths
@@ -341,12 +360,12 @@ def main():
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        n64, _, kms64, _, h64 = count_step(tp, ctx, D, R, bins, tp.FP64)
+        n64, _, kms64, _, h64 = count_step(tp, ctx, D, R, bins, tp.FP64, sharded=sharded)
         e1.record(stream)
         e1.synchronize()
         ms64 = e0.elapsed_time(e1)
         exact = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(hists, h64))
-        fp64 = {"value": n64 / (ms64 * 1e-3), "ms_per_step": ms64, "kernel_ms": kms64,
+        fp64 = {"value": dist_sum(n64, ws) / (dist_max(ms64, ws) * 1e-3), "ms_per_step": ms64, "kernel_ms": kms64,
                 "speedup_fp32_guard": (ms64 / (sum(step_ms) / len(step_ms))),
                 "bit_exact_histograms": bool(exact), "in_range_equal": int(n64) == int(tot_in // args.steps)}
 
@@ -368,7 +387,7 @@ def main():
                             pin["d"]["jk"], n_jk)
             Rp = tp.Catalog(ctx, pin["r"]["xyz"], pin["r"]["x_norm"], pin["r"]["d_comov"], pin["r"]["weight"], None,
                             pin["r"]["jk"], n_jk)
-            n_in = count_step(tp, ctx, Dp, Rp, bins, tp.FP32_GUARD, release=False)[0]
+            n_in = count_step(tp, ctx, Dp, Rp, bins, tp.FP32_GUARD, release=False, sharded=sharded)[0]
             torch.cuda.synchronize()
             dt = time.perf_counter() - t0
             Dp.close()
@@ -377,7 +396,7 @@ def main():
                 e_ms.append(dt * 1e3)
                 e_in += n_in
         e_total = dist_max(sum(e_ms), ws)
-        e2e = {"value": e_in * ws / (e_total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e2e = {"value": dist_sum(e_in, ws) / (e_total * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": e_total / len(e_ms)}
 
     cpu = None
@@ -392,7 +411,8 @@ def main():
     achieved = tot_flops / (tot_kms * 1e-3) / 1e12 if tot_kms > 0 else 0.0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong" if sharded else "weak",
+        "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
         "config": {"workload": "survey slab: 1M clustered data + 5M randoms, weights lognormal(0,0.2), 100 jk "
                                "regions; sigma-pi 50x50 linear 0-50 + s-mu 40 log(1.3) 0-100 x 50 mu; "
@@ -400,7 +420,7 @@ def main():
                    "scale": args.scale, "n_data": int(d["xyz"].shape[0]), "n_rand": int(r["xyz"].shape[0]),
                    "l2": "inputs larger than L2 (sorted tiles 192 MB + catalogues) and a 256 MB L2 flush "
                          "between steps",
-                   "parallelism": f"replicas{ws}" if ws > 1 else "single"},
+                   "parallelism": (f"shards{ws}" if sharded else f"replicas{ws}") if ws > 1 else "single"},
         "in_range_pairs_per_step": tot_in // args.steps, "candidates_per_step": tot_cand // args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops, "unit": "TFLOP/s",
                      "frac": achieved / fp32_tflops if fp32_tflops else None,

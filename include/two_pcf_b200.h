@@ -284,6 +284,30 @@ int tpcf_upweight_eval(const tpcf_weight_spec *spec, const double *values, int64
 int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                        int precision, double *full_out, double *region_out, tpcf_stats *stats);
 
+/* One shard of a count split across processes or GPUs (strong scaling; no
+ * counterpart in the reference, whose counts run on one node's threads).
+ * Every shard plans the same work list (it depends only on the catalogues,
+ * the binning and the refinement) and runs the items k with
+ * k % n_shards == shard, dealt from the largest down.  It returns its partial
+ * sums instead of doubles: per histogram slot (the nb full bins, then the
+ * n_jk * nb region bins of tpcf_count's region_out) TPCF_PARTIAL_WORDS int64:
+ * the slot's 128-bit two's-complement fixed-point sum as four 32-bit limbs,
+ * least significant first, then the numbers of NaN, +inf and -inf pair
+ * weights met.  Adding the partial arrays of all shards word by word (for
+ * example an all-reduce SUM over int64) cannot overflow for up to 2^31
+ * shards, and tpcf_shard_combine turns the sum into exactly the doubles one
+ * tpcf_count would return, weighted sums included.  *scale_exp receives the
+ * fixed-point exponent, the same on every shard.
+ *   partial[(1 + n_jk) * nb * TPCF_PARTIAL_WORDS] */
+#define TPCF_PARTIAL_WORDS 7
+int tpcf_count_shard(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                     const tpcf_weight_spec *spec, int precision, int32_t shard, int32_t n_shards, int64_t *partial,
+                     int32_t *scale_exp, tpcf_stats *stats);
+/* Summed partials to full_out[nb] and region_out[n_jk * nb] (may be NULL), as
+ * tpcf_count returns them.  Host-only. */
+int tpcf_shard_combine(const tpcf_binning *bin, const int64_t *partial, int32_t scale_exp, double *full_out,
+                       double *region_out);
+
 /* The reference's counting entry points with its output convention: the
  * histograms after invert_jk_hists() and, for auto counts, multiply_hists(2.0)
  * — what auto_pair_count_{monopole,sigma_pi,s_mu}(const GalaxyBoxes*, JKHists*)

@@ -36,7 +36,7 @@ __all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "au
            "normalise_cross",
            "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
            "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR", "WEIGHTS_INVP_DD_DITHER", "LOS_ANGULAR", "LOS_MIDPOINT", "iip_weights",
-           "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE"]
+           "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE", "count_shard", "shard_combine", "count_sharded"]
 
 
 class TpcfError(RuntimeError):
@@ -300,6 +300,58 @@ def iip_weights(bitmask, weight, n_bitwise_runs: int, dither_mask=None):
     iw = np.empty(n, np.float32)
     _check(_capi.lib().tpcf_iip_weights(n, m.shape[1], _ptr(m), _ptr(d), int(n_bitwise_runs), _ptr(w), _ptr(iw)))
     return w, iw
+
+
+def count_shard(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, shard: int, n_shards: int,
+                precision: int = FP32_GUARD, weights: Weights | None = None):
+    """One shard of a count split across processes (tpcf_count_shard): returns
+    (partial[(1 + n_jk) * nb, PARTIAL_WORDS] int64, scale_exp, stats).  Partials
+    of all shards add word by word; shard_combine turns the sum into the
+    count's histograms."""
+    partial = np.zeros(((1 + binning.n_jk) * binning.nb, _capi.PARTIAL_WORDS), np.int64)
+    se = C.c_int32()
+    st = Stats()
+    rc = _capi.lib().tpcf_count_shard(ctx._h, a._h, b._h if b is not None else None, binning._h,
+                                      C.byref(weights.spec) if weights is not None else None, int(precision),
+                                      int(shard), int(n_shards), _ptr(partial), C.byref(se), C.byref(st))
+    _check(rc, ctx)
+    return partial, se.value, st.as_dict()
+
+
+def shard_combine(binning: Binning, partial, scale_exp: int):
+    """Summed shard partials -> (full[nb], regions[n_jk, nb]) as count() returns them."""
+    p = np.ascontiguousarray(partial, np.int64)
+    if p.size != (1 + binning.n_jk) * binning.nb * _capi.PARTIAL_WORDS:
+        raise ValueError("partial has the wrong size for this binning")
+    full = np.empty(binning.nb)
+    reg = np.empty((binning.n_jk, binning.nb))
+    _check(_capi.lib().tpcf_shard_combine(binning._h, _ptr(p), int(scale_exp), _ptr(full), _ptr(reg)))
+    return full, reg
+
+
+def count_sharded(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, precision: int = FP32_GUARD,
+                  weights: Weights | None = None, group=None):
+    """One count split over the ranks of a torch.distributed process group,
+    one GPU per rank: each rank runs its shard and one all-reduce (SUM over
+    int64 limbs) adds the partial sums, so every rank returns exactly what
+    count() returns.  Returns (full, regions, stats of this rank's shard)."""
+    import torch
+    import torch.distributed as dist
+    if not (dist.is_available() and dist.is_initialized()):
+        partial, se, st = count_shard(ctx, a, b, binning, 0, 1, precision, weights)
+        return (*shard_combine(binning, partial, se), st)
+    rank, world = dist.get_rank(group), dist.get_world_size(group)
+    partial, se, st = count_shard(ctx, a, b, binning, rank, world, precision, weights)
+    on_gpu = dist.get_backend(group) == "nccl"
+    dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
+    t = torch.from_numpy(partial).to(dev)
+    chk = torch.tensor([se, -se], dtype=torch.int64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    dist.all_reduce(chk, op=dist.ReduceOp.MAX, group=group)
+    if int(chk[0]) != se or -int(chk[1]) != se:
+        raise TpcfError(_capi.TPCF_E_INVALID_ARG, "shards disagree on the fixed-point scale: different inputs per rank")
+    full, reg = shard_combine(binning, t.cpu().numpy(), se)
+    return full, reg, st
 
 
 def upweight_eval(weights: Weights, values) -> np.ndarray:

@@ -69,6 +69,9 @@ _PROTOTYPES = {
     "tpcf_binning_thresholds": (C.c_int, [_vp, C.c_int, _vp, C.c_int]),
     "tpcf_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_count_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_count_shard": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int32, C.c_int32, _vp,
+                                   C.POINTER(C.c_int32), C.POINTER(Stats)]),
+    "tpcf_shard_combine": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),
     "tpcf_count_weighted": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(WeightSpec), C.c_int, _vp, _vp,
                                       C.POINTER(Stats)]),
     "tpcf_pair_count_weighted": (C.c_int, [_vp, _vp, _vp, _vp, C.POINTER(WeightSpec), C.c_int, _vp, _vp,
@@ -117,6 +120,7 @@ _PROTOTYPES = {
 }
 
 CARTESIAN, EQUATORIAL = 0, 1
+PARTIAL_WORDS = 7
 
 _LIB = None
 

@@ -56,7 +56,7 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         obj = os.path.join(BUILD_DIR, f + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
-            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off",
+            cmd = [NVCC, *ARCH, "-lineinfo", "-O3", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-fopenmp",
                    "-I", CSRC, "-c", src, "-o", obj]
             if ptxas_info:
                 cmd.insert(1, "-Xptxas=-v")

@@ -443,10 +443,16 @@ int prepare_weights(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b,
     return TPCF_OK;
 }
 
+struct ShardArgs {
+    int shard = 0, n_shards = 1;
+    int64_t *partial = nullptr;
+    int32_t *scale_exp = nullptr;
+};
+
 int count_impl(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                const tpcf_weight_spec *spec, int precision, double *full_out, double *region_out, tpcf_stats *stats,
-               bool noalloc) {
-    if (!ctx || !a || !bin || !full_out) return TPCF_E_INVALID_ARG;
+               bool noalloc, const ShardArgs &sh = ShardArgs()) {
+    if (!ctx || !a || !bin || (!full_out && !sh.partial)) return TPCF_E_INVALID_ARG;
     if (precision != TPCF_FP32_GUARD && precision != TPCF_FP64) return fail(ctx, TPCF_E_INVALID_ARG, "bad precision");
     if (a->c.n_jk != bin->b.n_jk || (b && b->c.n_jk != bin->b.n_jk))
         return fail(ctx, TPCF_E_INVALID_ARG, "catalogue and binning disagree on n_jk_regions");
@@ -467,11 +473,18 @@ int count_impl(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, cons
     const bool all_points = bin->b.mode == TPCF_ANGULAR && req.weighting == TPCF_WEIGHTS_PLAIN;
     auto used = [&](const tpcf_catalog *c) { return all_points ? c->c.n_all : (int64_t)c->c.n_kept; };
     if (used(a) == 0 || (b && used(b) == 0)) {
-        std::memset(full_out, 0, sizeof(double) * nb);
+        if (full_out) std::memset(full_out, 0, sizeof(double) * nb);
         if (region_out) std::memset(region_out, 0, sizeof(double) * nb * bin->b.n_jk);
+        if (sh.partial)
+            std::memset(sh.partial, 0, sizeof(int64_t) * (size_t)(1 + bin->b.n_jk) * nb * tpcf::kPartialWords);
+        if (sh.scale_exp) *sh.scale_exp = 0;
         if (stats) std::memset(stats, 0, sizeof(*stats));
         return TPCF_OK;
     }
+    req.shard = sh.shard;
+    req.n_shards = sh.n_shards;
+    req.raw_out = reinterpret_cast<long long *>(sh.partial);
+    req.scale_exp_out = reinterpret_cast<int *>(sh.scale_exp);
     tpcf::Stats st;
     tpcf::Error err{0, ""};
     rc = noalloc ? tpcf::run_count_static(&ctx->c, req, full_out, region_out, &st, &err)
@@ -513,6 +526,30 @@ extern "C" {
 int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                int precision, double *full_out, double *region_out, tpcf_stats *stats) {
     return count_impl(ctx, a, b, bin, nullptr, precision, full_out, region_out, stats, false);
+}
+
+int tpcf_count_shard(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
+                     const tpcf_weight_spec *spec, int precision, int32_t shard, int32_t n_shards, int64_t *partial,
+                     int32_t *scale_exp, tpcf_stats *stats) {
+    if (!ctx || !partial || !scale_exp) return TPCF_E_INVALID_ARG;
+    if (n_shards < 1 || shard < 0 || shard >= n_shards) return fail(ctx, TPCF_E_INVALID_ARG, "bad shard index");
+    ShardArgs sh;
+    sh.shard = shard;
+    sh.n_shards = n_shards;
+    sh.partial = partial;
+    sh.scale_exp = scale_exp;
+    return count_impl(ctx, a, b, bin, spec, precision, nullptr, nullptr, stats, false, sh);
+}
+
+int tpcf_shard_combine(const tpcf_binning *bin, const int64_t *partial, int32_t scale_exp, double *full_out,
+                       double *region_out) {
+    if (!bin || !partial || !full_out || scale_exp < -100 || scale_exp > 100) return TPCF_E_INVALID_ARG;
+    const int nb = bin->b.nb, nj = bin->b.n_jk;
+    std::vector<double> v((size_t)(1 + nj) * nb);
+    tpcf::partial_to_double(reinterpret_cast<const long long *>(partial), v.size(), scale_exp, v.data());
+    std::copy(v.begin(), v.begin() + nb, full_out);
+    if (region_out) std::copy(v.begin() + nb, v.end(), region_out);
+    return TPCF_OK;
 }
 
 int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,

@@ -249,6 +249,12 @@ struct CountRequest {
     const UpTable *up = nullptr; // 3-D inverse-p counts
     int n_runs = 0;              // Params::n_bitwise_runs
     bool dither = false;         // _USE_DITHER_WEIGHTS: popc(dither masks) in place of n_runs
+    // one shard of a count split across processes: the work items k with
+    // k % n_shards == shard; with raw_out set, the fixed-point sums are
+    // returned as limbs (kPartialWords per slot) instead of doubles
+    int shard = 0, n_shards = 1;
+    long long *raw_out = nullptr;
+    int *scale_exp_out = nullptr;
     int refinement = 0;
     // adjoint of a plain-weight 3-D count: with adj_G = dL/d(raw full
     // histogram) set, the count writes per-point dL/dw into grad_a (n_all of
@@ -261,6 +267,12 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
 // one static device array of kStaticScratchBytes, and the catalogues' cell
 // grids must already be cached.
 constexpr size_t kStaticScratchBytes = size_t(32) << 20;
+// Words per histogram slot of a shard's partial sums: the 128-bit
+// two's-complement fixed-point sum as four 32-bit limbs (least significant
+// first), then the numbers of NaN, +inf and -inf pair weights met.
+constexpr int kPartialWords = 7;
+// Partial sums (already added over shards) to the doubles of a count.
+void partial_to_double(const long long *partial, size_t slots, int scale_exp, double *out);
 int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st,
                      Error *err);
 

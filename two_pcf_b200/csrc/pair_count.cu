@@ -1233,7 +1233,9 @@ namespace {
 // a work item's A points times the B points of all its segments.
 long long max_item_pairs(const std::vector<WorkItem> &items, const std::vector<Segment> &segs) {
     long long pmax = 1;
-    for (const WorkItem &w : items) {
+#pragma omp parallel for schedule(static) reduction(max : pmax)
+    for (long long q = 0; q < (long long)items.size(); ++q) {
+        const WorkItem &w = items[q];
         long long bl = 0;
         for (int k = w.seg_begin; k < w.seg_end; ++k) bl += segs[k].b_len;
         pmax = std::max(pmax, (long long)w.a_len * bl);
@@ -1270,6 +1272,8 @@ struct CountPlan {
     const double *adj_G_host = nullptr;
     double *grad_a_host = nullptr, *grad_b_host = nullptr;
     double inv = 1.0;  // 2^-S
+    int scale_exp = 0;  // S
+    long long *raw_out = nullptr;  // partial sums of a shard (kPartialWords per slot)
     std::vector<WorkItem> items;
     std::vector<Segment> segs;
     std::vector<JobK> jobs;  // one for a single count
@@ -1464,7 +1468,18 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
         wscale = std::ldexp(1.0f, S);
         C.inv = std::ldexp(1.0, -S);
+        C.scale_exp = S;
     }
+    if (req.n_shards > 1) {
+        // This shard's items, dealt round-robin from the largest down; the
+        // scale above came from the whole list, so every shard adds in the
+        // same fixed point.
+        std::vector<WorkItem> mine;
+        mine.reserve(C.items.size() / req.n_shards + 1);
+        for (size_t k = (size_t)req.shard; k < C.items.size(); k += (size_t)req.n_shards) mine.push_back(C.items[k]);
+        C.items.swap(mine);
+    }
+    C.raw_out = req.raw_out;
     C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk, C.adj);
     if (C.L.total + 1024 > ctx->smem_optin) {
         err->status = 6;
@@ -1607,6 +1622,37 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
         }
         return 0;
     }
+    if (C.raw_out) {
+        // Partial sums of a shard: limbs of the 128-bit sums and the
+        // non-finite markers as counts, slot by slot (full, then regions).
+        const size_t slots = (size_t)(1 + n_jk) * nb;
+        auto put = [&](size_t slot, const unsigned long long *w, unsigned f) {
+            long long *o = C.raw_out + slot * kPartialWords;
+            o[0] = (long long)(w[0] & 0xffffffffull);
+            o[1] = (long long)(w[0] >> 32);
+            o[2] = (long long)(w[1] & 0xffffffffull);
+            o[3] = (long long)(w[1] >> 32);
+            o[4] = (f & 1u) ? 1 : 0;
+            o[5] = (f & 2u) ? 1 : 0;
+            o[6] = (f & 4u) ? 1 : 0;
+        };
+        for (size_t slot = 0; slot < slots; ++slot) {
+            const bool full = slot < (size_t)nb;
+            const size_t b = full ? slot : (C.jk ? slot - nb : (slot - nb) % nb);
+            const unsigned long long *w = (full || !C.jk) ? &hf[2 * b] : &hs[2 * b];
+            const unsigned f = hflags.empty() ? 0u : hflags[(full || !C.jk) ? b : nb + b];
+            put(slot, w, f);
+        }
+        if (st) {
+            st->candidates += hc[0];
+            st->in_range += hc[1];
+            st->guard += hc[2];
+            st->overflow += hc[3];
+            st->items += C.items.size();
+            st->ms_kernel += ms;
+        }
+        return 0;
+    }
     // A bin that met a non-finite pair weight holds what double
     // accumulation would: NaN, or an infinity of one sign.  The NaN is the
     // one x86 arithmetic generates for 0/0 and inf - inf (sign bit set),
@@ -1645,9 +1691,27 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
 
 }  // namespace
 
+void partial_to_double(const long long *partial, size_t slots, int scale_exp, double *out) {
+    const double inv = std::ldexp(1.0, -scale_exp);
+    for (size_t s = 0; s < slots; ++s) {
+        const long long *q = partial + s * kPartialWords;
+        // sum of limbs * 2^(32 k), wrapped to 128 bits like the device sums
+        unsigned __int128 u = 0;
+        for (int k = 3; k >= 0; --k) u = (u << 32) + (unsigned __int128)(__int128)q[k];
+        const unsigned long long w[2] = {(unsigned long long)u, (unsigned long long)(u >> 64)};
+        double v = fixed_to_double(w, inv);
+        const bool nan = q[4] > 0 || (q[5] > 0 && q[6] > 0);
+        if (nan) v = std::copysign(std::numeric_limits<double>::quiet_NaN(), -1.0);
+        else if (q[5] > 0) v = std::numeric_limits<double>::infinity();
+        else if (q[6] > 0) v = -std::numeric_limits<double>::infinity();
+        out[s] = v;
+    }
+}
+
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
     CountPlan C;
     if (plan_count(ctx, req, true, C, err)) return err->status;
+    if (req.scale_exp_out) *req.scale_exp_out = C.scale_exp;
     const Binning *bin = req.bin;
     ScratchBuf<WorkItem> d_items;
     ScratchBuf<Segment> d_segs;

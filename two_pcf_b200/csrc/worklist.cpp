@@ -75,6 +75,7 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
             }
     struct Part {
         std::vector<WorkItem> items;
+        std::vector<long long> cost;  // A points x B points of each item
         std::vector<Segment> segs;
     };
     int nthreads = 1;
@@ -142,6 +143,7 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
                         if (bl > 0 && bl + sg.b_len > kItemMaxB) {
                             w.seg_end = (int)pt.segs.size();
                             pt.items.push_back(w);
+                            pt.cost.push_back((long long)w.a_len * bl);
                             w.seg_begin = (int)pt.segs.size();
                             bl = 0;
                         }
@@ -150,41 +152,44 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
                     }
                     w.seg_end = (int)pt.segs.size();
                     pt.items.push_back(w);
+                    pt.cost.push_back((long long)w.a_len * bl);
                 }
             }
         }
     }
-    items.clear();
-    segs.clear();
-    size_t ni = 0, ns = 0;
-    for (const Part &pt : parts) {
-        ni += pt.items.size();
-        ns += pt.segs.size();
+    // Concatenate the parts in block order (in parallel: prefix offsets, then
+    // each part copies itself into place).
+    std::vector<size_t> io(nblk + 1, 0), so(nblk + 1, 0);
+    for (int k = 0; k < nblk; ++k) {
+        io[k + 1] = io[k] + parts[k].items.size();
+        so[k + 1] = so[k] + parts[k].segs.size();
     }
-    items.reserve(ni);
-    segs.reserve(ns);
-    std::vector<std::pair<long long, int>> cost;  // (cost, item)
-    cost.reserve(ni);
-    for (Part &pt : parts) {
-        const int off = (int)segs.size();
-        for (WorkItem w : pt.items) {
-            long long bl = 0;
-            for (int k = w.seg_begin; k < w.seg_end; ++k) bl += pt.segs[k].b_len;
+    const size_t ni = io[nblk];
+    std::vector<WorkItem> all(ni);
+    std::vector<std::pair<long long, int>> cost(ni);  // (cost, item)
+    segs.resize(so[nblk]);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int k = 0; k < nblk; ++k) {
+        Part &pt = parts[k];
+        const int off = (int)so[k];
+        for (size_t q = 0; q < pt.items.size(); ++q) {
+            WorkItem w = pt.items[q];
             w.seg_begin += off;
             w.seg_end += off;
-            cost.push_back({(long long)w.a_len * bl, (int)items.size()});
-            items.push_back(w);
+            all[io[k] + q] = w;
+            cost[io[k] + q] = {pt.cost[q], (int)(io[k] + q)};
         }
-        segs.insert(segs.end(), pt.segs.begin(), pt.segs.end());
+        if (!pt.segs.empty()) std::memcpy(segs.data() + so[k], pt.segs.data(), sizeof(Segment) * pt.segs.size());
+        std::vector<Segment>().swap(pt.segs);
     }
     // Largest items first, so the dynamic queue ends balanced.
     std::stable_sort(cost.begin(), cost.end(),
                      [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
                          return x.first > y.first;
                      });
-    std::vector<WorkItem> sorted(items.size());
-    for (size_t k = 0; k < cost.size(); ++k) sorted[k] = items[cost[k].second];
-    items.swap(sorted);
+    items.resize(ni);
+#pragma omp parallel for schedule(static)
+    for (long long k = 0; k < (long long)ni; ++k) items[k] = all[cost[k].second];
 }
 
 }  // namespace tpcf
