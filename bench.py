@@ -184,17 +184,18 @@ def count_step(tp, ctx, D, R, bins, precision, release=True, sharded=False):
     kms = 0.0
     flops = 0.0
     hists = []
-    for mode, b in bins:
-        for a, bb in ((D, None), (D, R), (R, None)):
-            if sharded:
-                full, reg, st = tp.count_sharded(ctx, a, bb, b, precision)
-            else:
-                full, reg, st = tp.count(ctx, a, bb, b, precision)
-            in_range += st["in_range"]
-            cand += st["candidates"]
-            kms += st["ms_kernel"]
-            flops += 8.0 * st["candidates"] + F_MODE[mode] * st["in_range"]
-            hists.append((full, reg))
+    jobs = [(mode, a, bb, b) for mode, b in bins for a, bb in ((D, None), (D, R), (R, None))]
+    if sharded:
+        results = [tp.count_sharded(ctx, a, bb, b, precision) for _, a, bb, b in jobs]
+    else:
+        # one call: each count's host planning overlaps the previous kernel
+        results = tp.count_many(ctx, [(a, bb, b) for _, a, bb, b in jobs], precision)
+    for (mode, _, _, _), (full, reg, st) in zip(jobs, results):
+        in_range += st["in_range"]
+        cand += st["candidates"]
+        kms += st["ms_kernel"]
+        flops += 8.0 * st["candidates"] + F_MODE[mode] * st["in_range"]
+        hists.append((full, reg))
     return in_range, cand, kms, flops, hists
 
 

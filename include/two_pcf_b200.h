@@ -284,6 +284,27 @@ int tpcf_upweight_eval(const tpcf_weight_spec *spec, const double *values, int64
 int tpcf_count_noalloc(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                        int precision, double *full_out, double *region_out, tpcf_stats *stats);
 
+/* Several counts in one call (no counterpart in the reference, whose driver
+ * runs DD, DR and RR one after another): the results are those of one
+ * tpcf_count_weighted per job, in order (reference_form: those of
+ * tpcf_pair_count_weighted — inverted regions, auto counts doubled).  Every
+ * cell grid is built first; then each count's host work (work list, tables,
+ * staging through pinned memory) runs while the previous count's kernel is
+ * on the device, so the host work leaves the critical path.  stats->ms_total
+ * is the wall time of the whole call. */
+typedef struct {
+    const tpcf_catalog *a;
+    const tpcf_catalog *b;          /* NULL: auto count of a */
+    const tpcf_binning *bin;
+    const tpcf_weight_spec *spec;   /* NULL: TPCF_WEIGHTS_PLAIN */
+    int32_t precision;
+    int32_t reference_form;
+    double *full_out;               /* nb */
+    double *region_out;             /* n_jk * nb, or NULL (required with reference_form) */
+    tpcf_stats *stats;              /* or NULL */
+} tpcf_count_job;
+int tpcf_count_many(tpcf_ctx *ctx, const tpcf_count_job *jobs, int32_t n_jobs);
+
 /* One shard of a count split across processes or GPUs (strong scaling; no
  * counterpart in the reference, whose counts run on one node's threads).
  * Every shard plans the same work list (it depends only on the catalogues,

@@ -36,7 +36,8 @@ __all__ = ["Context", "Catalog", "Binning", "TpcfError", "Weights", "count", "au
            "normalise_cross",
            "ls_estimator", "MONOPOLE", "SIGMA_PI", "S_MU", "ANGULAR", "FP32_GUARD", "FP64", "WEIGHTS_PLAIN",
            "WEIGHTS_INVP_DD", "WEIGHTS_INVP_DR", "WEIGHTS_INVP_DD_DITHER", "LOS_ANGULAR", "LOS_MIDPOINT", "iip_weights",
-           "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE", "count_shard", "shard_combine", "count_sharded"]
+           "Batch", "BATCH_DD", "BATCH_DR", "BATCH_AUTOTUNE", "count_shard", "shard_combine", "count_sharded",
+           "count_many"]
 
 
 class TpcfError(RuntimeError):
@@ -300,6 +301,29 @@ def iip_weights(bitmask, weight, n_bitwise_runs: int, dither_mask=None):
     iw = np.empty(n, np.float32)
     _check(_capi.lib().tpcf_iip_weights(n, m.shape[1], _ptr(m), _ptr(d), int(n_bitwise_runs), _ptr(w), _ptr(iw)))
     return w, iw
+
+
+def count_many(ctx: Context, jobs, precision: int = FP32_GUARD, reference_form: bool = False):
+    """Several counts in one call (tpcf_count_many): jobs is a list of
+    (a, b or None, binning) or (a, b, binning, weights).  Results as one
+    count() (reference_form: auto_/cross_pair_count) per job, in order; each
+    count's host work overlaps the previous count's kernel.  Returns a list of
+    (full, regions, stats)."""
+    outs = []
+    arr = (_capi.CountJob * max(1, len(jobs)))()
+    for k, job in enumerate(jobs):
+        a, b, binning = job[0], job[1], job[2]
+        weights = job[3] if len(job) > 3 else None
+        full = np.zeros(binning.nb)
+        reg = np.zeros((binning.n_jk, binning.nb))
+        st = Stats()
+        outs.append((full, reg, st, weights))
+        arr[k] = _capi.CountJob(a._h, b._h if b is not None else None, binning._h,
+                                C.cast(C.pointer(weights.spec), C.c_void_p) if weights is not None else None,
+                                int(precision), int(bool(reference_form)), _ptr(full), _ptr(reg),
+                                C.cast(C.pointer(st), C.c_void_p))
+    _check(_capi.lib().tpcf_count_many(ctx._h, arr, len(jobs)), ctx)
+    return [(f, r, st.as_dict()) for f, r, st, _ in outs]
 
 
 def count_shard(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, shard: int, n_shards: int,

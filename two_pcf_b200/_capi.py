@@ -46,6 +46,12 @@ class WeightSpec(C.Structure):
                 ("up_numerator", C.c_void_p), ("up_denominator", C.c_void_p)]
 
 
+class CountJob(C.Structure):
+    _fields_ = [("a", C.c_void_p), ("b", C.c_void_p), ("bin", C.c_void_p), ("spec", C.c_void_p),
+                ("precision", C.c_int32), ("reference_form", C.c_int32), ("full_out", C.c_void_p),
+                ("region_out", C.c_void_p), ("stats", C.c_void_p)]
+
+
 # Every symbol the header declares, with (restype, argtypes).
 _vp = C.c_void_p
 _PROTOTYPES = {
@@ -69,6 +75,7 @@ _PROTOTYPES = {
     "tpcf_binning_thresholds": (C.c_int, [_vp, C.c_int, _vp, C.c_int]),
     "tpcf_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_count_noalloc": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
+    "tpcf_count_many": (C.c_int, [_vp, _vp, C.c_int32]),
     "tpcf_count_shard": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int, C.c_int32, C.c_int32, _vp,
                                    C.POINTER(C.c_int32), C.POINTER(Stats)]),
     "tpcf_shard_combine": (C.c_int, [_vp, _vp, C.c_int32, _vp, _vp]),

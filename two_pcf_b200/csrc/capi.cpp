@@ -109,6 +109,8 @@ int tpcf_destroy(tpcf_ctx *ctx) {
     if (!ctx) return TPCF_E_INVALID_ARG;
     cudaSetDevice(ctx->c.device);
     if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
+    for (unsigned char *p : ctx->c.pinned)
+        if (p) cudaFreeHost(p);
     if (ctx->c.pool) cudaMemPoolDestroy(ctx->c.pool);
     if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
@@ -526,6 +528,78 @@ extern "C" {
 int tpcf_count(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                int precision, double *full_out, double *region_out, tpcf_stats *stats) {
     return count_impl(ctx, a, b, bin, nullptr, precision, full_out, region_out, stats, false);
+}
+
+int tpcf_count_many(tpcf_ctx *ctx, const tpcf_count_job *jobs, int32_t n_jobs) {
+    if (!ctx || n_jobs < 0 || (n_jobs > 0 && !jobs)) return TPCF_E_INVALID_ARG;
+    std::vector<tpcf::CountRequest> reqs;
+    std::vector<tpcf::CountOut> outs;
+    std::vector<tpcf::UpTable> ups(n_jobs);
+    std::vector<tpcf::Stats> sts(n_jobs);
+    std::vector<int> run;  // jobs that reach the device
+    for (int k = 0; k < n_jobs; ++k) {
+        const tpcf_count_job &J = jobs[k];
+        if (!J.a || !J.bin || !J.full_out) return fail(ctx, TPCF_E_INVALID_ARG, "job " + std::to_string(k) + ": NULL argument");
+        if (J.reference_form && !J.region_out)
+            return fail(ctx, TPCF_E_INVALID_ARG, "job " + std::to_string(k) + ": reference_form needs region_out");
+        if (J.precision != TPCF_FP32_GUARD && J.precision != TPCF_FP64)
+            return fail(ctx, TPCF_E_INVALID_ARG, "job " + std::to_string(k) + ": bad precision");
+        if (J.a->c.n_jk != J.bin->b.n_jk || (J.b && J.b->c.n_jk != J.bin->b.n_jk))
+            return fail(ctx, TPCF_E_INVALID_ARG, "job " + std::to_string(k) + ": catalogue and binning disagree on n_jk_regions");
+        tpcf::CountRequest req;
+        int rc = prepare_weights(ctx, J.a, J.b, J.bin, J.spec, req, ups[k]);
+        if (rc) return rc;
+        req.a = &J.a->c;
+        req.b = J.b ? &J.b->c : nullptr;
+        req.bin = &J.bin->b;
+        req.exact_fp64 = J.precision == TPCF_FP64 || J.bin->b.los_midpoint;
+        const int nb = J.bin->b.nb;
+        const bool all_points = J.bin->b.mode == TPCF_ANGULAR && req.weighting == TPCF_WEIGHTS_PLAIN;
+        auto used = [&](const tpcf_catalog *c) { return all_points ? c->c.n_all : (int64_t)c->c.n_kept; };
+        if (used(J.a) == 0 || (J.b && used(J.b) == 0)) {
+            std::memset(J.full_out, 0, sizeof(double) * nb);
+            if (J.region_out) std::memset(J.region_out, 0, sizeof(double) * nb * J.bin->b.n_jk);
+            if (J.stats) std::memset(J.stats, 0, sizeof(*J.stats));
+            continue;
+        }
+        if (req.up) req.up = &ups[k];
+        reqs.push_back(req);
+        tpcf::CountOut o;
+        o.full = J.full_out;
+        o.region = J.region_out;
+        o.st = &sts[k];
+        outs.push_back(o);
+        run.push_back(k);
+    }
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    auto t0 = std::chrono::steady_clock::now();
+    tpcf::Error err{0, ""};
+    if (!reqs.empty() && tpcf::run_count_many(&ctx->c, reqs, outs, &err)) return fail(ctx, err.status, err.msg);
+    const double ms_total = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    for (int k : run) {
+        const tpcf_count_job &J = jobs[k];
+        if (J.stats) {
+            const tpcf::Stats &st = sts[k];
+            J.stats->candidates = st.candidates;
+            J.stats->in_range = st.in_range;
+            J.stats->guard_evals = st.guard;
+            J.stats->overflow_updates = st.overflow;
+            J.stats->work_items = st.items;
+            J.stats->ms_kernel = st.ms_kernel;
+            J.stats->ms_total = ms_total;
+        }
+        if (J.reference_form) {
+            const int nb = J.bin->b.nb, nj = J.bin->b.n_jk;
+            for (int r = 0; r < nj; ++r)
+                for (int q = 0; q < nb; ++q) J.region_out[(size_t)r * nb + q] = J.full_out[q] - J.region_out[(size_t)r * nb + q];
+            if (!J.b) {
+                for (int q = 0; q < nb; ++q) J.full_out[q] *= 2.0;
+                for (size_t q = 0; q < (size_t)nb * nj; ++q) J.region_out[q] *= 2.0;
+            }
+        }
+    }
+    return TPCF_OK;
 }
 
 int tpcf_count_shard(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,

@@ -104,19 +104,26 @@ bool correlate(tpcf_ctx *ctx, const char *what, int mode, const tpcf_axis_spec &
         sub[k].assign((size_t)n_jk * nb, 0.0);
     }
     tpcf_stats st[3];
-    log("%s: DD", what);
-    rc = tpcf_pair_count_weighted(ctx, data, nullptr, b, dd_spec, precision, full[0].data(), sub[0].data(), &st[0]);
+    // DD, DR and RR in one call: each count's host planning overlaps the
+    // previous count's kernel
+    log("%s: DD, DR, RR", what);
+    tpcf_count_job jobs[3];
+    const tpcf_catalog *ja[3] = {data, data, rand}, *jb[3] = {nullptr, rand, nullptr};
+    const tpcf_weight_spec *js[3] = {dd_spec, dr_spec, nullptr};
+    for (int k = 0; k < 3; ++k) {
+        jobs[k].a = ja[k];
+        jobs[k].b = jb[k];
+        jobs[k].bin = b;
+        jobs[k].spec = js[k];
+        jobs[k].precision = precision;
+        jobs[k].reference_form = 1;
+        jobs[k].full_out = full[k].data();
+        jobs[k].region_out = sub[k].data();
+        jobs[k].stats = &st[k];
+    }
+    rc = tpcf_count_many(ctx, jobs, 3);
     if (!rc) rc = tpcf_normalise_auto(data, nb, full[0].data(), sub[0].data());
-    if (!rc) {
-        log("%s: DR", what);
-        rc = tpcf_pair_count_weighted(ctx, data, rand, b, dr_spec, precision, full[1].data(), sub[1].data(),
-                                      &st[1]);
-    }
     if (!rc) rc = tpcf_normalise_cross(data, rand, nb, full[1].data(), sub[1].data());
-    if (!rc) {
-        log("%s: RR", what);
-        rc = tpcf_auto_pair_count(ctx, rand, b, precision, full[2].data(), sub[2].data(), &st[2]);
-    }
     if (!rc) rc = tpcf_normalise_auto(rand, nb, full[2].data(), sub[2].data());
     if (rc) return e.set(rc, std::string(what) + ": " + tpcf_last_error(ctx));
     log("%s: %.3e + %.3e + %.3e pairs in range, kernels %.1f + %.1f + %.1f ms", what, (double)st[0].in_range,

@@ -52,6 +52,10 @@ struct Ctx {
     int refinement = 0;  // 0 = automatic
     unsigned long long launches = 0;  // kernels launched by this context
     cudaMemPool_t pool = nullptr;     // stream-ordered pool for the scratch of each call
+    // pinned staging of the counts in flight in count_many (two slots, grown
+    // on demand, freed with the context)
+    unsigned char *pinned[2] = {nullptr, nullptr};
+    size_t pinned_cap[2] = {0, 0};
 };
 
 // Device scratch of one call, from the context's stream-ordered memory pool:
@@ -263,6 +267,14 @@ struct CountRequest {
     double *grad_a = nullptr, *grad_b = nullptr;
 };
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err);
+// Several counts, results identical to run_count on each in order: every
+// grid is built first, then each count's host planning (work list, tables)
+// runs while the previous count's kernel is on the device.
+struct CountOut {
+    double *full = nullptr, *region = nullptr;
+    Stats *st = nullptr;
+};
+int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs, const std::vector<CountOut> &outs, Error *err);
 // run_count without device allocation: every scratch buffer is carved from
 // one static device array of kStaticScratchBytes, and the catalogues' cell
 // grids must already be cached.

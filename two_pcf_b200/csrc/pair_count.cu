@@ -1364,7 +1364,7 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     }
 }
 
-int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Error *err) {
+int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Error *err, bool grids_only = false) {
     const Binning *bin = req.bin;
     Catalog *A = const_cast<Catalog *>(req.a);
     Catalog *B = const_cast<Catalog *>(req.b ? req.b : req.a);
@@ -1454,6 +1454,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
             return err->status;
         }
     }
+    if (grids_only) return 0;
     build_work_items(*ga, *gb, C.is_auto, m, side, rb, C.items, C.segs);
 
     float wscale = 1.0f;
@@ -1510,30 +1511,75 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     return 0;
 }
 
-// Upload the tables and the work list, clear the accumulators, launch, read
-// back, and convert the fixed-point sums; timed: record the kernel's device
-// time in the stats.
-int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, double *region_out, Stats *st,
-            Error *err, bool timed) {
+// Host side of one count in flight: where its uploads are staged and where
+// its results land.  With `stage` set (pinned memory, a count of
+// count_many), every copy is asynchronous and the host can plan the next
+// count while this one runs; otherwise the plan's vectors are uploaded
+// directly and the results land in `own` (pageable).
+struct HostIO {
+    unsigned char *stage = nullptr;  // pinned: uploads, then results
+    size_t stage_cap = 0;
+    std::vector<unsigned long long> own;
+    unsigned long long *hf = nullptr, *hs = nullptr, *hc = nullptr;
+    int *herr = nullptr;
+    unsigned *hflags = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr, done = nullptr;
+    ~HostIO() {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        if (done) cudaEventDestroy(done);
+    }
+};
+
+// Bytes of pinned staging a count needs (uploads and results).
+size_t stage_bytes(const CountPlan &C) {
+    auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    const Binning *bin = C.bin;
+    size_t t = 0;
+    t += up16(sizeof(WorkItem) * C.items.size()) + up16(sizeof(Segment) * C.segs.size());
+    t += up16(sizeof(JobK) * C.jobs.size()) + up16(sizeof(float) * bin->t1.size()) + up16(sizeof(float) * bin->t2.size());
+    t += up16(LUT1_N) + up16(LUT2_N);
+    t += 3 * up16(sizeof(double) * C.n_up());
+    if (C.adj) t += up16(sizeof(double) * C.nb);
+    t += up16(sizeof(unsigned long long) * 2 * C.nb) + up16(sizeof(unsigned long long) * 2 * (size_t)C.nb * C.n_jk);
+    t += up16(sizeof(unsigned long long) * 4) + 16 + up16(sizeof(unsigned) * C.n_flags());
+    return t;
+}
+
+// Upload the tables and the work list, clear the accumulators, launch, and
+// queue the read-back of the results; timed: events around the kernel.
+int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Error *err, bool timed) {
     const Binning *bin = C.bin;
     const int nb = C.nb, n_jk = C.n_jk;
     cudaStream_t stm = ctx->stream;
+    size_t off = 0;
+    // host source of an upload: the plan's own memory, or its copy in the
+    // pinned stage
+    auto src = [&](const void *h, size_t bytes) -> const void * {
+        if (!io.stage) return h;
+        unsigned char *d = io.stage + off;
+        if (bytes) std::memcpy(d, h, bytes);
+        off += (bytes + 15) / 16 * 16;
+        return d;
+    };
+    auto h2d = [&](void *dst, const void *h, size_t bytes) -> cudaError_t {
+        const void *s2 = src(h, bytes);
+        return bytes ? cudaMemcpyAsync(dst, s2, bytes, cudaMemcpyHostToDevice, stm) : cudaSuccess;
+    };
     if (!C.items.empty()) {
-        TPCF_TRY(cudaMemcpyAsync(D.items, C.items.data(), sizeof(WorkItem) * C.items.size(), cudaMemcpyHostToDevice,
-                                 stm));
-        TPCF_TRY(cudaMemcpyAsync(D.segs, C.segs.data(), sizeof(Segment) * C.segs.size(), cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(h2d(D.items, C.items.data(), sizeof(WorkItem) * C.items.size()));
+        TPCF_TRY(h2d(D.segs, C.segs.data(), sizeof(Segment) * C.segs.size()));
     }
-    TPCF_TRY(cudaMemcpyAsync(D.jobs, C.jobs.data(), sizeof(JobK) * C.jobs.size(), cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(D.t1, bin->t1.data(), sizeof(float) * bin->t1.size(), cudaMemcpyHostToDevice, stm));
-    if (!bin->t2.empty())
-        TPCF_TRY(cudaMemcpyAsync(D.t2, bin->t2.data(), sizeof(float) * bin->t2.size(), cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(D.l1, C.luts.l1.data(), LUT1_N, cudaMemcpyHostToDevice, stm));
-    TPCF_TRY(cudaMemcpyAsync(D.l2, C.luts.l2.data(), LUT2_N, cudaMemcpyHostToDevice, stm));
+    TPCF_TRY(h2d(D.jobs, C.jobs.data(), sizeof(JobK) * C.jobs.size()));
+    TPCF_TRY(h2d(D.t1, bin->t1.data(), sizeof(float) * bin->t1.size()));
+    if (!bin->t2.empty()) TPCF_TRY(h2d(D.t2, bin->t2.data(), sizeof(float) * bin->t2.size()));
+    TPCF_TRY(h2d(D.l1, C.luts.l1.data(), LUT1_N));
+    TPCF_TRY(h2d(D.l2, C.luts.l2.data(), LUT2_N));
     if (C.up) {
         const size_t k = C.n_up();
-        TPCF_TRY(cudaMemcpyAsync(D.up_thr, C.up->thr.data(), sizeof(float) * k, cudaMemcpyHostToDevice, stm));
-        TPCF_TRY(cudaMemcpyAsync(D.up_bins, C.up->bins.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stm));
-        TPCF_TRY(cudaMemcpyAsync(D.up_centre, C.up->centre.data(), sizeof(double) * k, cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(h2d(D.up_thr, C.up->thr.data(), sizeof(float) * k));
+        TPCF_TRY(h2d(D.up_bins, C.up->bins.data(), sizeof(double) * k));
+        TPCF_TRY(h2d(D.up_centre, C.up->centre.data(), sizeof(double) * k));
     }
     // What the kernel accumulates into starts at zero on every call.
     TPCF_TRY(cudaMemsetAsync(D.full, 0, sizeof(unsigned long long) * 2 * nb, stm));
@@ -1543,7 +1589,7 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     TPCF_TRY(cudaMemsetAsync(D.err, 0, sizeof(int), stm));
     if (C.n_flags()) TPCF_TRY(cudaMemsetAsync(D.flags, 0, sizeof(unsigned) * C.n_flags(), stm));
     if (C.adj) {
-        TPCF_TRY(cudaMemcpyAsync(D.adj_G, C.adj_G_host, sizeof(double) * nb, cudaMemcpyHostToDevice, stm));
+        TPCF_TRY(h2d(D.adj_G, C.adj_G_host, sizeof(double) * nb));
         TPCF_TRY(cudaMemsetAsync(D.grad_a, 0, sizeof(double) * std::max(C.n_a, 1), stm));
         if (!C.is_auto) TPCF_TRY(cudaMemsetAsync(D.grad_b, 0, sizeof(double) * std::max(C.n_b, 1), stm));
     }
@@ -1574,11 +1620,10 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     int per_sm = 1;
     TPCF_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, C.fn, NT, C.L.total));
     per_sm = std::max(per_sm, 1);
-    cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (timed) {
-        TPCF_TRY(cudaEventCreate(&e0));
-        TPCF_TRY(cudaEventCreate(&e1));
-        TPCF_TRY(cudaEventRecord(e0, stm));
+        TPCF_TRY(cudaEventCreate(&io.e0));
+        TPCF_TRY(cudaEventCreate(&io.e1));
+        TPCF_TRY(cudaEventRecord(io.e0, stm));
     }
     if (!C.items.empty()) {
         const int grid = (int)std::min<long long>((long long)ctx->num_sms * per_sm, (long long)C.items.size());
@@ -1586,25 +1631,44 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
         ++ctx->launches;
         TPCF_TRY(cudaGetLastError());
     }
-    if (timed) TPCF_TRY(cudaEventRecord(e1, stm));
-    std::vector<unsigned long long> hf(2 * (size_t)nb), hs(2 * (size_t)nb * n_jk), hc(4);
-    std::vector<unsigned> hflags(C.n_flags());
-    int herr = 0;
-    TPCF_TRY(cudaMemcpyAsync(hf.data(), D.full, sizeof(unsigned long long) * hf.size(), cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hs.data(), D.sub, sizeof(unsigned long long) * hs.size(), cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(hc.data(), D.cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(&herr, D.err, sizeof(int), cudaMemcpyDeviceToHost, stm));
-    if (!hflags.empty())
-        TPCF_TRY(cudaMemcpyAsync(hflags.data(), D.flags, sizeof(unsigned) * hflags.size(), cudaMemcpyDeviceToHost,
-                                 stm));
-    TPCF_TRY(cudaStreamSynchronize(stm));
-    float ms = 0;
-    if (timed) {
-        cudaEventElapsedTime(&ms, e0, e1);
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
+    if (timed) TPCF_TRY(cudaEventRecord(io.e1, stm));
+    // results: into the pinned stage after the uploads, or into `own`
+    const size_t n_hf = 2 * (size_t)nb, n_hs = 2 * (size_t)nb * n_jk, n_fl = C.n_flags();
+    unsigned char *r = nullptr;
+    if (io.stage) {
+        r = io.stage + off;
+    } else {
+        io.own.assign(n_hf + n_hs + 4 + 1 + (n_fl + 1) / 2, 0ull);
+        r = reinterpret_cast<unsigned char *>(io.own.data());
     }
-    if (herr) {
+    io.hf = reinterpret_cast<unsigned long long *>(r);
+    io.hs = io.hf + n_hf;
+    io.hc = io.hs + n_hs;
+    io.herr = reinterpret_cast<int *>(io.hc + 4);
+    io.hflags = reinterpret_cast<unsigned *>(io.hc + 5);
+    TPCF_TRY(cudaMemcpyAsync(io.hf, D.full, sizeof(unsigned long long) * n_hf, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(io.hs, D.sub, sizeof(unsigned long long) * n_hs, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(io.hc, D.cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(io.herr, D.err, sizeof(int), cudaMemcpyDeviceToHost, stm));
+    if (n_fl) TPCF_TRY(cudaMemcpyAsync(io.hflags, D.flags, sizeof(unsigned) * n_fl, cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaEventCreateWithFlags(&io.done, cudaEventDisableTiming));
+    TPCF_TRY(cudaEventRecord(io.done, stm));
+    return 0;
+}
+
+// Wait for a launched count and convert its fixed-point sums (or hand back
+// the shard's partial sums, or the adjoint's gradients).
+int finish_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, double *full_out, double *region_out,
+                 Stats *st, Error *err, bool timed) {
+    (void)ctx;
+    const int nb = C.nb, n_jk = C.n_jk;
+    TPCF_TRY(cudaEventSynchronize(io.done));
+    float ms = 0;
+    if (timed) cudaEventElapsedTime(&ms, io.e0, io.e1);
+    const unsigned long long *hf = io.hf, *hs = io.hs, *hc = io.hc;
+    const bool has_flags = C.n_flags() > 0;
+    const unsigned *hflags = io.hflags;
+    if (*io.herr) {
         err->status = 4;
         err->msg = "device wait exceeded its iteration limit; results discarded";
         return err->status;
@@ -1640,7 +1704,7 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
             const bool full = slot < (size_t)nb;
             const size_t b = full ? slot : (C.jk ? slot - nb : (slot - nb) % nb);
             const unsigned long long *w = (full || !C.jk) ? &hf[2 * b] : &hs[2 * b];
-            const unsigned f = hflags.empty() ? 0u : hflags[(full || !C.jk) ? b : nb + b];
+            const unsigned f = has_flags ? hflags[(full || !C.jk) ? b : nb + b] : 0u;
             put(slot, w, f);
         }
         if (st) {
@@ -1666,13 +1730,13 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
     };
     for (int b = 0; b < nb; ++b) {
         full_out[b] = fixed_to_double(&hf[2 * (size_t)b], C.inv);
-        if (!hflags.empty()) full_out[b] = flagged(hflags[b], full_out[b]);
+        if (has_flags) full_out[b] = flagged(hflags[b], full_out[b]);
     }
     if (region_out) {
         if (C.jk) {
             for (size_t k = 0; k < (size_t)nb * n_jk; ++k) {
                 region_out[k] = fixed_to_double(&hs[2 * k], C.inv);
-                if (!hflags.empty()) region_out[k] = flagged(hflags[nb + k], region_out[k]);
+                if (has_flags) region_out[k] = flagged(hflags[nb + k], region_out[k]);
             }
         } else {
             for (int b = 0; b < nb; ++b) region_out[b] = full_out[b];
@@ -1687,6 +1751,18 @@ int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, dou
         st->ms_kernel += ms;
     }
     return 0;
+}
+
+// One count from upload to results, synchronously, staging through the
+// C++ heap.
+int execute(Ctx *ctx, CountPlan &C, const CountBuffers &D, double *full_out, double *region_out, Stats *st,
+            Error *err, bool timed) {
+    HostIO io;
+    if (launch_count(ctx, C, D, io, err, timed)) {
+        if (!err->status) err->status = 3;
+        return err->status;
+    }
+    return finish_count(ctx, C, D, io, full_out, region_out, st, err, timed);
 }
 
 }  // namespace
@@ -1708,66 +1784,140 @@ void partial_to_double(const long long *partial, size_t slots, int scale_exp, do
     }
 }
 
+namespace {
+
+// The device scratch of one count, from the context's pool.
+struct CountScratch {
+    ScratchBuf<WorkItem> items;
+    ScratchBuf<Segment> segs;
+    ScratchBuf<unsigned long long> full, sub, cnt;
+    ScratchBuf<int> head, err;
+    ScratchBuf<float> t1, t2, up_thr;
+    ScratchBuf<unsigned char> l1, l2;
+    ScratchBuf<unsigned> flags;
+    ScratchBuf<double> up_bins, up_centre;
+    ScratchBuf<JobK> jobs;
+    ScratchBuf<double> adj_G, grad_a, grad_b;
+    CountBuffers D;
+};
+
+int alloc_scratch(Ctx *ctx, const CountPlan &C, CountScratch &S, Error *err) {
+    const Binning *bin = C.bin;
+    const Ctx &X = *ctx;
+    TPCF_TRY(S.items.alloc(X, C.items.size()));
+    TPCF_TRY(S.segs.alloc(X, C.segs.size()));
+    TPCF_TRY(S.full.alloc(X, 2 * (size_t)C.nb));
+    TPCF_TRY(S.sub.alloc(X, 2 * (size_t)C.nb * C.n_jk));
+    TPCF_TRY(S.cnt.alloc(X, 4));
+    TPCF_TRY(S.head.alloc(X, 1));
+    TPCF_TRY(S.err.alloc(X, 1));
+    TPCF_TRY(S.t1.alloc(X, bin->t1.size()));
+    TPCF_TRY(S.t2.alloc(X, std::max<size_t>(bin->t2.size(), 1)));
+    TPCF_TRY(S.l1.alloc(X, LUT1_N));
+    TPCF_TRY(S.l2.alloc(X, LUT2_N));
+    if (C.n_flags()) TPCF_TRY(S.flags.alloc(X, C.n_flags()));
+    if (C.up) {
+        TPCF_TRY(S.up_thr.alloc(X, C.n_up()));
+        TPCF_TRY(S.up_bins.alloc(X, C.n_up()));
+        TPCF_TRY(S.up_centre.alloc(X, C.n_up()));
+    }
+    TPCF_TRY(S.jobs.alloc(X, C.jobs.size()));
+    if (C.adj) {
+        TPCF_TRY(S.adj_G.alloc(X, C.nb));
+        TPCF_TRY(S.grad_a.alloc(X, std::max(C.n_a, 1)));
+        if (!C.is_auto) TPCF_TRY(S.grad_b.alloc(X, std::max(C.n_b, 1)));
+    }
+    CountBuffers &D = S.D;
+    D.jobs = S.jobs.p;
+    D.adj_G = S.adj_G.p;
+    D.grad_a = S.grad_a.p;
+    D.grad_b = S.grad_b.p;
+    D.items = S.items.p;
+    D.segs = S.segs.p;
+    D.full = S.full.p;
+    D.sub = S.sub.p;
+    D.cnt = S.cnt.p;
+    D.head = S.head.p;
+    D.err = S.err.p;
+    D.t1 = S.t1.p;
+    D.t2 = S.t2.p;
+    D.l1 = S.l1.p;
+    D.l2 = S.l2.p;
+    D.flags = C.n_flags() ? S.flags.p : nullptr;
+    D.up_thr = S.up_thr.p;
+    D.up_bins = S.up_bins.p;
+    D.up_centre = S.up_centre.p;
+    return 0;
+}
+
+// A pinned staging slot of at least `bytes`; the slot's previous count has
+// finished when this is called.
+int pinned_slot(Ctx *ctx, int k, size_t bytes, unsigned char **out, size_t *cap, Error *err) {
+    if (ctx->pinned_cap[k] < bytes) {
+        if (ctx->pinned[k]) cudaFreeHost(ctx->pinned[k]);
+        ctx->pinned[k] = nullptr;
+        ctx->pinned_cap[k] = 0;
+        const size_t want = bytes + bytes / 2 + 4096;
+        TPCF_TRY(cudaHostAlloc((void **)&ctx->pinned[k], want, cudaHostAllocDefault));
+        ctx->pinned_cap[k] = want;
+    }
+    *out = ctx->pinned[k];
+    *cap = ctx->pinned_cap[k];
+    return 0;
+}
+
+}  // namespace
+
 int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
     CountPlan C;
     if (plan_count(ctx, req, true, C, err)) return err->status;
     if (req.scale_exp_out) *req.scale_exp_out = C.scale_exp;
-    const Binning *bin = req.bin;
-    ScratchBuf<WorkItem> d_items;
-    ScratchBuf<Segment> d_segs;
-    ScratchBuf<unsigned long long> d_full, d_sub, d_cnt;
-    ScratchBuf<int> d_head, d_err;
-    ScratchBuf<float> d_t1, d_t2, d_up_thr;
-    ScratchBuf<unsigned char> d_l1, d_l2;
-    ScratchBuf<unsigned> d_flags;
-    ScratchBuf<double> d_up_bins, d_up_centre;
-    const Ctx &X = *ctx;
-    TPCF_TRY(d_items.alloc(X, C.items.size()));
-    TPCF_TRY(d_segs.alloc(X, C.segs.size()));
-    TPCF_TRY(d_full.alloc(X, 2 * (size_t)C.nb));
-    TPCF_TRY(d_sub.alloc(X, 2 * (size_t)C.nb * C.n_jk));
-    TPCF_TRY(d_cnt.alloc(X, 4));
-    TPCF_TRY(d_head.alloc(X, 1));
-    TPCF_TRY(d_err.alloc(X, 1));
-    TPCF_TRY(d_t1.alloc(X, bin->t1.size()));
-    TPCF_TRY(d_t2.alloc(X, std::max<size_t>(bin->t2.size(), 1)));
-    TPCF_TRY(d_l1.alloc(X, LUT1_N));
-    TPCF_TRY(d_l2.alloc(X, LUT2_N));
-    if (C.n_flags()) TPCF_TRY(d_flags.alloc(X, C.n_flags()));
-    if (C.up) {
-        TPCF_TRY(d_up_thr.alloc(X, C.n_up()));
-        TPCF_TRY(d_up_bins.alloc(X, C.n_up()));
-        TPCF_TRY(d_up_centre.alloc(X, C.n_up()));
+    CountScratch S;
+    if (alloc_scratch(ctx, C, S, err)) return err->status;
+    return execute(ctx, C, S.D, full_out, region_out, st, err, true);
+}
+
+int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs, const std::vector<CountOut> &outs, Error *err) {
+    // every grid first: a grid build reads its cell tables back, which would
+    // otherwise wait for the count kernel ahead of it on the stream
+    for (const CountRequest &req : reqs) {
+        CountPlan C;
+        if (plan_count(ctx, req, true, C, err, true)) return err->status;
     }
-    ScratchBuf<JobK> d_jobs;
-    TPCF_TRY(d_jobs.alloc(X, C.jobs.size()));
-    ScratchBuf<double> d_adj_G, d_grad_a, d_grad_b;
-    if (C.adj) {
-        TPCF_TRY(d_adj_G.alloc(X, C.nb));
-        TPCF_TRY(d_grad_a.alloc(X, std::max(C.n_a, 1)));
-        if (!C.is_auto) TPCF_TRY(d_grad_b.alloc(X, std::max(C.n_b, 1)));
+    struct Flight {
+        CountPlan C;
+        CountScratch S;
+        HostIO io;
+        const CountOut *out = nullptr;
+    };
+    std::unique_ptr<Flight> prev;
+    auto finish = [&](std::unique_ptr<Flight> &f) -> int {
+        if (!f) return 0;
+        const int rc = finish_count(ctx, f->C, f->S.D, f->io, f->out->full, f->out->region, f->out->st, err, true);
+        f.reset();
+        return rc;
+    };
+    for (size_t i = 0; i < reqs.size(); ++i) {
+        std::unique_ptr<Flight> f(new Flight());
+        f->out = &outs[i];
+        // planned on the host while the previous count runs
+        int rc = plan_count(ctx, reqs[i], true, f->C, err);
+        if (!rc) rc = alloc_scratch(ctx, f->C, f->S, err);
+        if (!rc) rc = pinned_slot(ctx, (int)(i & 1), stage_bytes(f->C), &f->io.stage, &f->io.stage_cap, err);
+        if (!rc) rc = launch_count(ctx, f->C, f->S.D, f->io, err, true);
+        if (rc) {
+            cudaStreamSynchronize(ctx->stream);
+            return err->status ? err->status : 3;
+        }
+        // the previous count's results, while this one runs
+        rc = finish(prev);
+        if (rc) {
+            cudaStreamSynchronize(ctx->stream);
+            return rc;
+        }
+        prev = std::move(f);
     }
-    CountBuffers D;
-    D.jobs = d_jobs.p;
-    D.adj_G = d_adj_G.p;
-    D.grad_a = d_grad_a.p;
-    D.grad_b = d_grad_b.p;
-    D.items = d_items.p;
-    D.segs = d_segs.p;
-    D.full = d_full.p;
-    D.sub = d_sub.p;
-    D.cnt = d_cnt.p;
-    D.head = d_head.p;
-    D.err = d_err.p;
-    D.t1 = d_t1.p;
-    D.t2 = d_t2.p;
-    D.l1 = d_l1.p;
-    D.l2 = d_l2.p;
-    D.flags = C.n_flags() ? d_flags.p : nullptr;
-    D.up_thr = d_up_thr.p;
-    D.up_bins = d_up_bins.p;
-    D.up_centre = d_up_centre.p;
-    return execute(ctx, C, D, full_out, region_out, st, err, true);
+    return finish(prev);
 }
 
 // ---------------------------------------------------------------------------
