@@ -4,7 +4,7 @@
 //
 // Points are bucketed by (cell, jackknife region), buckets are scanned, and
 // every point is scattered into structure-of-arrays tiles: float4
-// (cell-relative position, weight) and float4 (unit vector, region).  Cells
+// (cell-relative position, weight) and float4 (unit vector, weight).  Cells
 // are numbered in Morton order of their lattice coordinates when the padded
 // cube stays small, so that neighbouring cells are close in memory.
 #include <cuda_runtime.h>
@@ -167,7 +167,7 @@ __global__ void scatter_kernel(GeomDev g, const double *__restrict__ xyz, const 
     float wi = w ? w[i] : 1.0f;
     pos[dst] = make_float4(__double2float_rn(x - ox), __double2float_rn(y - oy), __double2float_rn(z - oz), wi);
     const int r = jk ? jk[i] : 0;
-    aux[dst] = make_float4(__double2float_rn(nx), __double2float_rn(ny), __double2float_rn(nz), __int_as_float(r));
+    aux[dst] = make_float4(__double2float_rn(nx), __double2float_rn(ny), __double2float_rn(nz), wi);
     idx[dst] = i;
     if (xyz_s) {
         xyz_s[dst] = make_double4(x, y, z, (double)wi);
@@ -226,11 +226,12 @@ __global__ void regions_kernel(GeomDev g, int ncell, const int *__restrict__ bst
 // New weights for the points of a cached grid: pos.w (and xyz_s.w) from the
 // catalogue's weight array through the grid's index.
 __global__ void reweight_kernel(int n, const int *__restrict__ idx, const float *__restrict__ w,
-                                float4 *__restrict__ pos, double4 *__restrict__ xyz_s) {
+                                float4 *__restrict__ pos, float4 *__restrict__ aux, double4 *__restrict__ xyz_s) {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float wi = w[idx[k]];
     pos[k].w = wi;
+    aux[k].w = wi;
     if (xyz_s) xyz_s[k].w = (double)wi;
 }
 
@@ -393,7 +394,7 @@ int reweight_grids(Ctx *ctx, Catalog *cat, Error *err) {
         Grid *g = kv.second.get();
         if (g->input_w && cat->iw.p) continue;  // carries input weights, which did not change
         if (g->n == 0) continue;
-        reweight_kernel<<<(g->n + 255) / 256, 256, 0, ctx->stream>>>(g->n, g->idx.p, cat->w.p, g->pos.p,
+        reweight_kernel<<<(g->n + 255) / 256, 256, 0, ctx->stream>>>(g->n, g->idx.p, cat->w.p, g->pos.p, g->aux.p,
                                                                      g->has_fp64 ? g->xyz_s.p : nullptr);
         ++ctx->launches;
         TPCF_CUDA_TRY(cudaGetLastError());

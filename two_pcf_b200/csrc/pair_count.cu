@@ -473,11 +473,14 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
     const float dx = e.x, dy = e.y, dz = e.z;
     const float s2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));  // as in the candidate test
     const float4 qa = s_achunk[ka];
-    const float wa = qa.w, wb = s_pos[jl].w;
-    float pi = 0.f;
+    const float wa = qa.w;
+    float wb, pi = 0.f;
     if constexpr (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU) {
-        const float4 ab = s_aux[jl];
+        const float4 ab = s_aux[jl];  // unit vector and weight of the B point
+        wb = ab.w;
         pi = 0.5f * fmaf(dz, qa.z + ab.z, fmaf(dy, qa.y + ab.y, dx * (qa.x + ab.x)));
+    } else {
+        wb = s_pos[jl].w;
     }
     int bin;
     bool amb;
