@@ -325,50 +325,60 @@ def main():
         count_step(tp, ctx, D, R, bins, tp.FP32_GUARD, sharded=sharded)
     torch.cuda.synchronize()
 
-    launches0 = tp._capi.lib().tpcf_kernel_launches(ctx._h)
-    tot_in = tot_cand = 0
-    tot_kms = tot_flops = 0.0
-    step_ms = []
-    with ClockSampler(local) as clk:
-        dist_barrier(ws)
-        torch.cuda.synchronize()
-        for _ in range(args.steps):
+    def timed_steps(precision, k):
+        """k steps of `precision`, each after an L2 flush, bracketed by CUDA
+        events on the engine's stream; returns per-step device ms and the
+        step totals."""
+        ms, n_in, n_c, kms, fl, last = [], 0, 0, 0.0, 0.0, None
+        for _ in range(k):
             with torch.cuda.stream(stream):
                 flush.random_(0, 255)   # evict the L2 between steps
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            n_in, n_c, kms, fl, hists = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD, sharded=sharded)
+            a, c, km, f, last = count_step(tp, ctx, D, R, bins, precision, sharded=sharded)
             e1.record(stream)
             e1.synchronize()
-            step_ms.append(e0.elapsed_time(e1))
-            tot_in += n_in
-            tot_cand += n_c
-            tot_kms += kms
-            tot_flops += fl
+            ms.append(e0.elapsed_time(e1))
+            n_in += a
+            n_c += c
+            kms += km
+            fl += f
+        return ms, n_in, n_c, kms, fl, last
+
+    launches0 = tp._capi.lib().tpcf_kernel_launches(ctx._h)
+    with ClockSampler(local) as clk:
+        dist_barrier(ws)
+        torch.cuda.synchronize()
+        step_ms, tot_in, tot_cand, tot_kms, tot_flops, hists = timed_steps(tp.FP32_GUARD, args.steps)
         torch.cuda.synchronize()
         dist_barrier(ws)
-    launches = tp._capi.lib().tpcf_kernel_launches(ctx._h) - launches0
+        launches = tp._capi.lib().tpcf_kernel_launches(ctx._h) - launches0
+        # the plain FP64 path on the same steps, timed the same way (one
+        # untimed step first builds its grids and warms its kernels)
+        fp64_run = None
+        if not args.no_fp64:
+            count_step(tp, ctx, D, R, bins, tp.FP64, sharded=sharded)
+            torch.cuda.synchronize()
+            dist_barrier(ws)
+            fp64_run = timed_steps(tp.FP64, args.steps)
+            torch.cuda.synchronize()
+            dist_barrier(ws)
     total_ms = dist_max(sum(step_ms), ws)
     # whole job: pairs counted by all ranks (replicas, or the shards of one workload)
     value = dist_sum(tot_in, ws) / (total_ms * 1e-3)
     clocks = clk.summary()
 
-    # plain FP64 path on one step, and bit-exactness of the two paths
     fp64 = None
-    if not args.no_fp64:
-        torch.cuda.synchronize()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        n64, _, kms64, _, h64 = count_step(tp, ctx, D, R, bins, tp.FP64, sharded=sharded)
-        e1.record(stream)
-        e1.synchronize()
-        ms64 = e0.elapsed_time(e1)
+    if fp64_run is not None:
+        ms64, n64, _, kms64, _, h64 = fp64_run
+        t64 = dist_max(sum(ms64), ws)
         exact = all(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1]) for a, b in zip(hists, h64))
-        fp64 = {"value": dist_sum(n64, ws) / (dist_max(ms64, ws) * 1e-3), "ms_per_step": ms64, "kernel_ms": kms64,
-                "speedup_fp32_guard": (ms64 / (sum(step_ms) / len(step_ms))),
-                "bit_exact_histograms": bool(exact), "in_range_equal": int(n64) == int(tot_in // args.steps)}
+        fp64 = {"value": dist_sum(n64, ws) / (t64 * 1e-3), "steps": args.steps, "ms_per_step": t64 / args.steps,
+                "kernel_ms_per_step": kms64 / args.steps,
+                "speedup_fp32_guard": t64 / total_ms,
+                "speedup_fp32_guard_kernels": kms64 / tot_kms if tot_kms > 0 else None,
+                "bit_exact_histograms": bool(exact), "in_range_equal": int(n64) == int(tot_in)}
 
     # end to end through the C ABI: pinned host catalogues in, histograms out
     e2e = None

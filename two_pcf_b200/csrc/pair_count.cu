@@ -23,7 +23,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -42,10 +45,20 @@ constexpr int NT = 256;        // threads per CTA
 constexpr int NWARP = NT / 32;
 constexpr int R = 4;           // A points per thread
 constexpr int TA = NT * R;     // A chunk
-constexpr int TB = 256;        // B points per staged tile
-constexpr int QPUSH = 2;                 // A slots pushed between two consume checks
-constexpr int QCAP = 32 + 32 * QPUSH;   // queue entries per warp: a partial round plus QPUSH ballots
-static_assert(R % QPUSH == 0, "the push loops consume after every QPUSH A slots");
+constexpr int TB = 256;        // B points per staged tile (FP32 path)
+constexpr int TB_EXACT = 256;  // B points per staged tile (FP64 path)
+constexpr int kTileMax = TB > TB_EXACT ? TB : TB_EXACT;
+// queue entries pack (A chunk index << kTileShift | tile index)
+constexpr int kTileShift = kTileMax <= 256 ? 8 : (kTileMax <= 512 ? 9 : 10);
+constexpr int kTileMask = (1 << kTileShift) - 1;
+static_assert(kTileMax <= 1024 && (size_t)TA << kTileShift < (1u << 31), "queue entry packing");
+// A slots pushed between two consume checks: FP32 path, FP64 path by mode
+// (measured on the survey benchmark: s-mu counts run faster at 4, sigma-pi
+// counts at 2); the warp's queue holds a partial round plus 4 ballots
+constexpr int QPUSH = 4;
+__host__ __device__ constexpr int qpush_exact(int mode) { return mode == MODE_S_MU ? 4 : 2; }
+constexpr int kQueueCap = 32 + 32 * 4;
+static_assert(R % QPUSH == 0 && R % 2 == 0 && QPUSH <= 4, "the push loops consume after every QPUSH A slots");
 constexpr int LUT1_BITS = 8;   // buckets per octave of the float-indexed table
 constexpr int LUT1_OCTAVES = 24;
 constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
@@ -137,7 +150,8 @@ struct SmemLayout {
     size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, achunk, ga, gb, tile0, tile1, misc, total;
 };
 
-__host__ __device__ inline size_t tile_bytes(bool exact) { return (size_t)TB * (exact ? 64 : 32); }
+// FP32 path: pos and aux float4 per point; FP64 path: one double4 per point
+__host__ __device__ inline size_t tile_bytes(bool exact) { return exact ? (size_t)TB_EXACT * 32 : (size_t)TB * 32; }
 
 // lo/hi: the histogram pairs are added to (per segment region when there
 // are jackknife regions); alo/ahi: the item's A-side total (jackknife only).
@@ -162,7 +176,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o += LUT2_N;
     o = (o + 15) / 16 * 16;
     L.queue = o;
-    o += (size_t)NWARP * QCAP * 16;
+    o += (size_t)NWARP * kQueueCap * 16;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
     if (!exact) o += (size_t)TA * 16;
     L.ga = o;      // adjoint: per-point gradient sums (double)
@@ -466,9 +480,9 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
                                          const Shm &S, const float4 *s_pos, const float4 *s_aux,
                                          const float4 *s_achunk, const float4 e, int a_start, int jbase, int ra,
                                          int rb, Counters &cnt) {
-    // queue entry: (dx, dy, dz, A chunk index << 8 | tile index)
+    // queue entry: (dx, dy, dz, A chunk index << kTileShift | tile index)
     const int pk = __float_as_int(e.w);
-    const int ka = pk >> 8, jl = pk & 0xff;
+    const int ka = pk >> kTileShift, jl = pk & kTileMask;
     const int ia = a_start + ka, jb = jbase + jl;
     const float dx = e.x, dy = e.y, dz = e.z;
     const float s2 = fmaf(dz, dz, fmaf(dy, dy, dx * dx));  // as in the candidate test
@@ -632,6 +646,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
     constexpr bool ADJ = (WK == W_ADJ);
+    constexpr int TBK = EXACT ? TB_EXACT : TB;  // B points per tile
     const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
@@ -648,7 +663,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     uint64_t *bar = (uint64_t *)(smem + L.misc + 16);
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float4 *s_q = (float4 *)(smem + L.queue) + warp * QCAP;
+    float4 *s_q = (float4 *)(smem + L.queue) + warp * kQueueCap;
     const unsigned lt_mask = (1u << lane) - 1u;
     const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo), (double *)(smem + L.ga),
                 (double *)(smem + L.gb)};
@@ -657,7 +672,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         // the histogram words hold dL/d(full histogram) instead
         for (int i = tid; i < P.nb; i += NT) ((double *)(smem + L.lo))[i] = P.adj_G[i];
         for (int i = tid; i < TA; i += NT) S.ga[i] = 0.0;
-        for (int i = tid; i < TB; i += NT) S.gb[i] = 0.0;
+        for (int i = tid; i < TBK; i += NT) S.gb[i] = 0.0;
     } else {
         for (int i = tid; i < P.nb; i += NT) {
             s_lo[i] = 0;
@@ -714,7 +729,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             const uint32_t by = (uint32_t)len * 16u;
             dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
             dev::bulk_g2s(dst, J.b.pos + start, by, &bar[tc & 1]);
-            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TB * 16, J.b.aux + start, by, &bar[tc & 1]);
+            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TBK * 16, J.b.aux + start, by, &bar[tc & 1]);
         }
     };
 
@@ -741,7 +756,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             const int k = loc + r * G;
             const bool valid = thr_on && k < it.a_len;
             const int gi = it.a_start + k;
-            apack[r] = k << 8;  // queue entry: A chunk index << 8 | tile index
+            apack[r] = k << kTileShift;  // queue entry: A chunk index << kTileShift | tile index
             ai[r] = valid ? gi : 0x7fffffff;
             dax[r] = day[r] = daz[r] = 1e300;
             if (EXACT && valid) {
@@ -769,7 +784,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         }
         if (tid == 0) {
             const Segment s0 = P.segs[it.seg_begin];
-            issue(tcount, s0.b_start, min(TB, s0.b_len));
+            issue(tcount, s0.b_start, min(TBK, s0.b_len));
         }
         for (int si = it.seg_begin; si < it.seg_end; ++si) {
             const Segment sg = P.segs[si];
@@ -797,16 +812,16 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     az[r] = p.z + offz;
                 }
             }
-            const int ntiles = (sg.b_len + TB - 1) / TB;
+            const int ntiles = (sg.b_len + TBK - 1) / TBK;
             for (int t = 0; t < ntiles; ++t) {
-                const int tstart = t * TB;
-                const int tlen = min(TB, sg.b_len - tstart);
+                const int tstart = t * TBK;
+                const int tlen = min(TBK, sg.b_len - tstart);
                 if (tid == 0) {
                     if (t + 1 < ntiles) {
-                        issue(tcount + 1, sg.b_start + tstart + TB, min(TB, sg.b_len - tstart - TB));
+                        issue(tcount + 1, sg.b_start + tstart + TBK, min(TBK, sg.b_len - tstart - TBK));
                     } else if (si + 1 < it.seg_end) {
                         const Segment nx = P.segs[si + 1];
-                        issue(tcount + 1, nx.b_start, min(TB, nx.b_len));
+                        issue(tcount + 1, nx.b_start, min(TBK, nx.b_len));
                     }
                 }
                 if (!dev::mbar_wait_bounded(&bar[tcount & 1], (tcount >> 1) & 1u, kWaitLimit)) {
@@ -843,11 +858,12 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 hit[r] = jv && (s2 < P.max_r_sq) && (s2 > P.min_r_sq) && (!self || jg > ai[r]);
                             }
                         }
+                        constexpr int QPX = qpush_exact(MODE);
 #pragma unroll
-                        for (int r0 = 0; r0 < R; r0 += QPUSH) {
-                            // at most 31 + 32 * QPUSH entries: within QCAP
+                        for (int r0 = 0; r0 < R; r0 += QPX) {
+                            // at most 31 + 32 * QPX entries: within the queue
 #pragma unroll
-                            for (int r = r0; r < r0 + QPUSH; ++r) {
+                            for (int r = r0; r < r0 + QPX; ++r) {
                                 const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
                                 if (hit[r])
                                     s_q[qn + __popc(bal & lt_mask)] =
@@ -858,8 +874,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 __syncwarp();
                                 const float4 e = s_q[qn - 32 + lane];
                                 const int pk = __float_as_int(e.w);
-                                bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
-                                                           jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb,
+                                bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> kTileShift),
+                                                           jbase + (pk & kTileMask), pk >> kTileShift, pk & kTileMask,
+                                                           it.a_region, rb,
                                                            cnt);
                                 __syncwarp();
                                 qn -= 32;
@@ -871,15 +888,16 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         if (lane < qn) {
                             const float4 e = s_q[lane];
                             const int pk = __float_as_int(e.w);
-                            bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> 8),
-                                                       jbase + (pk & 0xff), pk >> 8, pk & 0xff, it.a_region, rb, cnt);
+                            bin_exact<MODE, UNITW, WK>(P, J, EA, S, e.x, e.y, e.z, it.a_start + (pk >> kTileShift),
+                                                       jbase + (pk & kTileMask), pk >> kTileShift, pk & kTileMask,
+                                                       it.a_region, rb, cnt);
                         }
                         __syncwarp();
                     }
                 } else {
                     const unsigned char *tile = tile_base + (tcount & 1) * tile_stride;
                     const float4 *s_pos = (const float4 *)tile;
-                    const float4 *s_aux = (const float4 *)(tile + (size_t)TB * 16);
+                    const float4 *s_aux = (const float4 *)(tile + (size_t)TBK * 16);
                     // Candidates: (dx, dy, dz) of the pair in the segment's cell
                     // frame; those inside the guard-widened range are pushed
                     // into the warp's queue with a ballot, and each time 32 are
@@ -1424,16 +1442,22 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         // hold a few hundred points on average in the denser catalogue (the
         // B points a cell's stencil visits set the candidate count; measured
         // on the survey benchmark, a cross count of sparse data against dense
-        // randoms runs ~10 % faster at side rb/2 than at rb).
-        auto per_cell = [&](const Catalog *X) {
+        // randoms runs ~10 % faster at side rb/2 than at rb).  The FP64
+        // path, whose candidate test costs several times the FP32 one, goes
+        // to side rb/3 once the A catalogue holds ~50 points per such cell
+        // (measured on the survey benchmark: 3-8 % faster on each count that
+        // meets it; the FP32 path gains under 1 % there and keeps rb/2).
+        auto per_cell = [&](const Catalog *X, int k) {
             const double *lo = C.angular ? (subset ? X->ulo_kept : X->ulo_all) : X->lo_kept;
             const double *hi = C.angular ? (subset ? X->uhi_kept : X->uhi_all) : X->hi_kept;
             const double n = subset ? (double)X->n_kept : (double)X->n_all;
             double vol = 1;
-            for (int k = 0; k < 3; ++k) vol *= std::max(hi[k] - lo[k], rb);
-            return n * (rb / 2) * (rb / 2) * (rb / 2) / vol;
+            for (int d = 0; d < 3; ++d) vol *= std::max(hi[d] - lo[d], rb);
+            const double c = rb / k;
+            return n * c * c * c / vol;
         };
-        m = std::max(per_cell(A), per_cell(B)) >= 256 ? 2 : 1;
+        m = std::max(per_cell(A, 2), per_cell(B, 2)) >= 256 ? 2 : 1;
+        if (req.exact_fp64 && per_cell(A, 3) >= 50) m = 3;
     }
     const double side = rb / m * (1.0 + 1e-9);
     GridSpec gs;
@@ -1881,30 +1905,63 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
 }
 
 int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs, const std::vector<CountOut> &outs, Error *err) {
+    // TPCF_TRACE=1: one stderr line per count with its host planning time
+    // and where its kernel ran on the device, in ms from the call's start
+    // (diagnostics of the pipelining; the counts are unchanged)
+    const char *tr_env = std::getenv("TPCF_TRACE");
+    const bool trace = tr_env && tr_env[0] && tr_env[0] != '0';
+    using clk = std::chrono::steady_clock;
+    const auto h0 = clk::now();
+    auto host_ms = [&](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+    struct EventGuard {
+        cudaEvent_t e = nullptr;
+        ~EventGuard() {
+            if (e) cudaEventDestroy(e);
+        }
+    } start;
+    if (trace) {
+        TPCF_TRY(cudaEventCreate(&start.e));
+        TPCF_TRY(cudaEventRecord(start.e, ctx->stream));
+    }
+    const cudaEvent_t ev0 = start.e;
     // every grid first: a grid build reads its cell tables back, which would
     // otherwise wait for the count kernel ahead of it on the stream
     for (const CountRequest &req : reqs) {
         CountPlan C;
         if (plan_count(ctx, req, true, C, err, true)) return err->status;
     }
+    if (trace) std::fprintf(stderr, "[tpcf trace] %zu counts: grids built at %.1f ms (host)\n", reqs.size(), host_ms(h0));
     struct Flight {
         CountPlan C;
         CountScratch S;
         HostIO io;
         const CountOut *out = nullptr;
+        size_t index = 0;
+        double plan_ms = 0;
     };
     std::unique_ptr<Flight> prev;
     auto finish = [&](std::unique_ptr<Flight> &f) -> int {
         if (!f) return 0;
         const int rc = finish_count(ctx, f->C, f->S.D, f->io, f->out->full, f->out->region, f->out->st, err, true);
+        if (trace && !rc) {
+            float k0 = 0, k1 = 0;
+            cudaEventElapsedTime(&k0, ev0, f->io.e0);
+            cudaEventElapsedTime(&k1, ev0, f->io.e1);
+            std::fprintf(stderr, "[tpcf trace] count %zu: %zu items, %zu segments, plan %.1f ms (host); "
+                         "kernel %.1f-%.1f ms (device); finished at %.1f ms (host)\n", f->index, f->C.items.size(),
+                         f->C.segs.size(), f->plan_ms, k0, k1, host_ms(h0));
+        }
         f.reset();
         return rc;
     };
     for (size_t i = 0; i < reqs.size(); ++i) {
         std::unique_ptr<Flight> f(new Flight());
         f->out = &outs[i];
+        f->index = i;
         // planned on the host while the previous count runs
+        const auto hp = clk::now();
         int rc = plan_count(ctx, reqs[i], true, f->C, err);
+        f->plan_ms = host_ms(hp);
         if (!rc) rc = alloc_scratch(ctx, f->C, f->S, err);
         if (!rc) rc = pinned_slot(ctx, (int)(i & 1), stage_bytes(f->C), &f->io.stage, &f->io.stage_cap, err);
         if (!rc) rc = launch_count(ctx, f->C, f->S.D, f->io, err, true);
