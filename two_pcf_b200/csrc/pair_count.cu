@@ -48,10 +48,17 @@ constexpr int TA = NT * R;     // A chunk
 constexpr int TB = 256;        // B points per staged tile (FP32 path)
 constexpr int TB_EXACT = 256;  // B points per staged tile (FP64 path)
 constexpr int kTileMax = TB > TB_EXACT ? TB : TB_EXACT;
+// Staged tile buffers (warps may run up to NBUF - 1 tiles apart): FP32 path,
+// FP64 path (whose per-pair loads of the double arrays lose L1 to a third
+// buffer; measured on the survey benchmark, each path at its faster depth)
+constexpr int NBUF = 3;
+constexpr int NBUF_EXACT = 2;
+constexpr int kNbufMax = NBUF > NBUF_EXACT ? NBUF : NBUF_EXACT;
+__host__ __device__ constexpr int n_buffers(bool exact) { return exact ? NBUF_EXACT : NBUF; }
 // queue entries pack (A chunk index << kTileShift | tile index)
 constexpr int kTileShift = kTileMax <= 256 ? 8 : (kTileMax <= 512 ? 9 : 10);
 constexpr int kTileMask = (1 << kTileShift) - 1;
-static_assert(kTileMax <= 1024 && (size_t)TA << kTileShift < (1u << 31), "queue entry packing");
+static_assert(16 + 12 * kNbufMax <= 64 && kTileMax <= 1024 && (size_t)TA << kTileShift < (1u << 31), "queue entry packing");
 // A slots pushed between two consume checks: FP32 path, FP64 path by mode
 // (measured on the survey benchmark: s-mu counts run faster at 4, sigma-pi
 // counts at 2); the warp's queue holds a partial round plus 4 ballots
@@ -187,9 +194,9 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     L.tile0 = o;
     o += tile_bytes(exact);
     L.tile1 = o;
-    o += tile_bytes(exact);
+    o += (size_t)(n_buffers(exact) - 1) * tile_bytes(exact);
     o = (o + 15) / 16 * 16;
-    L.misc = o;  // item index, mbarriers, the item's job
+    L.misc = o;  // item index, mbarriers, tile-done counters, the item's job
     o += 64 + sizeof(JobK);
     L.total = o;
     return L;
@@ -647,6 +654,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
     constexpr bool ADJ = (WK == W_ADJ);
     constexpr int TBK = EXACT ? TB_EXACT : TB;  // B points per tile
+    constexpr int NB = n_buffers(EXACT);          // tile buffers
     const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
@@ -660,7 +668,8 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     const size_t tile_stride = L.tile1 - L.tile0;
     float4 *s_achunk = (float4 *)(smem + L.achunk);
     int *s_item = (int *)(smem + L.misc);
-    uint64_t *bar = (uint64_t *)(smem + L.misc + 16);
+    uint64_t *bar = (uint64_t *)(smem + L.misc + 16);                  // one per tile buffer
+    unsigned *s_done = (unsigned *)(smem + L.misc + 16 + 8 * kNbufMax);  // warps done with each buffer (running count)
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4 *s_q = (float4 *)(smem + L.queue) + warp * kQueueCap;
@@ -688,8 +697,10 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     for (int i = tid; i < LUT1_N; i += NT) s_l1[i] = P.lut1g[i];
     for (int i = tid; i < LUT2_N; i += NT) s_l2[i] = P.lut2g[i];
     if (tid == 0) {
-        dev::mbar_init(&bar[0], 1);
-        dev::mbar_init(&bar[1], 1);
+        for (int b = 0; b < NB; ++b) {
+            dev::mbar_init(&bar[b], 1);
+            s_done[b] = 0;
+        }
         dev::mbar_init_fence();
     }
     __syncthreads();
@@ -719,17 +730,18 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         const JobK &J = JK ? *s_job : P.job0;
         const ExactArgs EA{J.a.xyz, J.a.unit, J.b.xyz, J.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2, P.los_mid};
     auto issue = [&](unsigned tc, int start, int len) {
-        unsigned char *dst = tile_base + (tc & 1) * tile_stride;
+        const unsigned buf = tc % NB;
+        unsigned char *dst = tile_base + buf * tile_stride;
         dev::fence_proxy_async();
         if (EXACT) {
             const uint32_t by = (uint32_t)len * 32u;
-            dev::mbar_expect_tx(&bar[tc & 1], by);
-            dev::bulk_g2s(dst, J.b.xyz_s + start, by, &bar[tc & 1]);
+            dev::mbar_expect_tx(&bar[buf], by);
+            dev::bulk_g2s(dst, J.b.xyz_s + start, by, &bar[buf]);
         } else {
             const uint32_t by = (uint32_t)len * 16u;
-            dev::mbar_expect_tx(&bar[tc & 1], kNeedAux ? 2 * by : by);
-            dev::bulk_g2s(dst, J.b.pos + start, by, &bar[tc & 1]);
-            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TBK * 16, J.b.aux + start, by, &bar[tc & 1]);
+            dev::mbar_expect_tx(&bar[buf], kNeedAux ? 2 * by : by);
+            dev::bulk_g2s(dst, J.b.pos + start, by, &bar[buf]);
+            if (kNeedAux) dev::bulk_g2s(dst + (size_t)TBK * 16, J.b.aux + start, by, &bar[buf]);
         }
     };
 
@@ -782,9 +794,31 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             }
             __syncthreads();
         }
+        // The item's tiles in order: (segment, tile within it).  Tiles 0 to
+        // NB - 1 are staged here; each later tile by the last warp to
+        // finish the tile NB before it, so no warp waits for the others
+        // between tiles.
+        auto tile_next = [&](int &psi, int &pt) -> bool {
+            if (pt + 1 < (P.segs[psi].b_len + TBK - 1) / TBK) {
+                ++pt;
+                return true;
+            }
+            if (psi + 1 < it.seg_end) {
+                ++psi;
+                pt = 0;
+                return true;
+            }
+            return false;
+        };
+        auto issue_at = [&](unsigned tc, int psi, int pt) {
+            const Segment sx = P.segs[psi];
+            const int st = pt * TBK;
+            issue(tc, sx.b_start + st, min(TBK, sx.b_len - st));
+        };
         if (tid == 0) {
-            const Segment s0 = P.segs[it.seg_begin];
-            issue(tcount, s0.b_start, min(TBK, s0.b_len));
+            int psi = it.seg_begin, pt = 0;
+            issue_at(tcount, psi, pt);
+            for (int b = 1; b < NB && tile_next(psi, pt); ++b) issue_at(tcount + b, psi, pt);
         }
         for (int si = it.seg_begin; si < it.seg_end; ++si) {
             const Segment sg = P.segs[si];
@@ -816,15 +850,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             for (int t = 0; t < ntiles; ++t) {
                 const int tstart = t * TBK;
                 const int tlen = min(TBK, sg.b_len - tstart);
-                if (tid == 0) {
-                    if (t + 1 < ntiles) {
-                        issue(tcount + 1, sg.b_start + tstart + TBK, min(TBK, sg.b_len - tstart - TBK));
-                    } else if (si + 1 < it.seg_end) {
-                        const Segment nx = P.segs[si + 1];
-                        issue(tcount + 1, nx.b_start, min(TBK, nx.b_len));
-                    }
-                }
-                if (!dev::mbar_wait_bounded(&bar[tcount & 1], (tcount >> 1) & 1u, kWaitLimit)) {
+                if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, kWaitLimit)) {
                     atomicExch(P.err, 4);  // device timeout: results are discarded by the host
                 }
                 const int jbase = sg.b_start + tstart;
@@ -834,7 +860,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                 // queued the whole warp bins them (no divergent binning).
                 int qn = 0;  // queued entries of this warp (warp-uniform)
                 if (EXACT) {
-                    const double4 *s_xyz = (const double4 *)(tile_base + (tcount & 1) * tile_stride);
+                    const double4 *s_xyz = (const double4 *)(tile_base + (tcount % NB) * tile_stride);
                     for (int m = 0; m < nsteps; ++m) {
                         const int jj = grp + m * Pn;
                         const bool jv = thr_on && jj < tlen;
@@ -895,7 +921,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         __syncwarp();
                     }
                 } else {
-                    const unsigned char *tile = tile_base + (tcount & 1) * tile_stride;
+                    const unsigned char *tile = tile_base + (tcount % NB) * tile_stride;
                     const float4 *s_pos = (const float4 *)tile;
                     const float4 *s_aux = (const float4 *)(tile + (size_t)TBK * 16);
                     // Candidates: (dx, dy, dz) of the pair in the segment's cell
@@ -954,9 +980,25 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                         __syncwarp();
                     }
                 }
-                __syncthreads();  // everyone is done with this buffer before it is refilled
+                // This warp is done with the buffer: the last warp to finish it
+                // refills it with the tile NB ahead (the arrivals of one tile
+                // all precede those of the next tile in the same buffer, whose
+                // data comes only after them).
+                __syncwarp();
+                if (lane == 0) {
+                    __threadfence_block();
+                    const unsigned done = atomicAdd(&s_done[tcount % NB], 1u);
+                    if (done % NWARP == NWARP - 1) {
+                        __threadfence_block();
+                        int psi = si, pt = t;
+                        bool more = true;
+                        for (int b = 0; b < NB && more; ++b) more = tile_next(psi, pt);
+                        if (more) issue_at(tcount + NB, psi, pt);
+                    }
+                }
                 if constexpr (ADJ) {
                     // this tile's B gradients to their points
+                    __syncthreads();
                     const int jb0 = sg.b_start + tstart;
                     for (int t2 = tid; t2 < tlen; t2 += NT) {
                         const double v = S.gb[t2];
@@ -973,6 +1015,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
             if (JK) {
                 const bool last = (si + 1 == it.seg_end) || ((P.segs[si + 1].meta & 0xffff) != rb);
                 if (last) {
+                    __syncthreads();  // every warp's pairs of this region are in the histogram
                     for (int b = tid; b < P.nb; b += NT) {
                         const unsigned long long v = ((unsigned long long)s_hi[b] << 32) | s_lo[b];
                         if (!v) continue;
