@@ -163,6 +163,7 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
     if (!cat) return TPCF_E_OOM;
     tpcf::Catalog &c = cat->c;
     c.ctx = &ctx->c;
+    c.ctx_alive = ctx->c.alive;
     c.n_all = n;
     c.n_jk = n_jk_regions;
     c.n_mask = bitmask ? n_mask_ints : 0;
@@ -310,6 +311,7 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
 
 int tpcf_catalog_destroy(tpcf_catalog *cat) {
     if (!cat) return TPCF_E_INVALID_ARG;
+    cat->c.release_device();
     delete cat;
     return TPCF_OK;
 }
@@ -318,7 +320,7 @@ int64_t tpcf_catalog_n_used(const tpcf_catalog *cat) { return cat ? cat->c.n_kep
 
 int tpcf_catalog_release_cache(tpcf_catalog *cat) {
     if (!cat) return TPCF_E_INVALID_ARG;
-    cat->c.grids.clear();
+    cat->c.release_grids();
     return TPCF_OK;
 }
 

@@ -56,6 +56,9 @@ struct Ctx {
     // on demand, freed with the context)
     unsigned char *pinned[2] = {nullptr, nullptr};
     size_t pinned_cap[2] = {0, 0};
+    // lives exactly as long as the context: catalogues hold a weak reference
+    // and release on the context's stream only while it lives
+    std::shared_ptr<int> alive = std::make_shared<int>(0);
 };
 
 // Device scratch of one call, from the context's stream-ordered memory pool:
@@ -106,12 +109,16 @@ struct PoolBuf {
     PoolBuf(const PoolBuf &) = delete;
     PoolBuf &operator=(const PoolBuf &) = delete;
     ~PoolBuf() { release(); }
-    void release() {
+    void release() { release_on(0); }
+    // Release in the order of stream `s` (the legacy stream when 0): a
+    // context that is still alive releases on its own stream, so that its
+    // next allocations reuse the memory in stream order.
+    void release_on(cudaStream_t s) {
         if (p) {
             int cur = device;
             cudaGetDevice(&cur);
             if (cur != device) cudaSetDevice(device);
-            cudaFreeAsync(p, 0);
+            cudaFreeAsync(p, s);
             if (cur != device) cudaSetDevice(cur);
         }
         p = nullptr;
@@ -157,10 +164,23 @@ struct Grid {
     std::vector<int> h_regions;
     std::vector<int> h_run_start;
     bool has_fp64 = false;
+    void release_on(cudaStream_t s) {
+        pos.release_on(s);
+        aux.release_on(s);
+        idx.release_on(s);
+        xyz_s.release_on(s);
+        unit_s.release_on(s);
+        cell_start.release_on(s);
+        cell_coord.release_on(s);
+        region_start.release_on(s);
+        regions.release_on(s);
+        run_start.release_on(s);
+    }
 };
 
 struct Catalog {
     Ctx *ctx = nullptr;
+    std::weak_ptr<int> ctx_alive;  // expired once the context is destroyed
     int64_t n_all = 0;
     int n_kept = 0;
     int n_mask = 0;
@@ -181,6 +201,27 @@ struct Catalog {
     std::vector<int> h_jk;
     std::vector<int> h_kept;
     std::map<std::string, std::unique_ptr<Grid>> grids;  // cached by geometry
+    // Release every device array: on the context's stream while the context
+    // lives (its next allocations reuse the memory in stream order), else on
+    // the legacy stream.
+    void release_device() {
+        const cudaStream_t s = ctx_alive.expired() ? (cudaStream_t)0 : ctx->stream;
+        for (auto &kv : grids) kv.second->release_on(s);
+        grids.clear();
+        xyz.release_on(s);
+        unit.release_on(s);
+        w.release_on(s);
+        iw.release_on(s);
+        jk.release_on(s);
+        masks.release_on(s);
+        dmasks.release_on(s);
+        kept.release_on(s);
+    }
+    void release_grids() {
+        const cudaStream_t s = ctx_alive.expired() ? (cudaStream_t)0 : ctx->stream;
+        for (auto &kv : grids) kv.second->release_on(s);
+        grids.clear();
+    }
 };
 
 struct Binning {

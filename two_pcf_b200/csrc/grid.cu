@@ -10,7 +10,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -74,7 +77,12 @@ __global__ void scan_add_kernel(int *__restrict__ out, const int *__restrict__ o
 }
 
 // Exclusive scan of n ints (in may equal out).  Totals must fit in int.
-cudaError_t exclusive_scan(const int *in, int *out, long long n, cudaStream_t st, unsigned long long *launches) {
+// The tile sums come from `pool` (the context's pool, which keeps released
+// memory): the device's default pool hands its memory back to the driver at
+// every synchronisation, and mapping it again was measured stalling a grid
+// build for up to 0.9 s.
+cudaError_t exclusive_scan(const int *in, int *out, long long n, cudaStream_t st, unsigned long long *launches,
+                           cudaMemPool_t pool) {
     if (n <= 0) return cudaSuccess;
     long long tiles = (n + kScanTile - 1) / kScanTile;
     if (tiles == 1) {
@@ -83,11 +91,12 @@ cudaError_t exclusive_scan(const int *in, int *out, long long n, cudaStream_t st
         return cudaGetLastError();
     }
     int *sums = nullptr;
-    cudaError_t e = cudaMallocAsync((void **)&sums, sizeof(int) * tiles, st);
+    cudaError_t e = pool ? cudaMallocFromPoolAsync((void **)&sums, sizeof(int) * tiles, pool, st)
+                         : cudaMallocAsync((void **)&sums, sizeof(int) * tiles, st);
     if (e != cudaSuccess) return e;
     scan_tile_kernel<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, sums, n);
     ++*launches;
-    e = exclusive_scan(sums, sums, tiles, st, launches);
+    e = exclusive_scan(sums, sums, tiles, st, launches, pool);
     if (e == cudaSuccess) {
         scan_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, sums, n);
         ++*launches;
@@ -272,6 +281,13 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
     const double side = spec.side;
     const bool subset_kept = spec.subset_kept;
     cudaStream_t st = ctx->stream;
+    // TPCF_TRACE=1: host time of the build's phases on stderr (diagnostics)
+    const char *tr_env = std::getenv("TPCF_TRACE");
+    const bool trace = tr_env && tr_env[0] && tr_env[0] != '0';
+    using clk = std::chrono::steady_clock;
+    const auto t0 = clk::now();
+    auto ms_since = [&](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
+    double t_alloc = 0, t_launch = 0, t_sync1 = 0;
     std::unique_ptr<Grid> g(new Grid());
     g->side = side;
     g->subset_kept = subset_kept;
@@ -332,6 +348,7 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
     TPCF_CUDA_TRY(g->cell_start.alloc(*ctx, ncell + 1));
     TPCF_CUDA_TRY(g->cell_coord.alloc(*ctx, ncell));
     TPCF_CUDA_TRY(g->region_start.alloc(*ctx, ncell + 1));
+    if (trace) t_alloc = ms_since(t0);
     TPCF_CUDA_TRY(cudaMemsetAsync(counts.p, 0, sizeof(int) * (nbucket + 1), st));
     const int *subset = subset_kept ? cat->kept.p : nullptr;
     const int *jk = cat->n_jk > 1 ? cat->jk.p : nullptr;
@@ -341,7 +358,7 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
         TPCF_CUDA_TRY(cudaGetLastError());
     }
     // counts -> bucket starts (exclusive); the extra element becomes n.
-    TPCF_CUDA_TRY(exclusive_scan(counts.p, counts.p, nbucket + 1, st, &ctx->launches));
+    TPCF_CUDA_TRY(exclusive_scan(counts.p, counts.p, nbucket + 1, st, &ctx->launches, ctx->pool));
     ScratchBuf<int> fill;
     TPCF_CUDA_TRY(fill.alloc(*ctx, nbucket));
     TPCF_CUDA_TRY(cudaMemsetAsync(fill.p, 0, sizeof(int) * nbucket, st));
@@ -360,14 +377,16 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
                                                                      g->cell_coord.p, nreg.p);
     ++ctx->launches;
     TPCF_CUDA_TRY(cudaGetLastError());
-    TPCF_CUDA_TRY(exclusive_scan(nreg.p, g->region_start.p, ncell + 1, st, &ctx->launches));
+    TPCF_CUDA_TRY(exclusive_scan(nreg.p, g->region_start.p, ncell + 1, st, &ctx->launches, ctx->pool));
     g->h_region_start.resize(ncell + 1);
     TPCF_CUDA_TRY(cudaMemcpyAsync(g->h_region_start.data(), g->region_start.p, sizeof(int) * (ncell + 1),
                                   cudaMemcpyDeviceToHost, st));
     g->h_cell_start.resize(ncell + 1);
     TPCF_CUDA_TRY(cudaMemcpyAsync(g->h_cell_start.data(), g->cell_start.p, sizeof(int) * (ncell + 1),
                                   cudaMemcpyDeviceToHost, st));
+    if (trace) t_launch = ms_since(t0);
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
+    if (trace) t_sync1 = ms_since(t0);
     int nregions = g->h_region_start[ncell];
     TPCF_CUDA_TRY(g->regions.alloc(*ctx, nregions));
     TPCF_CUDA_TRY(g->run_start.alloc(*ctx, nregions));
@@ -384,6 +403,9 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
                                       cudaMemcpyDeviceToHost, st));
     }
     TPCF_CUDA_TRY(cudaStreamSynchronize(st));
+    if (trace)
+        std::fprintf(stderr, "[tpcf trace] grid of %d points, %d cells: allocated %.1f, launched %.1f, first sync %.1f, "
+                     "done %.1f ms (host)\n", n, (int)ncell, t_alloc, t_launch, t_sync1, ms_since(t0));
     *out = g.get();
     cat->grids[key] = std::move(g);
     return 0;
