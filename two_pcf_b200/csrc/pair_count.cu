@@ -6,7 +6,8 @@
 // run of catalogue A against one run of catalogue B — from a device queue.
 // Each thread holds R points of A in registers; B streams through shared
 // memory in tiles staged by one-dimensional bulk copies (cp.async.bulk with
-// mbarrier completion, double buffered).
+// mbarrier completion) into a ring of buffers; the last warp to finish a
+// buffer stages the next tile into it, so no block barrier separates tiles.
 //
 // Producer/consumer inside every warp: the candidate loop evaluates s^2 in
 // FP32 from cell-relative coordinates and pushes the pairs that pass the
