@@ -82,3 +82,26 @@ def test_count_many_empty_and_errors(ctx, survey):
     with pytest.raises(tp.TpcfError):
         tp.count_many(ctx, [(survey["D"], None, b)], precision=7)
     assert tp.count_many(ctx, []) == []
+
+
+def test_count_many_trace_leaves_counts_unchanged(ctx, survey, capfd, monkeypatch):
+    """TPCF_TRACE=1 prints one timeline line per count (and per grid built)
+    on stderr; the counts are those of an untraced call."""
+    D, R = survey["D"], survey["R"]
+    b = binnings(ctx, survey["n_jk"])[1]
+    jobs = [(D, None, b), (D, R, b), (R, None, b)]
+    for c in (D, R):
+        _capi.lib().tpcf_catalog_release_cache(c._h)
+    plain = tp.count_many(ctx, jobs)
+    capfd.readouterr()
+    monkeypatch.setenv("TPCF_TRACE", "1")
+    for c in (D, R):
+        _capi.lib().tpcf_catalog_release_cache(c._h)
+    traced = tp.count_many(ctx, jobs)
+    err = capfd.readouterr().err
+    assert "[tpcf trace] 3 counts: grids built" in err
+    assert all(f"count {k}:" in err for k in range(3))
+    assert "[tpcf trace] grid of" in err
+    for (f, r, _), (f1, r1, _) in zip(plain, traced):
+        assert np.array_equal(f, f1)
+        assert np.array_equal(r, r1)
