@@ -58,6 +58,9 @@ def parse():
                         "default: one workload replica per rank (weak scaling)")
     p.add_argument("--one-count", choices=["s_mu", "sigma_pi"], default=None,
                    help="profiling case: one RR count of the workload's randoms at --scale, then exit")
+    p.add_argument("--workload", choices=["survey", "mocks", "invp", "adjoint"], default="survey",
+                   help="survey: the headline line (default); mocks / invp / adjoint: one JSON line for the "
+                        "batched-mocks, inverse-p angular and weight-gradient workloads at --scale (1 GPU)")
     return p.parse_args()
 
 
@@ -73,6 +76,130 @@ def one_count(args):
     b = tp.Binning(ctx, tp.S_MU if args.one_count == "s_mu" else tp.SIGMA_PI, *axes, w["n_jk"])
     full, _, st = tp.count(ctx, R, None, b, tp.FP32_GUARD)
     print(json.dumps({"one_count": args.one_count, "scale": args.scale, **st}))
+
+
+def other_workload(args):
+    """The spec's other workloads on one GPU, each one JSON line (FP32+guard
+    path, device time from CUDA events, median of --steps after --warmup):
+
+    mocks   -- 64 Neyman-Scott mocks in a 1000 Mpc/h box (sizes uniform on
+               [200k, 2M] x scale, cluster sigma uniform on [3, 8]), one shared
+               uniform random catalogue of 10M x scale, 27 sub-cube regions,
+               s-mu 40 log (1.3, 0-150) x 50: every mock's DD and DR in one
+               batched launch (graph replay, autotuned refinement), RR once;
+    invp    -- 500k x scale data on the survey footprint with 32 bitwise masks
+               (2048 runs, p uniform on [0.3, 1]) and 2M x scale randoms:
+               angular DD, DD-inverse-p, DR, DR-inverse-p (40 log bins, base
+               1.6, theta < 0.175 rad), then the 3-D s-mu inverse-p DD and DR
+               with the up-weights from those histograms;
+    adjoint -- the survey slab at scale: s-mu DD, DR, RR forward, and the
+               adjoint (per-point dL/dw) of the same counts."""
+    import two_pcf_b200 as tp
+    from two_pcf_b200 import synthetic
+    ctx = tp.Context(0)
+    scale = args.scale
+    rng = np.random.default_rng(11)
+
+    def median_ms(fn):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        ms, out = [], None
+        for _ in range(max(1, args.steps)):
+            out = fn()
+            ms.append(out[0])
+        return statistics.median(ms), out
+
+    line = {"workload": args.workload, "scale": scale, "unit": UNIT, "dtype": "f32", "data": "synthetic"}
+    if args.workload == "mocks":
+        box, n_mocks = 1000.0, 64
+
+        def cat(x):
+            c = np.clip((x / (box / 3)).astype(int), 0, 2)
+            return tp.Catalog(ctx, x, jk_region=((c[:, 0] * 3 + c[:, 1]) * 3 + c[:, 2]).astype(np.int32),
+                              n_jk_regions=27)
+        sizes = rng.integers(int(200_000 * scale), int(2_000_000 * scale) + 1, n_mocks)
+        M = [cat(synthetic.neyman_scott_box(rng, int(n), box, max(1, int(n) // 50), 50.0, rng.uniform(3, 8)))
+             for n in sizes]
+        R = cat(rng.uniform(0.0, box, (int(10_000_000 * scale), 3)))
+        b = tp.Binning(ctx, tp.S_MU, (0.0, 150.0, 1.3, 40), (0.0, 1.0, 0.0, 50), 27)
+        batch = tp.Batch(ctx, M, R, b, what=tp.BATCH_DD | tp.BATCH_DR, refinement=tp.BATCH_AUTOTUNE)
+
+        def run_batch():
+            _, _, st = batch.run()
+            return st["ms_kernel"], st
+        ms_b, (_, st_b) = median_ms(run_batch)
+
+        def run_rr():
+            _, _, st = tp.count(ctx, R, None, b)
+            return st["ms_kernel"], st
+        ms_r, (_, st_r) = median_ms(run_rr)
+        pairs = st_b["in_range"] + st_r["in_range"]
+        line.update({"metric": "in-range pairs/sec, 64 mocks DD+DR in one batched launch + shared RR",
+                     "value": pairs / ((ms_b + ms_r) * 1e-3), "ms": ms_b + ms_r, "batch_ms": ms_b, "rr_ms": ms_r,
+                     "batch_pairs": st_b["in_range"], "rr_pairs": st_r["in_range"], "mock_points": int(sizes.sum()),
+                     "random_points": int(10_000_000 * scale), "refinement": batch.refinement,
+                     "batch_work_items": st_b["work_items"]})
+    elif args.workload == "invp":
+        w = synthetic.survey_catalogue(seed=4, n_data=int(500_000 * scale), n_rand=int(2_000_000 * scale))
+        d, r = w["data"], w["rand"]
+        n_runs = 2048
+        md = synthetic.bitwise_masks(5, d["xyz"].shape[0], n_runs=n_runs)
+        mr = synthetic.bitwise_masks(6, r["xyz"].shape[0], n_runs=n_runs, all_set=True)
+        wd, iwd = tp.iip_weights(md, d["weight"], n_runs)
+        wr, iwr = tp.iip_weights(mr, r["weight"], n_runs)
+        D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], wd, iwd, d["jk"], w["n_jk"], md)
+        R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], wr, iwr, r["jk"], w["n_jk"], mr)
+        t_ax = (0.0, 1.0 - np.cos(0.175), 1.6, 40)
+        ba = tp.Binning(ctx, tp.ANGULAR, t_ax, None, w["n_jk"])
+        ang_jobs = [("DD", D, None, None), ("DD_invp", D, None, tp.Weights(tp.WEIGHTS_INVP_DD, n_runs)),
+                    ("DR", D, R, None), ("DR_invp", D, R, tp.Weights(tp.WEIGHTS_INVP_DR))]
+
+        def run_ang():
+            out = [tp.pair_count_weighted(ctx, a, bb, ba, wt) for _, a, bb, wt in ang_jobs]
+            return sum(o[2]["ms_kernel"] for o in out), out
+        ms_a, (_, ang) = median_ms(run_ang)
+        bs = tp.Binning(ctx, tp.S_MU, *S_MU_AXES, w["n_jk"])
+        w_dd = tp.Weights(tp.WEIGHTS_INVP_DD, n_runs, t_ax, ang[0][0], ang[1][0])
+        w_dr = tp.Weights(tp.WEIGHTS_INVP_DR, n_runs, t_ax, ang[2][0], ang[3][0])
+
+        def run_3d():
+            out = [tp.pair_count_weighted(ctx, D, None, bs, w_dd), tp.pair_count_weighted(ctx, D, R, bs, w_dr)]
+            return sum(o[2]["ms_kernel"] for o in out), out
+        ms_3, (_, td) = median_ms(run_3d)
+        pa = sum(o[2]["in_range"] for o in ang)
+        p3 = sum(o[2]["in_range"] for o in td)
+        line.update({"metric": "in-range pairs/sec, inverse-p angular stage + 3-D s-mu inverse-p DD and DR",
+                     "value": (pa + p3) / ((ms_a + ms_3) * 1e-3), "ms": ms_a + ms_3,
+                     "angular_ms": ms_a, "angular_pairs": pa, "angular_value": pa / (ms_a * 1e-3),
+                     "angular_ms_each": {n: o[2]["ms_kernel"] for (n, _, _, _), o in zip(ang_jobs, ang)},
+                     "s_mu_ms": ms_3, "s_mu_pairs": p3, "n_data": int(d["xyz"].shape[0]),
+                     "n_rand": int(r["xyz"].shape[0]), "mask_words": 32, "n_bitwise_runs": n_runs})
+    else:
+        w = make_workload(2, scale)
+        d, r = w["data"], w["rand"]
+        D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], w["n_jk"])
+        R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
+        b = tp.Binning(ctx, tp.S_MU, *S_MU_AXES, w["n_jk"])
+        jobs = [(D, None), (D, R), (R, None)]
+        G = rng.standard_normal(b.nb)
+
+        def fwd():
+            out = [tp.count(ctx, a, bb, b) for a, bb in jobs]
+            return sum(o[2]["ms_kernel"] for o in out), out
+        ms_f, (_, fo) = median_ms(fwd)
+
+        def bwd():
+            out = [tp.count_backward(ctx, a, bb, b, G) for a, bb in jobs]
+            return sum(o[2]["ms_kernel"] for o in out), out
+        ms_b, _ = median_ms(bwd)
+        pairs = sum(o[2]["in_range"] for o in fo)
+        line.update({"metric": "in-range pairs/sec of forward + backward (s-mu DD, DR, RR)",
+                     "value": pairs / ((ms_f + ms_b) * 1e-3), "ms": ms_f + ms_b, "forward_ms": ms_f,
+                     "backward_ms": ms_b, "forward_plus_backward_over_forward": (ms_f + ms_b) / ms_f,
+                     "pairs": pairs, "n_data": int(d["xyz"].shape[0]), "n_rand": int(r["xyz"].shape[0])})
+    line["steps"], line["warmup"] = args.steps, args.warmup
+    print(json.dumps(line))
+    ctx.close()
 
 
 def dist_setup():
@@ -294,6 +421,9 @@ def main():
     args = parse()
     if args.one_count:
         one_count(args)
+        return
+    if args.workload != "survey":
+        other_workload(args)
         return
     ws, rank, local = dist_setup()
     if args.impl == "reference":
