@@ -129,6 +129,7 @@ struct KParams {
     const long long *a_masks, *b_masks;  // original catalogue bitmasks, object-major
     const long long *a_dmasks, *b_dmasks;  // dither masks (dither != 0), same layout
     int n_mask;
+    int mask_vec2; // masks read 16 bytes at a time (even n_mask, 16-byte aligned arrays)
     int dither;    // _USE_DITHER_WEIGHTS: popc of the dither masks replaces n_runs
     int los_mid;   // pi along x1 + x2 (src/correlators.cpp:172-182), exact path only
     float n_runs_f;
@@ -413,6 +414,25 @@ __device__ __forceinline__ double upweight(const KParams &P, double v) {
 //   W_INVP_DR  (float)((w1 w2) interp(1-cos))         (:184-189)
 //   W_ANG_INVP (iw1 iw2) (n_runs / popc), float division (:742-764)
 // popc = float sum of the popcounts of mask1 & mask2, plus 1 when zero.
+// Sum over the mask words of popc(m1 & m2): exact integer work, read 16
+// bytes at a time where the rows allow it (half the load instructions and
+// L1 requests of word-by-word loads).
+__device__ __forceinline__ int and_popc(const long long *m1, const long long *m2, int n, int vec2) {
+    int c = 0;
+    if (vec2) {
+        const longlong2 *a = reinterpret_cast<const longlong2 *>(m1);
+        const longlong2 *b = reinterpret_cast<const longlong2 *>(m2);
+#pragma unroll 4
+        for (int k = 0; k < n / 2; ++k) {
+            const longlong2 x = __ldg(a + k), y = __ldg(b + k);
+            c += __popcll((unsigned long long)(x.x & y.x)) + __popcll((unsigned long long)(x.y & y.y));
+        }
+    } else {
+        for (int k = 0; k < n; ++k) c += __popcll((unsigned long long)(__ldg(m1 + k) & __ldg(m2 + k)));
+    }
+    return c;
+}
+
 template <int WK>
 __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, float wprod, int i, int j) {
     auto omct = [&]() {
@@ -422,8 +442,7 @@ __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, fl
     if (WK == W_INVP_DR) return __double2float_rn(__dmul_rn((double)wprod, upweight(P, omct())));
     const long long *m1 = P.a_masks + (size_t)i * P.n_mask;
     const long long *m2 = P.b_masks + (size_t)j * P.n_mask;
-    int c = 0;
-    for (int k = 0; k < P.n_mask; ++k) c += __popcll((unsigned long long)(__ldg(m1 + k) & __ldg(m2 + k)));
+    const int c = and_popc(m1, m2, P.n_mask, P.mask_vec2);
     float pw = (float)c;  // exact: at most 64 * kMaxMaskInts
     if (pw < 0.5f) pw += 1.0f;
     // numerator: n_runs, or with _USE_DITHER_WEIGHTS the same float popcount
@@ -432,8 +451,7 @@ __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, fl
     if (P.dither) {
         const long long *d1 = P.a_dmasks + (size_t)i * P.n_mask;
         const long long *d2 = P.b_dmasks + (size_t)j * P.n_mask;
-        int dc = 0;
-        for (int k = 0; k < P.n_mask; ++k) dc += __popcll((unsigned long long)(__ldg(d1 + k) & __ldg(d2 + k)));
+        const int dc = and_popc(d1, d2, P.n_mask, P.mask_vec2);
         num = (float)dc;
         if (num < 0.5f) num += 1.0f;
     }
@@ -1578,6 +1596,9 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         P.a_dmasks = A->dmasks.p;
         P.b_dmasks = B->dmasks.p;
     }
+    auto al16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
+    P.mask_vec2 = (P.n_mask % 2 == 0) && al16(P.a_masks) && al16(P.b_masks) &&
+                  (!P.dither || (al16(P.a_dmasks) && al16(P.b_dmasks)));
     C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
     return 0;
 }
