@@ -129,7 +129,7 @@ struct KParams {
     const long long *a_masks, *b_masks;  // original catalogue bitmasks, object-major
     const long long *a_dmasks, *b_dmasks;  // dither masks (dither != 0), same layout
     int n_mask;
-    int mask_vec2; // masks read 16 bytes at a time (even n_mask, 16-byte aligned arrays)
+    int mask_vec;  // mask words per load: 4 (n_mask % 4 == 0, 32-byte aligned), 2 (even, 16-byte aligned) or 1
     int dither;    // _USE_DITHER_WEIGHTS: popc of the dither masks replaces n_runs
     int los_mid;   // pi along x1 + x2 (src/correlators.cpp:172-182), exact path only
     float n_runs_f;
@@ -414,12 +414,26 @@ __device__ __forceinline__ double upweight(const KParams &P, double v) {
 //   W_INVP_DR  (float)((w1 w2) interp(1-cos))         (:184-189)
 //   W_ANG_INVP (iw1 iw2) (n_runs / popc), float division (:742-764)
 // popc = float sum of the popcounts of mask1 & mask2, plus 1 when zero.
-// Sum over the mask words of popc(m1 & m2): exact integer work, read 16
-// bytes at a time where the rows allow it (half the load instructions and
-// L1 requests of word-by-word loads).
-__device__ __forceinline__ int and_popc(const long long *m1, const long long *m2, int n, int vec2) {
+// 32-byte read-only load of four mask words (sm_100 vector load).
+__device__ __forceinline__ void ldg_u64x4(const long long *p, unsigned long long &a, unsigned long long &b,
+                                          unsigned long long &c, unsigned long long &d) {
+    asm("ld.global.nc.v4.u64 {%0, %1, %2, %3}, [%4];" : "=l"(a), "=l"(b), "=l"(c), "=l"(d) : "l"(p));
+}
+
+// Sum over the mask words of popc(m1 & m2): exact integer work, read 32 or
+// 16 bytes at a time where the rows allow it (a quarter or half of the load
+// instructions and L1 requests of word-by-word loads).
+__device__ __forceinline__ int and_popc(const long long *m1, const long long *m2, int n, int vec) {
     int c = 0;
-    if (vec2) {
+    if (vec == 4) {
+#pragma unroll 2
+        for (int k = 0; k < n; k += 4) {
+            unsigned long long a0, a1, a2, a3, b0, b1, b2, b3;
+            ldg_u64x4(m1 + k, a0, a1, a2, a3);
+            ldg_u64x4(m2 + k, b0, b1, b2, b3);
+            c += __popcll(a0 & b0) + __popcll(a1 & b1) + __popcll(a2 & b2) + __popcll(a3 & b3);
+        }
+    } else if (vec == 2) {
         const longlong2 *a = reinterpret_cast<const longlong2 *>(m1);
         const longlong2 *b = reinterpret_cast<const longlong2 *>(m2);
 #pragma unroll 4
@@ -442,7 +456,7 @@ __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, fl
     if (WK == W_INVP_DR) return __double2float_rn(__dmul_rn((double)wprod, upweight(P, omct())));
     const long long *m1 = P.a_masks + (size_t)i * P.n_mask;
     const long long *m2 = P.b_masks + (size_t)j * P.n_mask;
-    const int c = and_popc(m1, m2, P.n_mask, P.mask_vec2);
+    const int c = and_popc(m1, m2, P.n_mask, P.mask_vec);
     float pw = (float)c;  // exact: at most 64 * kMaxMaskInts
     if (pw < 0.5f) pw += 1.0f;
     // numerator: n_runs, or with _USE_DITHER_WEIGHTS the same float popcount
@@ -451,7 +465,7 @@ __device__ __forceinline__ float pair_weight(const KParams &P, const JobK &J, fl
     if (P.dither) {
         const long long *d1 = P.a_dmasks + (size_t)i * P.n_mask;
         const long long *d2 = P.b_dmasks + (size_t)j * P.n_mask;
-        const int dc = and_popc(d1, d2, P.n_mask, P.mask_vec2);
+        const int dc = and_popc(d1, d2, P.n_mask, P.mask_vec);
         num = (float)dc;
         if (num < 0.5f) num += 1.0f;
     }
@@ -1596,9 +1610,13 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         P.a_dmasks = A->dmasks.p;
         P.b_dmasks = B->dmasks.p;
     }
-    auto al16 = [](const void *q) { return ((uintptr_t)q & 15u) == 0; };
-    P.mask_vec2 = (P.n_mask % 2 == 0) && al16(P.a_masks) && al16(P.b_masks) &&
-                  (!P.dither || (al16(P.a_dmasks) && al16(P.b_dmasks)));
+    // widest mask load every row start allows (row stride n_mask words)
+    auto aligned = [&](uintptr_t a) {
+        const uintptr_t q = (uintptr_t)P.a_masks | (uintptr_t)P.b_masks |
+                            (P.dither ? ((uintptr_t)P.a_dmasks | (uintptr_t)P.b_dmasks) : 0);
+        return (q & (a - 1)) == 0;
+    };
+    P.mask_vec = (P.n_mask % 4 == 0 && aligned(32)) ? 4 : ((P.n_mask % 2 == 0 && aligned(16)) ? 2 : 1);
     C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
     return 0;
 }
