@@ -97,14 +97,14 @@ int tpcf_synchronize(tpcf_ctx *ctx);
 int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const double *x_norm, const double *d_comov,
                         const float *weight, const float *input_weight, const int32_t *jk_region,
                         int32_t n_jk_regions, const int64_t *bitmask, int32_t n_mask_ints, tpcf_catalog **out);
-/* Device arrays go back to the context's memory pool in the order of the
- * context's stream while the context lives (on the legacy stream after it is
- * destroyed; a catalogue may outlive its context). */
+/* Device arrays go back to the memory pool in the order of the legacy stream
+ * (a catalogue may outlive its context and the context's stream). */
 int tpcf_catalog_destroy(tpcf_catalog *cat);
 /* Points kept by the d_comov partition (GalaxyBoxes::n_gals). */
 int64_t tpcf_catalog_n_used(const tpcf_catalog *cat);
-/* Drop the cell grids cached on the catalogue; the next count rebuilds them
- * (their memory is released as in tpcf_catalog_destroy). */
+/* Drop the cell grids cached on the catalogue; the next count rebuilds them.
+ * While the catalogue's context lives, their memory is released in the order
+ * of the context's stream, which must still be valid (tpcf_set_stream). */
 int tpcf_catalog_release_cache(tpcf_catalog *cat);
 
 /* Histogram definition.  ax2 is the pi axis for TPCF_SIGMA_PI and supplies

@@ -311,8 +311,7 @@ int tpcf_catalog_create(tpcf_ctx *ctx, int64_t n, const double *xyz, const doubl
 
 int tpcf_catalog_destroy(tpcf_catalog *cat) {
     if (!cat) return TPCF_E_INVALID_ARG;
-    cat->c.release_device();
-    delete cat;
+    delete cat;  // arrays released on the legacy stream (valid whatever became of the context's stream)
     return TPCF_OK;
 }
 

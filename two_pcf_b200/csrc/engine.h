@@ -201,22 +201,9 @@ struct Catalog {
     std::vector<int> h_jk;
     std::vector<int> h_kept;
     std::map<std::string, std::unique_ptr<Grid>> grids;  // cached by geometry
-    // Release every device array: on the context's stream while the context
-    // lives (its next allocations reuse the memory in stream order), else on
-    // the legacy stream.
-    void release_device() {
-        const cudaStream_t s = ctx_alive.expired() ? (cudaStream_t)0 : ctx->stream;
-        for (auto &kv : grids) kv.second->release_on(s);
-        grids.clear();
-        xyz.release_on(s);
-        unit.release_on(s);
-        w.release_on(s);
-        iw.release_on(s);
-        jk.release_on(s);
-        masks.release_on(s);
-        dmasks.release_on(s);
-        kept.release_on(s);
-    }
+    // Drop the cached grids: on the context's stream while the context lives
+    // (its next grid builds reuse the memory in stream order), else on the
+    // legacy stream.
     void release_grids() {
         const cudaStream_t s = ctx_alive.expired() ? (cudaStream_t)0 : ctx->stream;
         for (auto &kv : grids) kv.second->release_on(s);
