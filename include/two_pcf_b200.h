@@ -193,9 +193,12 @@ int tpcf_pair_count_weighted(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_ca
  * tpcf_count (unordered pairs, before x2).  Every counted pair (i, j) in bin
  * k adds w_j * dL_dfull[k] to dL_dw_a[i] and w_i * dL_dfull[k] to dL_dw_b[j]
  * (auto counts: both to dL_dw_a).  Outputs are indexed by catalogue index
- * (n points each; points dropped by the d_comov partition get 0) and summed
- * in double.  Bin membership is the forward count's, decided by the same
- * kernels; no pair is stored between the two passes. */
+ * (n points each; points dropped by the d_comov partition get 0).  Terms
+ * are summed in 64-bit fixed point per work item (resolution about 1e-15 of
+ * max|dL_dfull| * max weight times the item's points), the item sums in
+ * double.  dL_dfull must be finite (else TPCF_E_INVALID_ARG).  Bin membership
+ * is the forward count's, decided by the same kernels; no pair is stored
+ * between the two passes. */
 int tpcf_count_backward(tpcf_ctx *ctx, const tpcf_catalog *a, const tpcf_catalog *b, const tpcf_binning *bin,
                         int precision, const double *dL_dfull, double *dL_dw_a, double *dL_dw_b,
                         tpcf_stats *stats);

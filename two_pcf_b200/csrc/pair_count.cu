@@ -144,6 +144,7 @@ struct KParams {
     // indexed by catalogue index (grad_b == grad_a for auto counts)
     const double *adj_G;
     double *grad_a, *grad_b;
+    double adj_scale, adj_inv;  // gradient terms are summed as round(term * adj_scale) in 64-bit fixed point
 };
 
 // Shared-memory views the binning steps use.
@@ -152,7 +153,8 @@ struct Shm {
     const unsigned char *l1, *l2;  // lookup tables
     uint32_t *lo, *hi;             // 64-bit fixed-point histogram as two 32-bit words per bin
     const double *G;               // adjoint: dL/d(full histogram) (aliases lo/hi)
-    double *ga, *gb;               // adjoint: gradient sums of the A chunk and of the B tile
+    uint32_t *ga_lo, *ga_hi;       // adjoint: fixed-point gradient sums of the A chunk (two words per point)
+    uint32_t *gb_lo, *gb_hi;       // and of the B tile
 };
 
 struct SmemLayout {
@@ -188,7 +190,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o += (size_t)NWARP * kQueueCap * 16;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
     if (!exact) o += (size_t)TA * 16;
-    L.ga = o;      // adjoint: per-point gradient sums (double)
+    L.ga = o;      // adjoint: per-point gradient sums (64-bit fixed point as two 32-bit words)
     if (adj) o += (size_t)TA * 8;
     L.gb = o;
     if (adj) o += (size_t)TB * 8;
@@ -493,8 +495,8 @@ __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, cons
     if constexpr (WK == W_ADJ) {
         // the pair adds wa * wb to its bin: dL/dwa += G wb, dL/dwb += G wa
         const double g = S.G[bin];
-        atomicAdd(&S.ga[ka], g * (double)wb);
-        atomicAdd(&S.gb[jl], g * (double)wa);
+        dev::acc_add(S.ga_lo, S.ga_hi, ka, __double2ll_rn(g * (double)wb * P.adj_scale));
+        dev::acc_add(S.gb_lo, S.gb_hi, jl, __double2ll_rn(g * (double)wa * P.adj_scale));
         return;
     }
     float w = UNITW ? 1.0f : __fmul_rn(wa, wb);
@@ -707,14 +709,15 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4 *s_q = (float4 *)(smem + L.queue) + warp * kQueueCap;
     const unsigned lt_mask = (1u << lane) - 1u;
-    const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo), (double *)(smem + L.ga),
-                (double *)(smem + L.gb)};
+    const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo),
+                (uint32_t *)(smem + L.ga), (uint32_t *)(smem + L.ga) + TA,
+                (uint32_t *)(smem + L.gb), (uint32_t *)(smem + L.gb) + TB};
 
     if (ADJ) {
         // the histogram words hold dL/d(full histogram) instead
         for (int i = tid; i < P.nb; i += NT) ((double *)(smem + L.lo))[i] = P.adj_G[i];
-        for (int i = tid; i < TA; i += NT) S.ga[i] = 0.0;
-        for (int i = tid; i < TBK; i += NT) S.gb[i] = 0.0;
+        for (int i = tid; i < TA; i += NT) S.ga_lo[i] = S.ga_hi[i] = 0u;
+        for (int i = tid; i < TB; i += NT) S.gb_lo[i] = S.gb_hi[i] = 0u;
     } else {
         for (int i = tid; i < P.nb; i += NT) {
             s_lo[i] = 0;
@@ -1034,9 +1037,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     __syncthreads();
                     const int jb0 = sg.b_start + tstart;
                     for (int t2 = tid; t2 < tlen; t2 += NT) {
-                        const double v = S.gb[t2];
-                        if (v != 0.0) atomicAdd(&P.grad_b[J.b.idx[jb0 + t2]], v);
-                        S.gb[t2] = 0.0;
+                        const long long q = (long long)(((unsigned long long)S.gb_hi[t2] << 32) | S.gb_lo[t2]);
+                        if (q != 0) atomicAdd(&P.grad_b[J.b.idx[jb0 + t2]], (double)q * P.adj_inv);
+                        S.gb_lo[t2] = S.gb_hi[t2] = 0u;
                     }
                     __syncthreads();
                 }
@@ -1078,9 +1081,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         // ---- adjoint: the A chunk's gradients to their points
         if constexpr (ADJ) {
             for (int k = tid; k < it.a_len; k += NT) {
-                const double v = S.ga[k];
-                if (v != 0.0) atomicAdd(&P.grad_a[J.a.idx[it.a_start + k]], v);
-                S.ga[k] = 0.0;
+                const long long q = (long long)(((unsigned long long)S.ga_hi[k] << 32) | S.ga_lo[k]);
+                if (q != 0) atomicAdd(&P.grad_a[J.a.idx[it.a_start + k]], (double)q * P.adj_inv);
+                S.ga_lo[k] = S.ga_hi[k] = 0u;
             }
             __syncthreads();
         }
@@ -1368,6 +1371,7 @@ struct CountPlan {
     int n_a = 0, n_b = 0;  // catalogue sizes (adjoint outputs)
     const double *adj_G_host = nullptr;
     double *grad_a_host = nullptr, *grad_b_host = nullptr;
+    double adj_scale = 1.0, adj_inv = 1.0;
     double inv = 1.0;  // 2^-S
     int scale_exp = 0;  // S
     long long *raw_out = nullptr;  // partial sums of a shard (kPartialWords per slot)
@@ -1560,6 +1564,32 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     if (grids_only) return 0;
     build_work_items(*ga, *gb, C.is_auto, m, side, rb, C.items, C.segs);
 
+    if (C.adj) {
+        // Fixed point of the gradient sums: an A point's sum takes one term
+        // G[bin] w_b per B point of its item, a B point's tile sum one term
+        // G[bin] w_a per A point of the chunk; the larger bound of the two
+        // gets 2^62, so no 64-bit sum can overflow, and a term is resolved to
+        // 2^-S (about 1e-15 of max|G| max w times the item's B points).
+        double gmax = 0.0;
+        for (int b = 0; b < C.nb; ++b) {
+            if (!std::isfinite(C.adj_G_host[b])) {
+                err->status = 1;
+                err->msg = "dL/d(full histogram) must be finite";
+                return err->status;
+            }
+            gmax = std::max(gmax, std::fabs(C.adj_G_host[b]));
+        }
+        long long nb_max = 1;
+        for (const WorkItem &w : C.items) {
+            long long bl = 0;
+            for (int k = w.seg_begin; k < w.seg_end; ++k) bl += C.segs[k].b_len;
+            nb_max = std::max(nb_max, bl);
+        }
+        const double bound = gmax * std::max((double)B->w_max * (double)nb_max, (double)A->w_max * (double)TA);
+        const int S = bound > 0 ? std::max(-1000, std::min(1000, (int)std::floor(62.0 - std::log2(bound)))) : 0;
+        C.adj_scale = std::ldexp(1.0, S);
+        C.adj_inv = std::ldexp(1.0, -S);
+    }
     float wscale = 1.0f;
     if (!C.unitw && !C.adj) {
         double wmax = wmax_of(A) * wmax_of(B);
@@ -1723,6 +1753,8 @@ int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Erro
     P.up_bins = D.up_bins;
     P.up_centre = D.up_centre;
     P.adj_G = D.adj_G;
+    P.adj_scale = C.adj_scale;
+    P.adj_inv = C.adj_inv;
     P.grad_a = D.grad_a;
     P.grad_b = C.is_auto ? D.grad_a : D.grad_b;
 
