@@ -152,6 +152,19 @@ def test_backward_matches_oracle_adjoint(ctx, setup, auto, precision):
     assert st["in_range"] > 0
 
 
+def test_backward_rejects_nonfinite_histogram_gradient(ctx, setup):
+    """The gradient terms are summed in fixed point scaled by max|dL/dfull|:
+    a non-finite entry is refused before any launch."""
+    s = setup
+    G = np.ones(s["b"].nb)
+    G[3] = np.nan
+    with pytest.raises(tp.TpcfError):
+        tp.count_backward(ctx, s["D"], None, s["b"], G)
+    G[3] = np.inf
+    with pytest.raises(tp.TpcfError):
+        tp.count_backward(ctx, s["D"], s["R"], s["b"], G)
+
+
 def test_weight_gradient_vs_fp64_cpu_and_finite_differences(ctx, setup):
     s = setup
     rng = np.random.default_rng(5)
