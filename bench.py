@@ -79,7 +79,7 @@ def one_count(args):
 
 
 def other_workload(args):
-    """The spec's other workloads on one GPU, each one JSON line (FP32+guard
+    """The other survey workloads on one GPU, each one JSON line (FP32+guard
     path, device time from CUDA events, median of --steps after --warmup):
 
     mocks   -- 64 Neyman-Scott mocks in a 1000 Mpc/h box (sizes uniform on
