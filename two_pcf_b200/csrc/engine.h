@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 #include <map>
 #include <memory>
 #include <string>
@@ -36,6 +37,13 @@ struct DevBuf {
         return e;
     }
 };
+
+// TPCF_TRACE set (and not "0"): count_many and the grid builds print their
+// timelines on stderr.
+inline bool trace_enabled() {
+    const char *e = std::getenv("TPCF_TRACE");
+    return e && e[0] && e[0] != '0';
+}
 
 struct Error {
     int status;

@@ -282,8 +282,7 @@ int build_grid(Ctx *ctx, Catalog *cat, const GridSpec &spec, bool want_fp64, Gri
     const bool subset_kept = spec.subset_kept;
     cudaStream_t st = ctx->stream;
     // TPCF_TRACE=1: host time of the build's phases on stderr (diagnostics)
-    const char *tr_env = std::getenv("TPCF_TRACE");
-    const bool trace = tr_env && tr_env[0] && tr_env[0] != '0';
+    const bool trace = trace_enabled();
     using clk = std::chrono::steady_clock;
     const auto t0 = clk::now();
     auto ms_since = [&](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };

@@ -2023,8 +2023,7 @@ int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs, const std::v
     // TPCF_TRACE=1: one stderr line per count with its host planning time
     // and where its kernel ran on the device, in ms from the call's start
     // (diagnostics of the pipelining; the counts are unchanged)
-    const char *tr_env = std::getenv("TPCF_TRACE");
-    const bool trace = tr_env && tr_env[0] && tr_env[0] != '0';
+    const bool trace = trace_enabled();
     using clk = std::chrono::steady_clock;
     const auto h0 = clk::now();
     auto host_ms = [&](clk::time_point a) { return std::chrono::duration<double, std::milli>(clk::now() - a).count(); };
