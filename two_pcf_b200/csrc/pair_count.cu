@@ -1089,6 +1089,16 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
         }
     }
 
+    // ---- a copy can still be in flight only after a wait gave up (the
+    // results are discarded then): give the last copy into each buffer a
+    // bounded wait before the CTA's shared memory is released
+    if (tid == 0) {
+        for (unsigned b = 0; b < (unsigned)NB && b < tcount; ++b) {
+            const unsigned t_last = (tcount - 1) - ((tcount - 1 - b) % NB);  // last tile staged in buffer b
+            dev::mbar_wait_bounded(&bar[b], (t_last / NB) & 1u, kWaitLimit);
+        }
+    }
+
     // ---- merge the privatised histogram
     __syncthreads();
     if (!JK && !ADJ) {
