@@ -361,6 +361,14 @@ double tpcf_ls_estimator(double dd, double dr, double rr);
 uint64_t tpcf_kernel_launches(const tpcf_ctx *ctx);
 int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s);
 
+/* Self-test of the device give-up path (no counterpart in the reference): one
+ * kernel runs the pair kernels' bounded wait on a shared-memory barrier.  With
+ * arrive != 0 the barrier is completed first and the call returns TPCF_OK;
+ * with arrive == 0 nothing ever completes it, the wait gives up after `limit`
+ * tries and the call returns TPCF_E_DEVICE_TIMEOUT, leaving the context
+ * usable.  limit == 0: TPCF_E_INVALID_ARG. */
+int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit);
+
 /* ---------------------------------------------------------------------------
  * The command-line flow around the counts (src/main.cpp:11-84): parameter
  * file, redshift -> comoving distance, catalogue reader, result writers.

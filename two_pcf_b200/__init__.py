@@ -386,6 +386,13 @@ def upweight_eval(weights: Weights, values) -> np.ndarray:
     return out
 
 
+def wait_selftest(ctx: Context, arrive: bool, limit: int = 1000) -> int:
+    """The device give-up path (tpcf_wait_selftest): the pair kernels' bounded
+    wait on a barrier that is completed first (arrive) or never; returns the
+    status, TPCF_OK or TPCF_E_DEVICE_TIMEOUT (the context stays usable)."""
+    return int(_capi.lib().tpcf_wait_selftest(ctx._h, int(bool(arrive)), int(limit)))
+
+
 def count_backward(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning, dL_dfull,
                    precision: int = FP32_GUARD):
     """Adjoint of count(): per-point dL/dw of a and b (b None: auto count,

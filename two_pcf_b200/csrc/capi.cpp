@@ -921,4 +921,18 @@ int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_
     return TPCF_OK;
 }
 
+int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit) {
+    if (!ctx || limit == 0) return TPCF_E_INVALID_ARG;
+    cudaError_t e = cudaSetDevice(ctx->c.device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "set device");
+    tpcf::Error err{0, ""};
+    int status = -1;
+    int rc = tpcf::wait_selftest(&ctx->c, arrive ? 1 : 0, limit, &status, &err);
+    if (rc) return fail(ctx, rc, err.msg);
+    ++ctx->c.launches;
+    if (status == 4) return fail(ctx, TPCF_E_DEVICE_TIMEOUT, "device wait exceeded its iteration limit (self-test)");
+    if (status != 0) return fail(ctx, TPCF_E_CUDA, "self-test kernel reported no status");
+    return TPCF_OK;
+}
+
 }  // extern "C"

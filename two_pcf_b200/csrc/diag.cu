@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "engine.h"
+#include "pair_kernels.cuh"
 
 namespace tpcf {
 namespace {
@@ -53,7 +54,46 @@ __global__ void smem_atomic_kernel(unsigned long long *out, int iters) {
     atomicAdd(out, s);
 }
 
+// The pair kernels' bounded wait on a shared-memory mbarrier (count 1):
+// with `arrive` thread 0 completes the phase first and the wait succeeds;
+// without it nothing ever arrives and the wait gives up after `limit` tries.
+// One thread reports the outcome: 0 done, 4 gave up (TPCF_E_DEVICE_TIMEOUT).
+__global__ void wait_selftest_kernel(int arrive, unsigned limit, int *status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        dev::mbar_init(&bar, 1);
+        dev::mbar_init_fence();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && arrive) {
+        asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(dev::smem_u32(&bar)) : "memory");
+    }
+    __syncthreads();
+    const bool ok = dev::mbar_wait_bounded(&bar, 0u, limit);
+    if (threadIdx.x == 0) *status = ok ? 0 : 4;
+}
+
 }  // namespace
+
+int wait_selftest(Ctx *ctx, int arrive, unsigned limit, int *device_status, Error *err) {
+    DevBuf<int> st;
+    if (st.alloc(1) != cudaSuccess) {
+        err->status = 2;
+        err->msg = "allocation failed";
+        return err->status;
+    }
+    cudaMemsetAsync(st.p, 0xff, sizeof(int), ctx->stream);
+    wait_selftest_kernel<<<1, 32, 0, ctx->stream>>>(arrive, limit, st.p);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(device_status, st.p, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) {
+        err->status = 3;
+        err->msg = cudaGetErrorString(e);
+        return err->status;
+    }
+    return 0;
+}
 
 int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err) {
     cudaStream_t st = ctx->stream;

@@ -349,5 +349,6 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
 
 // diag.cu
 int measure_peaks(Ctx *ctx, double *fp32_tflops, double *smem_atomics_per_s, Error *err);
+int wait_selftest(Ctx *ctx, int arrive, unsigned limit, int *device_status, Error *err);
 
 }  // namespace tpcf
