@@ -4,6 +4,13 @@ include/two_pcf_b200.h) for sm_100a only, plus the command-line driver.
 Host C++ is compiled with -ffp-contract=off: the threshold tables and the
 cosmology table must round every float/double operation once, like the
 reference's x86-64 build.
+
+TPCF_SANITIZE=1 builds the host C++ with AddressSanitizer and
+UndefinedBehaviorSanitizer instead (objects in lib/obj-sanitize; the library
+is relinked whenever the mode changes).  Python is not instrumented, so run
+with the runtime preloaded, e.g.
+  LD_PRELOAD=$(gcc -print-file-name=libasan.so) ASAN_OPTIONS=detect_leaks=0 \
+      python -m pytest tests -m "not gpu"
 """
 from __future__ import annotations
 
@@ -17,8 +24,11 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB_DIR = os.path.join(PKG, "lib")
-BUILD_DIR = os.path.join(PKG, "lib", "obj")
+SANITIZE = os.environ.get("TPCF_SANITIZE", "") == "1"
+BUILD_DIR = os.path.join(PKG, "lib", "obj-sanitize" if SANITIZE else "obj")
 LIB_PATH = os.path.join(LIB_DIR, "libtpcf_b200.so")
+MODE_STAMP = os.path.join(LIB_DIR, ".build_mode")
+SAN_FLAGS = ["-fsanitize=address,undefined", "-fno-omit-frame-pointer", "-g"]
 
 CUDA_HOME = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA_HOME, "bin", "nvcc")
@@ -66,17 +76,26 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         obj = os.path.join(BUILD_DIR, f + ".o")
         objs.append(obj)
         if _stale(obj, [src] + headers):
-            jobs.append([CXX, "-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fopenmp", "-I", CSRC,
+            jobs.append([CXX, *(["-O1", *SAN_FLAGS] if SANITIZE else ["-O2"]), "-std=c++17", "-fPIC",
+                         "-ffp-contract=off", "-fopenmp", "-I", CSRC,
                          "-I", os.path.join(CUDA_HOME, "include"), "-c", src, "-o", obj])
     with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as ex:
         outs = list(ex.map(_run, jobs))
     if verbose:
         for o in outs:
             sys.stdout.write(o)
-    if jobs or not os.path.exists(LIB_PATH):
+    mode = "sanitize" if SANITIZE else "release"
+    last_mode = open(MODE_STAMP).read().strip() if os.path.exists(MODE_STAMP) else "release"
+    if jobs or not os.path.exists(LIB_PATH) or mode != last_mode:
         tmp = LIB_PATH + ".tmp"
-        _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static", "-lgomp"])
+        if SANITIZE:
+            _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC,-fsanitize=address,-fsanitize=undefined", *objs,
+                  "-o", tmp, "-lcudart_static", "-lgomp", "-lasan", "-lubsan"])
+        else:
+            _run([NVCC, *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", tmp, "-lcudart_static", "-lgomp"])
         shutil.move(tmp, LIB_PATH)
+        with open(MODE_STAMP, "w") as f:
+            f.write(mode + "\n")
     cli_src = os.path.join(CSRC, CLI_SOURCE)
     if _stale(CLI_PATH, [cli_src, LIB_PATH] + headers):
         tmp = CLI_PATH + ".tmp"
