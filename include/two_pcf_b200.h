@@ -369,6 +369,13 @@ int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_
  * usable.  limit == 0: TPCF_E_INVALID_ARG. */
 int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit);
 
+/* Fault injection for the allocation error paths (no counterpart in the
+ * reference; process-wide, for tests): after `after` more successful device
+ * allocations of catalogues, cell grids and per-call scratch, every further
+ * one fails as out of memory until this is called with after < 0.  The
+ * failing call returns an error status and releases what it had allocated. */
+int tpcf_debug_fail_allocations(int64_t after);
+
 /* ---------------------------------------------------------------------------
  * The command-line flow around the counts (src/main.cpp:11-84): parameter
  * file, redshift -> comoving distance, catalogue reader, result writers.

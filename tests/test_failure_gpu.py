@@ -31,3 +31,52 @@ def test_bounded_wait_gives_up_and_the_context_stays_usable(ctx):
 
 def test_zero_limit_is_refused(ctx):
     assert tp.wait_selftest(ctx, arrive=True, limit=0) == _capi.TPCF_E_INVALID_ARG
+
+
+def _survey_pair(ctx, seed, n_data, n_rand):
+    from two_pcf_b200 import synthetic
+    w = synthetic.survey_catalogue(seed=seed, n_data=n_data, n_rand=n_rand)
+    d, r = w["data"], w["rand"]
+    D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], w["n_jk"])
+    R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
+    return w, D, R
+
+
+def test_allocation_failures_return_status_and_leave_the_context_usable(ctx):
+    """Every device allocation of a catalogue, a cell grid or a count's
+    scratch made to fail in turn (tpcf_debug_fail_allocations): the call
+    fails with TPCF_E_OOM, and once the injection is off the same counts come
+    out exactly as before."""
+    lib = _capi.lib()
+    w, D, R = _survey_pair(ctx, 31, 3000, 9000)
+    b = tp.Binning(ctx, tp.S_MU, (0.0, 100.0, 1.3, 40), (0.0, 1.0, 0.0, 50), w["n_jk"])
+    jobs = [(D, None, b), (D, R, b), (R, None, b)]
+    for c in (D, R):
+        lib.tpcf_catalog_release_cache(c._h)
+    ref = tp.count_many(ctx, jobs)
+    try:
+        failed = 0
+        for after in range(0, 40):
+            for c in (D, R):
+                lib.tpcf_catalog_release_cache(c._h)
+            lib.tpcf_debug_fail_allocations(after)
+            try:
+                tp.count_many(ctx, jobs)
+            except tp.TpcfError as ex:
+                assert ex.status == _capi.TPCF_E_OOM, ex
+                failed += 1
+            finally:
+                lib.tpcf_debug_fail_allocations(-1)
+        assert failed > 5
+        lib.tpcf_debug_fail_allocations(0)
+        with pytest.raises(tp.TpcfError) as exc:
+            tp.Catalog(ctx, np.zeros((10, 3)) + 5.0)
+        assert exc.value.status == _capi.TPCF_E_OOM
+    finally:
+        lib.tpcf_debug_fail_allocations(-1)
+    for c in (D, R):
+        lib.tpcf_catalog_release_cache(c._h)
+    again = tp.count_many(ctx, jobs)
+    for (f, r, _), (f1, r1, _) in zip(ref, again):
+        assert np.array_equal(f, f1)
+        assert np.array_equal(r, r1)

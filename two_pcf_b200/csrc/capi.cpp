@@ -921,6 +921,11 @@ int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_
     return TPCF_OK;
 }
 
+int tpcf_debug_fail_allocations(int64_t after) {
+    tpcf::alloc_fail_budget().store(after < 0 ? -1 : (long long)after);
+    return TPCF_OK;
+}
+
 int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit) {
     if (!ctx || limit == 0) return TPCF_E_INVALID_ARG;
     cudaError_t e = cudaSetDevice(ctx->c.device);

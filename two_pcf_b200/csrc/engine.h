@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <map>
@@ -37,6 +38,23 @@ struct DevBuf {
         return e;
     }
 };
+
+// Injected allocation failure (tpcf_debug_fail_allocations): while the
+// budget is >= 0, each device allocation of the engine's pool-backed buffers
+// takes one from it and fails once it is exhausted.  -1: off.
+inline std::atomic<long long> &alloc_fail_budget() {
+    static std::atomic<long long> budget{-1};
+    return budget;
+}
+inline bool alloc_injected_failure() {
+    auto &b = alloc_fail_budget();
+    long long v = b.load(std::memory_order_relaxed);
+    while (v >= 0) {
+        if (v == 0) return true;
+        if (b.compare_exchange_weak(v, v - 1, std::memory_order_relaxed)) return false;
+    }
+    return false;
+}
 
 // TPCF_TRACE set (and not "0"): count_many and the grid builds print their
 // timelines on stderr.
@@ -93,6 +111,7 @@ struct ScratchBuf {
         release();
         if (count == 0) count = 1;
         s = ctx.stream;
+        if (alloc_injected_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = ctx.pool ? cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), ctx.pool, s)
                                  : cudaMallocAsync((void **)&p, count * sizeof(T), s);
         if (e == cudaSuccess) n = count;
@@ -136,6 +155,7 @@ struct PoolBuf {
         release();
         if (count == 0) count = 1;
         device = ctx.device;
+        if (alloc_injected_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = ctx.pool ? cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), ctx.pool, ctx.stream)
                                  : cudaMallocAsync((void **)&p, count * sizeof(T), ctx.stream);
         if (e == cudaSuccess) n = count;

@@ -250,7 +250,7 @@ __global__ void reweight_kernel(int n, const int *__restrict__ idx, const float 
     do {                                                                                 \
         cudaError_t _e = (expr);                                                         \
         if (_e != cudaSuccess) {                                                         \
-            err->status = 3;                                                             \
+            err->status = (_e == cudaErrorMemoryAllocation) ? 2 : 3;                     \
             err->msg = std::string("CUDA error in grid build: ") + cudaGetErrorString(_e); \
             return err->status;                                                          \
         }                                                                                \
