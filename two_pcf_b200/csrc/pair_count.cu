@@ -55,7 +55,14 @@ constexpr int kTileMax = TB > TB_EXACT ? TB : TB_EXACT;
 constexpr int NBUF = 3;
 constexpr int NBUF_EXACT = 2;
 constexpr int kNbufMax = NBUF > NBUF_EXACT ? NBUF : NBUF_EXACT;
-__host__ __device__ constexpr int n_buffers(bool exact) { return exact ? NBUF_EXACT : NBUF; }
+// Count kernels without jackknife regions keep the lighter settings (two
+// buffers, a push width of 2) so that their shared memory allows three CTAs
+// per SM (the adjoint runs two CTAs per SM either way and keeps the others).
+constexpr int NBUF_NOJK = 2;
+__host__ __device__ constexpr bool light_fast(bool exact, bool jk, bool adj) { return !exact && !jk && !adj; }
+__host__ __device__ constexpr int n_buffers(bool exact, bool jk, bool adj) {
+    return exact ? NBUF_EXACT : (light_fast(exact, jk, adj) ? NBUF_NOJK : NBUF);
+}
 // queue entries pack (A chunk index << kTileShift | tile index)
 constexpr int kTileShift = kTileMax <= 256 ? 8 : (kTileMax <= 512 ? 9 : 10);
 constexpr int kTileMask = (1 << kTileShift) - 1;
@@ -64,9 +71,13 @@ static_assert(16 + 12 * kNbufMax <= 64 && kTileMax <= 1024 && (size_t)TA << kTil
 // (measured on the survey benchmark: s-mu counts run faster at 4, sigma-pi
 // counts at 2); the warp's queue holds a partial round plus 4 ballots
 constexpr int QPUSH = 4;
+constexpr int QPUSH_NOJK = 2;
 __host__ __device__ constexpr int qpush_exact(int mode) { return mode == MODE_S_MU ? 4 : 2; }
-constexpr int kQueueCap = 32 + 32 * 4;
-static_assert(R % QPUSH == 0 && R % 2 == 0 && QPUSH <= 4, "the push loops consume after every QPUSH A slots");
+__host__ __device__ constexpr int queue_cap(bool exact, bool jk, bool adj) {
+    return 32 + 32 * (light_fast(exact, jk, adj) ? QPUSH_NOJK : 4);
+}
+static_assert(R % QPUSH == 0 && R % QPUSH_NOJK == 0 && R % 2 == 0 && QPUSH <= 4 && QPUSH_NOJK <= 4,
+              "the push loops consume after every QPUSH A slots");
 constexpr int LUT1_BITS = 8;   // buckets per octave of the float-indexed table
 constexpr int LUT1_OCTAVES = 24;
 constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
@@ -187,7 +198,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o += LUT2_N;
     o = (o + 15) / 16 * 16;
     L.queue = o;
-    o += (size_t)NWARP * kQueueCap * 16;
+    o += (size_t)NWARP * queue_cap(exact, jk, adj) * 16;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
     if (!exact) o += (size_t)TA * 16;
     L.ga = o;      // adjoint: per-point gradient sums (64-bit fixed point as two 32-bit words)
@@ -198,7 +209,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     L.tile0 = o;
     o += tile_bytes(exact);
     L.tile1 = o;
-    o += (size_t)(n_buffers(exact) - 1) * tile_bytes(exact);
+    o += (size_t)(n_buffers(exact, jk, adj) - 1) * tile_bytes(exact);
     o = (o + 15) / 16 * 16;
     L.misc = o;  // item index, mbarriers, tile-done counters, the item's job
     o += 64 + sizeof(JobK);
@@ -689,7 +700,8 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
     constexpr bool ADJ = (WK == W_ADJ);
     constexpr int TBK = EXACT ? TB_EXACT : TB;  // B points per tile
-    constexpr int NB = n_buffers(EXACT);          // tile buffers
+    constexpr int NB = n_buffers(EXACT, JK, ADJ);                        // tile buffers
+    constexpr int QPF = light_fast(EXACT, JK, ADJ) ? QPUSH_NOJK : QPUSH;  // FP32 path push width
     const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
@@ -707,7 +719,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     unsigned *s_done = (unsigned *)(smem + L.misc + 16 + 8 * kNbufMax);  // warps done with each buffer (running count)
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float4 *s_q = (float4 *)(smem + L.queue) + warp * kQueueCap;
+    float4 *s_q = (float4 *)(smem + L.queue) + warp * queue_cap(EXACT, JK, ADJ);
     const unsigned lt_mask = (1u << lane) - 1u;
     const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo),
                 (uint32_t *)(smem + L.ga), (uint32_t *)(smem + L.ga) + TA,
@@ -984,9 +996,9 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 if (SELF) hit[r] = hit[r] && jg > ai[r];
                             }
 #pragma unroll
-                            for (int r0 = 0; r0 < R; r0 += QPUSH) {
+                            for (int r0 = 0; r0 < R; r0 += QPF) {
 #pragma unroll
-                                for (int r = r0; r < r0 + QPUSH; ++r) {
+                                for (int r = r0; r < r0 + QPF; ++r) {
                                     const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
                                     if (hit[r])
                                         s_q[qn + __popc(bal & lt_mask)] =
