@@ -326,17 +326,13 @@ def count_step(tp, ctx, D, R, bins, precision, release=True, sharded=False):
     return in_range, cand, kms, flops, hists
 
 
-def cpu_reference_sample(w, target_s: float = 12.0, ctx=None):
-    """Time the reference's own OpenMP code (oracle/_ref, built from the
-    reference sources) on a random subsample of the same workload.  The
-    in-range pair count of the sample comes from the engine on the identical
-    sample.  Returns a cpu_baseline dict."""
-    from oracle import refl
-    import two_pcf_b200 as tp
-    n_threads = os.cpu_count() or 1
-    rng = np.random.default_rng(7)
-
-    def run(frac):
+def reference_sample(w, target_s: float, rng):
+    """A random subsample of the workload sized so that one pass of the
+    reference's own OpenMP code (oracle/_ref, built from the reference
+    sources) over the step's six counts takes about target_s on this host:
+    a 1 % sample calibrates the size.  Returns (data, randoms, fraction,
+    seconds of the last pass)."""
+    def draw(frac):
         d, r = w["data"], w["rand"]
         nd = max(200, int(d["xyz"].shape[0] * frac))
         nr = max(1000, int(r["xyz"].shape[0] * frac))
@@ -346,73 +342,107 @@ def cpu_reference_sample(w, target_s: float = 12.0, ctx=None):
         def cat(c, idx):
             return {"xyz": c["xyz"][idx], "unit": c["x_norm"][idx], "dcom": c["d_comov"][idx],
                     "w": c["weight"][idx], "jk": c["jk"][idx]}
-
-        cd, cr = cat(d, di), cat(r, ri)
-        t0 = time.perf_counter()
-        for ax, mode in ((SIGMA_PI_AXES, refl.SIGMA_PI), (S_MU_AXES, refl.S_MU)):
-            axes = (*ax[0][:3], ax[0][3], *ax[1][:3], ax[1][3])
-            refl.count_3d(mode, cd, cr, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
-            refl.count_3d(mode, cd, cr, is_auto=False, n_jk=100, axes=axes, n_threads=n_threads)
-            refl.count_3d(mode, cr, cd, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
-        dt = time.perf_counter() - t0
-        pairs = None
-        if ctx is not None:
-            D = tp.Catalog(ctx, cd["xyz"], cd["unit"], cd["dcom"], cd["w"], None, cd["jk"], 100)
-            R = tp.Catalog(ctx, cr["xyz"], cr["unit"], cr["dcom"], cr["w"], None, cr["jk"], 100)
-            bins = [(1, tp.Binning(ctx, tp.SIGMA_PI, *SIGMA_PI_AXES, 100)),
-                    (2, tp.Binning(ctx, tp.S_MU, *S_MU_AXES, 100))]
-            pairs = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)[0]
-        return dt, pairs, nd, nr
+        return cat(d, di), cat(r, ri)
 
     frac = 0.01
-    dt, pairs, nd, nr = run(frac)
+    cd, cr = draw(frac)
+    dt = time_reference(cd, cr)
     if dt < target_s / 8:
         frac = min(1.0, frac * np.sqrt(target_s / max(dt, 1e-3)))
-        dt, pairs, nd, nr = run(frac)
-    return {"value": (pairs / dt) if pairs else None, "unit": UNIT, "cores": n_threads, "kind": "reference",
-            "seconds": dt, "in_range_pairs": pairs,
-            "sample": f"random {frac:.3f} subsample of the workload: {nd} data, {nr} randoms; sigma-pi and s-mu "
-                      f"DD+DR+RR through the reference's auto_/cross_pair_count_* built from its sources "
-                      f"(g++ -O3 -fopenmp), {n_threads} OpenMP threads"}
+        cd, cr = draw(frac)
+        dt = time_reference(cd, cr)
+    return cd, cr, frac, dt
+
+
+def time_reference(cd, cr):
+    """Seconds of one pass of the reference's auto_/cross_pair_count_* over
+    the step's six counts (sigma-pi and s-mu DD, DR, RR) on all host threads."""
+    from oracle import refl
+    n_threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    for ax, mode in ((SIGMA_PI_AXES, refl.SIGMA_PI), (S_MU_AXES, refl.S_MU)):
+        axes = (*ax[0][:3], ax[0][3], *ax[1][:3], ax[1][3])
+        refl.count_3d(mode, cd, cr, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
+        refl.count_3d(mode, cd, cr, is_auto=False, n_jk=100, axes=axes, n_threads=n_threads)
+        refl.count_3d(mode, cr, cd, is_auto=True, n_jk=100, axes=axes, n_threads=n_threads)
+    return time.perf_counter() - t0
+
+
+def sample_text(cd, cr, frac):
+    return (f"random {frac:.3f} subsample of the workload: {cd['xyz'].shape[0]} data, {cr['xyz'].shape[0]} "
+            f"randoms; sigma-pi and s-mu DD+DR+RR through the reference's auto_/cross_pair_count_* built from its "
+            f"sources (g++ -O3 -fopenmp), {os.cpu_count() or 1} OpenMP threads")
+
+
+def cpu_reference_sample(w, target_s: float = 12.0, ctx=None):
+    """The reference's own OpenMP code timed on a random subsample of the
+    workload (this arm's cpu_baseline); the sample's in-range pairs come from
+    the engine on the identical sample.  Returns a cpu_baseline dict."""
+    import two_pcf_b200 as tp
+    cd, cr, frac, dt = reference_sample(w, target_s, np.random.default_rng(7))
+    D = tp.Catalog(ctx, cd["xyz"], cd["unit"], cd["dcom"], cd["w"], None, cd["jk"], 100)
+    R = tp.Catalog(ctx, cr["xyz"], cr["unit"], cr["dcom"], cr["w"], None, cr["jk"], 100)
+    bins = [(1, tp.Binning(ctx, tp.SIGMA_PI, *SIGMA_PI_AXES, 100)), (2, tp.Binning(ctx, tp.S_MU, *S_MU_AXES, 100))]
+    pairs = count_step(tp, ctx, D, R, bins, tp.FP32_GUARD)[0]
+    return {"value": pairs / dt, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference", "seconds": dt,
+            "in_range_pairs": pairs, "sample": sample_text(cd, cr, frac)}
+
+
+def _kdtree_count(job):
+    """One count's in-range pairs (0 < s < r) by KD-tree pair counting."""
+    from scipy.spatial import cKDTree
+    a, b, r = job
+    ta = cKDTree(a)
+    if b is None:  # unordered pairs of distinct points
+        return (int(ta.count_neighbors(ta, r)) - int(ta.count_neighbors(ta, 0.0))) // 2
+    tb = cKDTree(b)
+    return int(tb.count_neighbors(ta, r)) - int(tb.count_neighbors(ta, 0.0))
+
+
+def in_range_pairs_kdtree(cd, cr):
+    """In-range pairs of the step's six counts on a sample (the reference's
+    range test 0 < s^2 < max^2 of sigma-pi and s-mu), counted with scipy's
+    KD-tree in spawned worker processes, no part of this engine involved.
+    Separations are compared in double; pairs within ~1e-7 relative of a
+    range limit may fall on the other side of the reference's float test."""
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    xd = cd["xyz"][cd["dcom"] >= 0]
+    xr = cr["xyz"][cr["dcom"] >= 0]
+    radii = [float(np.sqrt(SIGMA_PI_AXES[0][1] ** 2 + SIGMA_PI_AXES[1][1] ** 2)), float(S_MU_AXES[0][1])]
+    jobs = [(a, b, r * (1.0 - 1e-12)) for r in radii for a, b in ((xd, None), (xd, xr), (xr, None))]
+    with ProcessPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 1),
+                             mp_context=mp.get_context("spawn")) as ex:
+        return int(sum(ex.map(_kdtree_count, jobs)))
 
 
 def run_reference_arm(args, ws, rank):
-    """--impl reference: the reference's CPU implementation on the host cores."""
+    """--impl reference: the reference's CPU implementation on the host cores.
+    One sample of the workload is drawn (sized for ~8 s of reference work per
+    step) and its in-range pairs are counted once by KD-tree; each of the
+    --steps steps times one pass of the reference's code over it."""
     if rank != 0:
         return
     from oracle import refl
-    ctx = None
-    try:
-        import torch
-        if torch.cuda.is_available():
-            import two_pcf_b200 as tp
-            ctx = tp.Context(0)
-    except Exception:
-        ctx = None
     if not refl.available("plain"):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtwopcf_ref_plain.so not built "
                           "(oracle/build_ref.sh needs the reference sources)"}))
         return
     w = make_workload(2, args.scale)
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    vals, secs, base = [], [], None
-    for s in range(args.steps):
-        base = cpu_reference_sample(w, target_s=8.0, ctx=ctx)
-        if base["value"] is None:
-            # no GPU for the pair tally: count in-range pairs with the oracle restatement is too slow here
-            print(json.dumps({"impl": "reference", "unavailable": "needs a GPU to tally in-range pairs"}))
-            return
-        vals.append(base["value"])
-        secs.append(base["seconds"])
-    v = statistics.median(vals)
+    cd, cr, frac, _ = reference_sample(w, 8.0, np.random.default_rng(7))   # also the warm-up pass
+    pairs = in_range_pairs_kdtree(cd, cr)
+    secs = [time_reference(cd, cr) for _ in range(max(1, args.steps))]
+    v = pairs / statistics.median(secs)
+    sample = sample_text(cd, cr, frac) + "; in-range pairs of the sample by KD-tree pair counting"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(secs),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
             "data": "synthetic", "config": {"workload": "survey slab 1M data / 5M randoms, sigma-pi 50x50 + "
                                                         "s-mu 40x50, 100 jackknife regions, weighted",
-                                            "sample": base["sample"]},
-            "cpu_baseline": {k: base[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                                            "sample": sample},
+            "in_range_pairs_per_step": pairs,
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": os.cpu_count() or 1, "kind": "reference",
+                             "sample": sample},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 

@@ -1,0 +1,39 @@
+"""The reference arm of bench.py counts the in-range pairs of its sample by
+KD-tree (no part of the engine on that path).  Its count must equal the
+reference's range test (src/correlators.cpp:33-40: d = (float)(x1 - x2) per
+axis, s^2 = (d0^2 + d1^2) + d2^2 in float, min^2 < s^2 < max^2, auto counts
+over unordered pairs), restated here in float32 numpy on a small sample with
+a duplicate point (s^2 = 0 is never in range)."""
+import numpy as np
+
+import bench
+from two_pcf_b200 import synthetic
+
+
+def float_range_pairs(a, b, max_sq, auto):
+    tot = 0
+    m = np.float32(max_sq)
+    for i0 in range(0, a.shape[0], 500):
+        A = a[i0:i0 + 500]
+        d = [(A[:, None, q] - b[None, :, q]).astype(np.float32) for q in range(3)]
+        s2 = (d[0] * d[0] + d[1] * d[1]) + d[2] * d[2]
+        ok = (s2 > np.float32(0)) & (s2 < m)
+        if auto:
+            ok &= np.arange(b.shape[0])[None, :] > np.arange(i0, i0 + A.shape[0])[:, None]
+        tot += int(ok.sum())
+    return tot
+
+
+def test_kdtree_tally_matches_the_reference_range_test():
+    w = synthetic.survey_catalogue(seed=9, n_data=3000, n_rand=8000)
+    cd = {"xyz": w["data"]["xyz"].copy(), "dcom": w["data"]["d_comov"]}
+    cr = {"xyz": w["rand"]["xyz"], "dcom": w["rand"]["d_comov"]}
+    cd["xyz"][1] = cd["xyz"][0]
+    got = bench.in_range_pairs_kdtree(cd, cr)
+    xd, xr = cd["xyz"], cr["xyz"]
+    sp, sm = bench.SIGMA_PI_AXES, bench.S_MU_AXES
+    want = 0
+    for max_sq in (sp[0][1] ** 2 + sp[1][1] ** 2, sm[0][1] ** 2):  # sigma-pi: sigma_max^2 + pi_max^2
+        want += (float_range_pairs(xd, xd, max_sq, True) + float_range_pairs(xd, xr, max_sq, False)
+                 + float_range_pairs(xr, xr, max_sq, True))
+    assert got == want and got > 0
