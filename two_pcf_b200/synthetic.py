@@ -22,10 +22,24 @@ import numpy as np
 C_KMS = 299792.458
 
 
+# Footprint and jackknife boundaries as decimal literals (sin 10 deg, tan 60 deg,
+# tan(6k deg), sin(-10 + 2k deg)), so that no run-time libm call decides them.
+SIN_DEC_LIM = 0.17364817766693033
+TAN_RA_MAX = 1.7320508075688772
+TAN_RA_EDGES = np.array([0.10510423526567647, 0.21255656167002213, 0.3249196962329063, 0.4452286853085362,
+                         0.5773502691896257, 0.7265425280053609, 0.9004040442978399, 1.110612514829193,
+                         1.3763819204711734])
+SIN_DEC_EDGES = np.array([-0.13917310096006544, -0.10452846326765347, -0.0697564737441253, -0.03489949670250097,
+                          0.0, 0.03489949670250097, 0.0697564737441253, 0.10452846326765347, 0.13917310096006544])
+
+
 def comoving_table(omega_m: float = 0.25, h: float = 1.0, z_max: float = 1.0, n: int = 20001):
-    """(z, d_c) table of a flat LCDM cosmology in Mpc/h (trapezoid rule)."""
+    """(z, d_c) table of a flat LCDM cosmology in Mpc/h (trapezoid rule).
+    Only correctly rounded operations (+, *, /, sqrt, a sequential cumsum),
+    so the table is the same on every x86-64 host."""
     z = np.linspace(0.0, z_max, n)
-    e = 1.0 / np.sqrt(omega_m * (1 + z) ** 3 + (1 - omega_m))
+    a = 1.0 + z
+    e = 1.0 / np.sqrt(omega_m * (a * a * a) + (1 - omega_m))
     d = np.concatenate([[0.0], np.cumsum(0.5 * (e[1:] + e[:-1]) * np.diff(z))]) * C_KMS / (100.0 * h)
     return z, d
 
@@ -72,67 +86,107 @@ def box_catalogue(seed: int = 1, n_data: int = 100_000, n_rand: int = 300_000, b
     return {"data": {"xyz": _avoid_first_point_max(data)}, "rand": {"xyz": _avoid_first_point_max(rand)}}
 
 
-def _survey_points(rng, n, z_tab, d_tab, ra_max=60.0, dec_lim=10.0, z_mu=0.3, z_sd=0.08, z_lo=0.1, z_hi=0.5):
-    ra = rng.uniform(0.0, ra_max, n)
-    s = rng.uniform(np.sin(np.radians(-dec_lim)), np.sin(np.radians(dec_lim)), n)
-    dec = np.degrees(np.arcsin(s))
+def _footprint_directions(rng, n):
+    """n unit vectors uniform on the footprint (ra in [0, 60) deg, sin(dec)
+    uniform on [-sin 10, sin 10]): the azimuth of a point drawn uniformly in
+    the 60-degree sector of the unit disc, the z component drawn uniformly."""
+    cs, sn = [], []
+    have = 0
+    while have < n:
+        m = 2 * (n - have) + 64   # the sector is 52 % of the unit square
+        a = rng.uniform(0.0, 1.0, m)
+        b = rng.uniform(0.0, 1.0, m)
+        r2 = a * a + b * b
+        ok = (r2 <= 1.0) & (r2 > 1e-4) & (b < TAN_RA_MAX * a)
+        rho = np.sqrt(r2[ok])
+        cs.append(a[ok] / rho)
+        sn.append(b[ok] / rho)
+        have += int(ok.sum())
+    cphi = np.concatenate(cs)[:n]
+    sphi = np.concatenate(sn)[:n]
+    uz = rng.uniform(-SIN_DEC_LIM, SIN_DEC_LIM, n)
+    c = np.sqrt(1.0 - uz * uz)
+    return np.stack([c * cphi, c * sphi, uz], axis=1)
+
+
+def _redshifts(rng, n, z_mu=0.3, z_sd=0.08, z_lo=0.1, z_hi=0.5):
     z = np.empty(0)
     while z.size < n:
         t = rng.normal(z_mu, z_sd, 2 * n)
         z = np.concatenate([z, t[(t >= z_lo) & (t <= z_hi)]])
-    z = z[:n]
-    return ra, dec, z
+    return z[:n]
 
 
 def survey_catalogue(seed: int = 2, n_data: int = 1_000_000, n_rand: int = 5_000_000, n_jk_ra: int = 10,
                      n_jk_dec: int = 10, weights: bool = True, cluster_frac: float = 1.0, mean_members: float = 20.0,
                      sigma: float = 5.0, omega_m: float = 0.25, h: float = 1.0):
-    """Equatorial slab; returns dict(data=..., rand=...) with ra, dec, z, xyz,
-    x_norm, d_comov, weight (float32) and jk (int32) per catalogue."""
+    """Equatorial slab; returns dict(data=..., rand=..., n_jk=...) with
+    xyz, x_norm, d_comov, z, weight (float32), jk (int32) and, for reference
+    only, ra and dec (degrees) per catalogue.
+
+    Positions and unit vectors are formed from numpy's seeded draws with
+    correctly rounded operations only (no vectorised sin, cos, arcsin or
+    power, whose SIMD implementations differ between CPUs), so the same seed
+    gives bit-identical catalogues on any x86-64 host with this numpy: the
+    full-size parity fixtures regenerate their inputs from the seed.  The
+    jackknife grid is 10 x 10 regions, 6 deg in ra by 2 deg in dec, defined
+    by the literal boundaries above."""
+    if (n_jk_ra, n_jk_dec) != (10, 10):
+        raise ValueError("the survey footprint's jackknife grid is 10 x 10")
     rng = np.random.default_rng(seed)
     z_tab, d_tab = comoving_table(omega_m, h)
+    d_lo, d_hi = np.interp([0.1, 0.5], z_tab, d_tab)
 
-    def finish(ra, dec, z, w):
-        d = np.interp(z, z_tab, d_tab)
-        u = radec_to_unit(ra, dec)
-        jk_ra = np.minimum((ra / (60.0 / n_jk_ra)).astype(np.int32), n_jk_ra - 1)
-        jk_dec = np.minimum(((dec + 10.0) / (20.0 / n_jk_dec)).astype(np.int32), n_jk_dec - 1)
-        return {"ra": ra, "dec": dec, "z": z, "d_comov": d, "x_norm": u, "xyz": u * d[:, None],
-                "weight": w, "jk": (jk_ra * n_jk_dec + jk_dec).astype(np.int32)}
+    def finish(u, d, w):
+        jk_ra = (u[:, 1][:, None] >= TAN_RA_EDGES[None, :] * u[:, 0][:, None]).sum(1)
+        jk_dec = (u[:, 2][:, None] >= SIN_DEC_EDGES[None, :]).sum(1)
+        ra = np.degrees(np.arctan2(u[:, 1], u[:, 0]))
+        dec = np.degrees(np.arcsin(np.clip(u[:, 2], -1.0, 1.0)))
+        return {"ra": ra, "dec": dec, "z": np.interp(d, d_tab, z_tab), "d_comov": d, "x_norm": u,
+                "xyz": u * d[:, None], "weight": w, "jk": (jk_ra * n_jk_dec + jk_dec).astype(np.int32)}
 
     # data: Neyman-Scott in comoving space around centres drawn from the selection
     n_cl = int(n_data * cluster_frac)
-    parts_ra, parts_dec, parts_z = [], [], []
+    parts_u, parts_d = [], []
     have = 0
     while have < n_cl:
         nc = max(1, int((n_cl - have) / mean_members * 1.3))
-        cra, cdec, cz = _survey_points(rng, nc, z_tab, d_tab)
-        cxyz = radec_to_unit(cra, cdec) * np.interp(cz, z_tab, d_tab)[:, None]
+        cxyz = _footprint_directions(rng, nc) * np.interp(_redshifts(rng, nc), z_tab, d_tab)[:, None]
         k = rng.poisson(mean_members, nc)
         m = np.repeat(cxyz, k, axis=0) + rng.normal(0.0, sigma, (int(k.sum()), 3))
-        dist = np.linalg.norm(m, axis=1)
-        ra = np.degrees(np.arctan2(m[:, 1], m[:, 0])) % 360.0
-        dec = np.degrees(np.arcsin(np.clip(m[:, 2] / dist, -1, 1)))
-        z = np.interp(dist, d_tab, z_tab)
-        keep = (ra < 60.0) & (np.abs(dec) < 10.0) & (z >= 0.1) & (z <= 0.5)
-        parts_ra.append(ra[keep])
-        parts_dec.append(dec[keep])
-        parts_z.append(z[keep])
+        dist = np.sqrt(m[:, 0] * m[:, 0] + m[:, 1] * m[:, 1] + m[:, 2] * m[:, 2])
+        keep = ((m[:, 0] > 0) & (m[:, 1] >= 0) & (m[:, 1] < TAN_RA_MAX * m[:, 0])
+                & (np.abs(m[:, 2]) < SIN_DEC_LIM * dist) & (dist >= d_lo) & (dist <= d_hi))
+        parts_u.append(m[keep] / dist[keep][:, None])
+        parts_d.append(dist[keep])
         have += int(keep.sum())
-    ra = np.concatenate(parts_ra)[:n_cl]
-    dec = np.concatenate(parts_dec)[:n_cl]
-    z = np.concatenate(parts_z)[:n_cl]
+    u = np.concatenate(parts_u)[:n_cl]
+    d = np.concatenate(parts_d)[:n_cl]
     if n_cl < n_data:
-        r2, d2, z2 = _survey_points(rng, n_data - n_cl, z_tab, d_tab)
-        ra, dec, z = np.concatenate([ra, r2]), np.concatenate([dec, d2]), np.concatenate([z, z2])
+        u2 = _footprint_directions(rng, n_data - n_cl)
+        d2 = np.interp(_redshifts(rng, n_data - n_cl), z_tab, d_tab)
+        u, d = np.concatenate([u, u2]), np.concatenate([d, d2])
     perm = rng.permutation(n_data)
-    ra, dec, z = ra[perm], dec[perm], z[perm]
+    u, d = u[perm], d[perm]
     wd = rng.lognormal(0.0, 0.2, n_data).astype(np.float32) if weights else np.ones(n_data, np.float32)
-    data = finish(ra, dec, z, wd)
-    rra, rdec, rz = _survey_points(rng, n_rand, z_tab, d_tab)
+    data = finish(u, d, wd)
+    ur = _footprint_directions(rng, n_rand)
+    dr = np.interp(_redshifts(rng, n_rand), z_tab, d_tab)
     wr = rng.lognormal(0.0, 0.2, n_rand).astype(np.float32) if weights else np.ones(n_rand, np.float32)
-    rand = finish(rra, rdec, rz, wr)
+    rand = finish(ur, dr, wr)
     return {"data": data, "rand": rand, "n_jk": n_jk_ra * n_jk_dec}
+
+
+def catalogue_digest(cat: dict) -> str:
+    """sha256 over the arrays that enter a count (xyz, x_norm, d_comov,
+    weight, jk) of one catalogue: a fixture made from a seed records it so a
+    test can tell whether the seed regenerated the same inputs."""
+    import hashlib
+    h = hashlib.sha256()
+    for k in ("xyz", "x_norm", "d_comov", "weight", "jk"):
+        if cat.get(k) is not None:
+            h.update(np.ascontiguousarray(cat[k]).tobytes())
+    return h.hexdigest()
 
 
 def bitwise_masks(seed: int, n: int, n_runs: int = 2048, n_mask_ints: int = 32, p_lo: float = 0.3,
