@@ -15,7 +15,7 @@ import two_pcf_b200 as tp
 pytestmark = pytest.mark.gpu
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("sky_"))  # 3-D plain-build fixtures
+                if not os.path.basename(p).startswith(("sky_", "full_")))  # 3-D plain-build fixtures
 W_RTOL = 1e-12
 MODES = {0: tp.MONOPOLE, 1: tp.SIGMA_PI, 2: tp.S_MU}
 

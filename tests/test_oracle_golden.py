@@ -14,7 +14,7 @@ import pytest
 from oracle import port, refl
 
 GOLDEN = sorted(p for p in glob.glob(os.path.join(os.path.dirname(__file__), "golden", "*.npz"))
-                if not os.path.basename(p).startswith("sky_"))  # 3-D plain-build fixtures
+                if not os.path.basename(p).startswith(("sky_", "full_")))  # 3-D plain-build fixtures
 W_RTOL = 1e-12
 
 
