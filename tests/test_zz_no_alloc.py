@@ -4,6 +4,10 @@ scratch in a static device array — against tpcf_count, through the C ABI.
 Each case counts once with tpcf_count (which also caches the cell grids the
 allocation-free call needs) and then twice in a row with tpcf_count_noalloc:
 the second call must not see the first call's leftovers in the shared array.
+The two allocation-free calls run with every device allocation made to fail
+(tpcf_debug_fail_allocations(0)), so they succeed only if they allocate
+nothing; tpcf_count under the same setting fails with TPCF_E_OOM, which shows
+the setting is in force.
 Unit-weight counts must be identical; weighted sums agree to 1e-12 relative,
 the tolerance of the other parity tests (both calls run the same kernel and
 sum in the same fixed point, so they are in fact identical)."""
@@ -36,6 +40,16 @@ def count_noalloc(ctx, a, b, binning, precision=tp.FP32_GUARD):
     return rc, msg, full, reg, st.as_dict()
 
 
+class allocations_fail:
+    """Every device allocation of the engine fails inside the block."""
+
+    def __enter__(self):
+        assert _capi.lib().tpcf_debug_fail_allocations(0) == 0
+
+    def __exit__(self, *exc):
+        _capi.lib().tpcf_debug_fail_allocations(-1)
+
+
 def same(x, y, weighted):
     if weighted:
         np.testing.assert_allclose(x, y, rtol=W_RTOL, atol=1e-9 * max(1.0, float(np.abs(y).max())))
@@ -65,8 +79,12 @@ def test_noalloc_matches_count_twice(ctx, survey, mode, ax1, ax2, precision):
     for a, bb, weighted in ((D, None, True), (D, R, True), (U, None, False)):
         full, reg, st = tp.count(ctx, a, bb, b, precision)
         assert full.sum() > 0
-        for _ in range(2):
-            rc, msg, f2, r2, st2 = count_noalloc(ctx, a, bb, b, precision)
+        with allocations_fail():
+            runs = [count_noalloc(ctx, a, bb, b, precision) for _ in range(2)]
+            with pytest.raises(tp.TpcfError) as refused:
+                tp.count(ctx, a, bb, b, precision)
+        assert refused.value.status == _capi.TPCF_E_OOM
+        for rc, msg, f2, r2, st2 in runs:
             assert rc == 0, msg
             same(f2, full, weighted)
             same(r2, reg, weighted)
@@ -88,9 +106,10 @@ def test_noalloc_refuses_without_cached_grid(ctx):
 
 
 def test_noalloc_refuses_oversized_scratch(ctx):
-    """4096 bins x 1100 regions of 64-bit sums need more than the 32 MiB array."""
+    """4096 bins x 1100 regions of 128-bit sums (16 bytes each) need more
+    than the 32 MiB array."""
     n_jk = 1100
-    assert 4096 * n_jk * 8 > STATIC_SCRATCH_BYTES
+    assert 4096 * n_jk * 16 > STATIC_SCRATCH_BYTES
     rng = np.random.default_rng(4)
     x = rng.uniform(100, 300, (2000, 3))
     A = tp.Catalog(ctx, x, jk_region=rng.integers(0, n_jk, 2000).astype(np.int32), n_jk_regions=n_jk)

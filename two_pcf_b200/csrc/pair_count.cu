@@ -169,8 +169,13 @@ struct Shm {
 };
 
 struct SmemLayout {
-    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, achunk, ga, gb, tile0, tile1, misc, total;
+    size_t lo, hi, alo, ahi, t1, t2, lut1, lut2, queue, slow, achunk, ga, gb, tile0, tile1, misc, total;
 };
+
+// Per-warp side queue of the FP32 path: the packed (A chunk index, tile
+// index) of pairs whose bin the tables leave ambiguous (bin_fast); at most
+// 31 wait between rounds and a round adds at most 32.
+constexpr int kSlowCap = 64;
 
 // FP32 path: pos and aux float4 per point; FP64 path: one double4 per point
 __host__ __device__ inline size_t tile_bytes(bool exact) { return exact ? (size_t)TB_EXACT * 32 : (size_t)TB * 32; }
@@ -199,6 +204,8 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o = (o + 15) / 16 * 16;
     L.queue = o;
     o += (size_t)NWARP * queue_cap(exact, jk, adj) * 16;
+    L.slow = o;
+    if (!exact) o += (size_t)NWARP * kSlowCap * 4;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
     if (!exact) o += (size_t)TA * 16;
     L.ga = o;      // adjoint: per-point gradient sums (64-bit fixed point as two 32-bit words)
@@ -528,8 +535,16 @@ __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, cons
 // pair's positions in the sorted grids (the exact path follows them back to
 // the original arrays) come from the queue entry; ra/rb are the regions of
 // its two points.
-template <int MODE, bool UNITW, int WK>
-__device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const PreciseArgs &PA, const ExactArgs &E,
+//
+// A pair whose table entries leave its bin ambiguous needs the threshold
+// search and possibly the exact sequence.  Resolved inline, that rare path
+// (well under 1 % of the pairs) would run for the whole warp in every round
+// where any lane met such a pair; so the first pass (SLOW = false) returns
+// true for it without binning it, the caller parks it in the warp's side
+// queue, and a second pass (SLOW = true) over 32 parked pairs at a time
+// resolves them.  Returns false otherwise.
+template <int MODE, bool UNITW, int WK, bool SLOW>
+__device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const PreciseArgs &PA, const ExactArgs &E,
                                          const Shm &S, const float4 *s_pos, const float4 *s_aux,
                                          const float4 *s_achunk, const float4 e, int a_start, int jbase, int ra,
                                          int rb, Counters &cnt) {
@@ -556,11 +571,12 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
         const float v = 0.5f * s2;
         bool amb1;
         const unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, v)], v, S.t1, P.g_ang, P.lut_edge1, &amb1);
-        if (c1 == LUT_INV) return;
+        if (c1 == LUT_INV) return false;
         if (!amb1) {
             cnt.in_range += 1;
             bin = (int)c1;
         } else {
+            if constexpr (!SLOW) return true;
             const dev::AxisK ax1{S.t1, P.n1, 0, 0.f, 0.f, 0.f, 0.f};
             int b = dev::locate_exact(S.t1, P.n1, v);
             bool inr;
@@ -571,14 +587,14 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
                 inr = b >= 0 && b < P.n1;
             }
             cnt.in_range += inr ? 1 : 0;
-            if (!inr) return;
+            if (!inr) return false;
             bin = b;
         }
         add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
-        return;
+        return false;
     } else {
         if (MODE == MODE_SIGMA_PI) {
-            if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return;  // certainly out of range
+            if (s2 >= P.max_r_sq + P.g_s2 || s2 <= P.min_r_sq - P.g_s2) return false;  // certainly out of range
             amb = (fabsf(s2 - P.max_r_sq) <= P.g_s2) || (fabsf(s2 - P.min_r_sq) <= P.g_s2);
             const float a = fmaf(-pi, pi, s2);
             const float api = fabsf(pi);
@@ -595,7 +611,7 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
             const unsigned c2 = lut_decode(S.l2[lut2_index(P.lut2_scale, api)], api, S.t2, P.g_pi, P.lut_edge2, &amb2);
             if (!amb && ((c1 == LUT_INV && !amb1) || (c2 == LUT_INV && !amb2))) {
                 cnt.in_range += 1;
-                return;
+                return false;
             }
             amb = amb || amb1 || amb2 || c1 == LUT_INV || c2 == LUT_INV;
             if (!amb) cnt.in_range += 1;
@@ -619,12 +635,12 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
                 cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
-                return;
+                return false;
             }
             if (MODE == MODE_S_MU) {
                 if (c2 == LUT_INV && !amb2 && !amb && s2 >= P.s2_lut_min) {
                     cnt.in_range += 1;
-                    return;
+                    return false;
                 }
                 amb = amb || amb2 || c2 == LUT_INV || s2 < P.s2_lut_min;
             }
@@ -632,13 +648,15 @@ __device__ __forceinline__ void bin_fast(const KParams &P, const JobK &J, const 
             bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
         }
         if (amb) {
+            if constexpr (!SLOW) return true;
             bool inr, guarded;
             bin = precise_bin<MODE>(PA, E, S.t1, S.t2, s2, pi, J.a.idx[ia], J.b.idx[jb], &inr, &guarded);
             cnt.in_range += inr ? 1 : 0;
             cnt.guard += guarded ? 1 : 0;
-            if (bin < 0) return;
+            if (bin < 0) return false;
         }
         add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+        return false;
     }
 }
 
@@ -720,6 +738,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float4 *s_q = (float4 *)(smem + L.queue) + warp * queue_cap(EXACT, JK, ADJ);
+    int *s_slow = (int *)(smem + L.slow) + warp * kSlowCap;
     const unsigned lt_mask = (1u << lane) - 1u;
     const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo),
                 (uint32_t *)(smem + L.ga), (uint32_t *)(smem + L.ga) + TA,
@@ -972,6 +991,27 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     const unsigned char *tile = tile_base + (tcount % NB) * tile_stride;
                     const float4 *s_pos = (const float4 *)tile;
                     const float4 *s_aux = (const float4 *)(tile + (size_t)TBK * 16);
+                    int ns = 0;  // parked entries of this warp (warp-uniform)
+                    // every lane of the warp calls park: a deferred pair's
+                    // packed indices go to the side queue
+                    auto park = [&](bool dfr, const float4 &e) {
+                        const unsigned bd = __ballot_sync(0xffffffffu, dfr);
+                        if (dfr) s_slow[ns + __popc(bd & lt_mask)] = __float_as_int(e.w);
+                        ns += __popc(bd);
+                    };
+                    // second pass over a parked pair: its separation again,
+                    // from the A point (global) in this segment's frame and
+                    // the B point of the tile, by the candidate loop's own
+                    // operations, so bit for bit the value it was queued with
+                    auto resolve = [&](int pk) {
+                        const int ka = pk >> kTileShift, jl = pk & kTileMask;
+                        const float4 pa = J.a.pos[it.a_start + ka];
+                        const float4 pb = s_pos[jl];
+                        const float ax0 = pa.x + offx, ay0 = pa.y + offy, az0 = pa.z + offz;
+                        const float4 e = make_float4(ax0 - pb.x, ay0 - pb.y, az0 - pb.z, __int_as_float(pk));
+                        bin_fast<MODE, UNITW, WK, true>(P, J, PA, EA, S, s_pos, s_aux, s_achunk, e, it.a_start, jbase,
+                                                        it.a_region, rb, cnt);
+                    };
                     // Candidates: (dx, dy, dz) of the pair in the segment's cell
                     // frame; those inside the guard-widened range are pushed
                     // into the warp's queue with a ballot, and each time 32 are
@@ -1008,9 +1048,14 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                                 while (qn >= 32) {
                                     __syncwarp();
                                     const float4 e = s_q[qn - 32 + lane];
-                                    bin_fast<MODE, UNITW, WK>(P, J, PA, EA, S, s_pos,
-                                                              s_aux, s_achunk, e, it.a_start, jbase, it.a_region, rb,
-                                                              cnt);
+                                    park(bin_fast<MODE, UNITW, WK, false>(P, J, PA, EA, S, s_pos, s_aux, s_achunk, e,
+                                                                          it.a_start, jbase, it.a_region, rb, cnt),
+                                         e);
+                                    if (ns >= 32) {
+                                        __syncwarp();
+                                        resolve(s_slow[ns - 32 + lane]);
+                                        ns -= 32;
+                                    }
                                     __syncwarp();
                                     qn -= 32;
                                 }
@@ -1019,14 +1064,26 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
                     };
                     if (self) run(std::true_type{});
                     else run(std::false_type{});
-                    // drain: the queued entries refer to this tile's positions
+                    // drain: the queued and parked entries refer to this
+                    // tile's positions
                     if (qn > 0) {
                         __syncwarp();
-                        if (lane < qn)
-                            bin_fast<MODE, UNITW, WK>(P, J, PA, EA, S, s_pos, s_aux,
-                                                      s_achunk, s_q[lane], it.a_start, jbase, it.a_region, rb, cnt);
+                        bool dfr = false;
+                        float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (lane < qn) {
+                            e = s_q[lane];
+                            dfr = bin_fast<MODE, UNITW, WK, false>(P, J, PA, EA, S, s_pos, s_aux, s_achunk, e,
+                                                                   it.a_start, jbase, it.a_region, rb, cnt);
+                        }
+                        park(dfr, e);
                         __syncwarp();
                     }
+                    while (ns > 0) {
+                        __syncwarp();
+                        if (lane < ns) resolve(s_slow[ns > 32 ? ns - 32 + lane : lane]);
+                        ns = ns > 32 ? ns - 32 : 0;
+                    }
+                    __syncwarp();
                 }
                 // This warp is done with the buffer: the last warp to finish it
                 // refills it with the tile NB ahead (the arrivals of one tile
@@ -2498,8 +2555,6 @@ int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double
     const size_t o_t2 = sp.take(sizeof(float) * std::max<size_t>(bin->t2.size(), 1));
     const size_t o_l1 = sp.take(LUT1_N);
     const size_t o_l2 = sp.take(LUT2_N);
-    const size_t n_flags = req.weighting == WEIGHTS_PLAIN ? 0 : (size_t)(1 + n_jk) * nb;
-    const size_t o_flags = sp.take(sizeof(unsigned) * n_flags);
     const size_t n_up = req.up ? req.up->thr.size() : 0;
     const size_t o_up_thr = sp.take(sizeof(float) * n_up);
     const size_t o_up_bins = sp.take(sizeof(double) * n_up);
@@ -2517,6 +2572,11 @@ int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double
 
     CountPlan C;
     if (plan_count(ctx, req, false, C, err)) return err->status;
+    // non-finite flags: exactly what the kernel and finish_count use (none
+    // for plain weights, and none for an angular count of inverse-p DR
+    // weights, whose plan has plain pair weights)
+    const size_t n_flags = C.n_flags();
+    const size_t o_flags = sp.take(sizeof(unsigned) * n_flags);
     const size_t o_items = sp.take(sizeof(WorkItem) * C.items.size());
     const size_t o_segs = sp.take(sizeof(Segment) * C.segs.size());
     if (sp.total > kStaticScratchBytes) return too_big(C.items.size(), C.segs.size());
