@@ -17,17 +17,25 @@ paths' histograms checked.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--scale f]
 
-Under torchrun each rank runs its own seeded copy of the workload (weak
-scaling, no data-path collective); the step time is the max over ranks.
+With --gpus N > 1 (started plainly, bench.py re-launches itself under
+torch.distributed.run with N ranks; under torchrun it uses the ranks it is
+given) one workload is split over the ranks: every count runs its share of
+the work items on each rank's GPU and one all-reduce of the exact int64
+partial sums -- NCCL when every rank has its own GPU, gloo when ranks share
+one -- gives every rank the histograms of the whole count (strong scaling).
+--replicas runs one seeded copy of the workload per rank instead (weak
+scaling, no exchange).  The step time is the max over ranks.
 """
 from __future__ import annotations
 
 import argparse
 import json
 import os
+import socket
 import statistics
 import subprocess
 import sys
+import tempfile
 import time
 
 import numpy as np
@@ -54,8 +62,15 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--strong", action="store_true",
-                   help="with --gpus N > 1: one workload, every count split over the ranks (strong scaling); "
-                        "default: one workload replica per rank (weak scaling)")
+                   help="with --gpus N > 1: one workload, every count split over the ranks (the default)")
+    p.add_argument("--replicas", action="store_true",
+                   help="with --gpus N > 1: one seeded workload replica per rank, no exchange (weak scaling)")
+    p.add_argument("--gloo", action="store_true", help="exchange over gloo on the host even with a GPU per rank")
+    p.add_argument("--save-hists", default=None,
+                   help="rank 0 writes the last FP32+guard step's histograms (full, regions per count) to this .npz")
+    p.add_argument("--exchange-selftest", action="store_true",
+                   help="launcher check without a GPU: the ranks reduce known partial sums through the sharded "
+                        "count's exchange and rank 0 prints whether every rank combined them exactly")
     p.add_argument("--one-count", choices=["s_mu", "sigma_pi"], default=None,
                    help="profiling case: one RR count of the workload's randoms at --scale, then exit")
     p.add_argument("--workload", choices=["survey", "mocks", "invp", "adjoint"], default="survey",
@@ -202,24 +217,61 @@ def other_workload(args):
     ctx.close()
 
 
-def dist_setup():
+def relaunch(args) -> int:
+    """bench.py --gpus N started without torchrun: run it again as N ranks
+    under torch.distributed.run (127.0.0.1, a free port) and return their
+    exit status."""
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={args.gpus}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *sys.argv[1:]]
+    return subprocess.call(cmd)
+
+
+def dist_setup(args):
+    """(world size, rank, local GPU index, backend).  NCCL when every rank
+    has a GPU of its own, gloo when ranks share one (NCCL refuses two ranks
+    on one device) or without a GPU.  NCCL_DEBUG=INFO unless set: its
+    communicator lines record the ranks of the exchange."""
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    backend = None
+    if ws > 1 and os.environ.get("OMP_NUM_THREADS") == "1":
+        # torchrun's default of one thread per rank would serialise the host
+        # planning of each count (work lists, tables): give every rank its
+        # share of the host cores before the engine library loads
+        per = max(1, (os.cpu_count() or 1) // int(os.environ.get("LOCAL_WORLD_SIZE", str(ws))))
+        os.environ["OMP_NUM_THREADS"] = str(per)
     if ws > 1:
+        import datetime
+        import torch
         import torch.distributed as dist
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
-        import datetime
-        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=600))
-    return ws, rank, local
+        n_dev = torch.cuda.device_count() if torch.cuda.is_available() else 0
+        if n_dev:
+            local = local % n_dev
+        backend = "nccl" if (n_dev >= ws and not args.gloo and not args.exchange_selftest) else "gloo"
+        if backend == "nccl":
+            os.environ.setdefault("NCCL_DEBUG", "INFO")
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=180))
+    return ws, rank, local, backend
+
+
+def _dist_tensor(x: float):
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    return torch.tensor([x], dtype=torch.float64, device=dev)
 
 
 def dist_max(x: float, ws: int) -> float:
     if ws == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
+    t = _dist_tensor(x)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -227,9 +279,8 @@ def dist_max(x: float, ws: int) -> float:
 def dist_sum(x: float, ws: int) -> float:
     if ws == 1:
         return x
-    import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64)
+    t = _dist_tensor(x)
     dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
@@ -238,6 +289,34 @@ def dist_barrier(ws: int):
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()
+
+
+def exchange_selftest(ws: int, rank: int):
+    """Every rank holds one shard's share of known 128-bit totals as int64
+    limbs; the sharded count's exchange (two_pcf_b200.reduce_partials) adds
+    them and tpcf_shard_combine converts; rank 0 prints whether every rank
+    got the totals exactly."""
+    import numpy as np
+    import torch.distributed as dist
+    import two_pcf_b200 as tp
+    from two_pcf_b200 import _capi
+    b = tp.Binning(None, tp.SIGMA_PI, (0.0, 40.0, 1.0, 6), (0.0, 40.0, 1.0, 6), 2)
+    rng = np.random.default_rng(5)
+    n_slots, se, words = 3 * b.nb, 20, _capi.PARTIAL_WORDS
+    totals = [int(rng.integers(-2**62, 2**62)) << int(rng.integers(0, 60)) for _ in range(n_slots)]
+    mine = np.zeros((n_slots, words), np.int64)
+    for k, t in enumerate(totals):
+        parts = [int(rng.integers(0, 2**63)) << int(rng.integers(0, 64)) for _ in range(ws - 1)]
+        parts.append(t - sum(parts))
+        u = parts[rank] & ((1 << 128) - 1)
+        mine[k, :4] = [(u >> (32 * j)) & 0xffffffff for j in range(4)]
+    full, reg = tp.shard_combine(b, tp.reduce_partials(mine, se), se)
+    ok = np.array_equal(np.concatenate([full, reg.ravel()]), np.array([float(t) * 2.0 ** -se for t in totals]))
+    flags = _dist_tensor(1.0 if ok else 0.0)
+    dist.all_reduce(flags)
+    if rank == 0:
+        print(json.dumps({"exchange_selftest": bool(int(flags.item()) == ws), "n_ranks": ws,
+                          "backend": dist.get_backend()}))
 
 
 def make_workload(seed: int, scale: float):
@@ -257,10 +336,10 @@ class ClockSampler:
     def __init__(self, device: int):
         self.device = device
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_{os.getpid()}.csv")
+        self.dir = tempfile.mkdtemp(prefix="tpcf_clocks_")
+        self.path = os.path.join(self.dir, "clocks.csv")
 
     def __enter__(self):
-        os.makedirs(os.path.dirname(self.path), exist_ok=True)
         try:
             self.fh = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}",
@@ -296,6 +375,8 @@ class ClockSampler:
             for nm, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
                     reasons.add(nm)
+        import shutil
+        shutil.rmtree(self.dir, ignore_errors=True)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "samples": len(sm),
                 "reasons": sorted(reasons)}
 
@@ -455,9 +536,20 @@ def main():
     if args.workload != "survey":
         other_workload(args)
         return
-    ws, rank, local = dist_setup()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        sys.exit(relaunch(args))
+    ws, rank, local, backend = dist_setup(args)
+    if args.exchange_selftest:
+        exchange_selftest(ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
     if args.impl == "reference":
         run_reference_arm(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
         return
     import torch
     import two_pcf_b200 as tp
@@ -466,7 +558,7 @@ def main():
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
 
-    sharded = args.strong and ws > 1
+    sharded = ws > 1 and not args.replicas
     w = make_workload(2 if sharded else 2 + rank, args.scale)
     n_jk = w["n_jk"]
     d, r = w["data"], w["rand"]
@@ -591,7 +683,8 @@ def main():
                    "scale": args.scale, "n_data": int(d["xyz"].shape[0]), "n_rand": int(r["xyz"].shape[0]),
                    "l2": "inputs larger than L2 (sorted tiles 192 MB + catalogues) and a 256 MB L2 flush "
                          "between steps",
-                   "parallelism": (f"shards{ws}" if sharded else f"replicas{ws}") if ws > 1 else "single"},
+                   "parallelism": (f"shards{ws}" if sharded else f"replicas{ws}") if ws > 1 else "single",
+                   "exchange": backend if sharded else None},
         "in_range_pairs_per_step": tot_in // args.steps, "candidates_per_step": tot_cand // args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops, "unit": "TFLOP/s",
                      "frac": achieved / fp32_tflops if fp32_tflops else None,
@@ -612,6 +705,10 @@ def main():
     }
     if rank == 0:
         print(json.dumps(line))
+        if args.save_hists:
+            names = [f"{m}_{c}" for m in ("sigma_pi", "s_mu") for c in ("dd", "dr", "rr")]
+            np.savez(args.save_hists, **{f"{n}_full": h[0] for n, h in zip(names, hists)},
+                     **{f"{n}_regions": h[1] for n, h in zip(names, hists)})
     ctx.close()
     if ws > 1:
         import torch.distributed as dist

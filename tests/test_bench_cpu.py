@@ -37,3 +37,21 @@ def test_kdtree_tally_matches_the_reference_range_test():
         want += (float_range_pairs(xd, xd, max_sq, True) + float_range_pairs(xd, xr, max_sq, False)
                  + float_range_pairs(xr, xr, max_sq, True))
     assert got == want and got > 0
+
+
+def test_gpus_2_launches_two_ranks_and_reduces_exactly():
+    """bench.py --gpus 2 started plainly re-launches itself as two ranks
+    (torch.distributed.run on 127.0.0.1); without a GPU the ranks exchange
+    over gloo.  The exchange of the sharded count (reduce_partials, then
+    tpcf_shard_combine) must give both ranks the known totals exactly."""
+    import json
+    import os
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py"), "--gpus", "2", "--exchange-selftest"],
+                       capture_output=True, text=True, timeout=300, cwd=root, env=env)
+    assert r.returncode == 0, r.stderr[-2000:]
+    line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
+    assert line == {"exchange_selftest": True, "n_ranks": 2, "backend": "gloo"}

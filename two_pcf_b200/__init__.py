@@ -359,23 +359,33 @@ def count_sharded(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning,
     one GPU per rank: each rank runs its shard and one all-reduce (SUM over
     int64 limbs) adds the partial sums, so every rank returns exactly what
     count() returns.  Returns (full, regions, stats of this rank's shard)."""
-    import torch
     import torch.distributed as dist
     if not (dist.is_available() and dist.is_initialized()):
         partial, se, st = count_shard(ctx, a, b, binning, 0, 1, precision, weights)
         return (*shard_combine(binning, partial, se), st)
     rank, world = dist.get_rank(group), dist.get_world_size(group)
     partial, se, st = count_shard(ctx, a, b, binning, rank, world, precision, weights)
+    full, reg = shard_combine(binning, reduce_partials(partial, se, group), se)
+    return full, reg, st
+
+
+def reduce_partials(partial, scale_exp: int, group=None):
+    """The exchange step of a sharded count: every rank's partial sums
+    (int64 limbs, count_shard) added by one all-reduce SUM over the process
+    group -- on the GPU for an NCCL group, on the host for gloo -- after
+    checking that all ranks planned the same fixed-point scale.  Returns the
+    summed limbs (as numpy) for shard_combine."""
+    import torch
+    import torch.distributed as dist
     on_gpu = dist.get_backend(group) == "nccl"
     dev = torch.device("cuda", torch.cuda.current_device()) if on_gpu else torch.device("cpu")
-    t = torch.from_numpy(partial).to(dev)
-    chk = torch.tensor([se, -se], dtype=torch.int64, device=dev)
+    t = torch.from_numpy(np.ascontiguousarray(partial, np.int64)).to(dev)
+    chk = torch.tensor([scale_exp, -scale_exp], dtype=torch.int64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     dist.all_reduce(chk, op=dist.ReduceOp.MAX, group=group)
-    if int(chk[0]) != se or -int(chk[1]) != se:
+    if int(chk[0]) != scale_exp or -int(chk[1]) != scale_exp:
         raise TpcfError(_capi.TPCF_E_INVALID_ARG, "shards disagree on the fixed-point scale: different inputs per rank")
-    full, reg = shard_combine(binning, t.cpu().numpy(), se)
-    return full, reg, st
+    return t.cpu().numpy()
 
 
 def upweight_eval(weights: Weights, values) -> np.ndarray:
