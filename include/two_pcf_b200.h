@@ -463,6 +463,20 @@ int tpcf_write_xi_ascii(const char *filename, const tpcf_binning *bin, const dou
  * library).  log: 0 quiet, 1 one line per step on stderr. */
 int tpcf_run_param_file(const char *path, int device, int precision, int log);
 
+/* tpcf_run_param_file with a run report (no counterpart in the reference,
+ * which prints only its ASCII outputs).  summary_path non-NULL: a JSON
+ * summary is written there, also when the run fails (its status and error):
+ * catalogue sizes read and kept, wall time, and per mode and count the
+ * in-range pairs, candidates, guard re-evaluations, kernel time and pairs/s.
+ * check_fp64 != 0 (with precision TPCF_FP32_GUARD): every count runs again on
+ * the plain FP64 path and the summary gives, per output (DD, DR, RR raw and
+ * normalised; xi; full histogram and every region's slice), the largest
+ * relative and absolute difference from the FP64 result and whether they
+ * agree bit for bit.  The ASCII outputs are those of the run's own
+ * precision. */
+int tpcf_run_param_file_report(const char *path, int device, int precision, int log, int check_fp64,
+                               const char *summary_path);
+
 /* The inverse-p program after its catalogues are read (src/main.cpp:51-60):
  * the angular stage of calc_angular_upweight
  * (src/correlators_invpweight.cpp:985-1033) — angular DD (every point,

@@ -20,10 +20,12 @@ can tell that it counts the same catalogue.
   the 100-region counts can be compared bit for bit.
 
 Per count (DD auto, DR cross, RR auto) the fixture holds the histograms as
-the reference leaves them after invert_jk_hists and (auto) x2, the number of
-points the grid kept, and per mode the normalised histograms
-(JKHists::normalise, src/hist.cpp:290-367, :512-589) and the Landy-Szalay xi
-(src/io.cpp:643-651) of the full sample and of every jackknife slice.  On 8
+the reference leaves them after invert_jk_hists and (auto) x2 -- the full
+histogram and every jackknife region's slice -- and the number of points the
+grid kept; per mode, the normalised full histograms (JKHists::normalise,
+src/hist.cpp:290-367, :512-589) and the Landy-Szalay xi (src/io.cpp:643-651)
+of the full sample.  (The normalised slices and their xi follow from the
+stored histograms and would triple the file.)  On 8
 host threads the box takes under a minute and each survey fixture about
 three quarters of an hour.
 """
@@ -101,12 +103,10 @@ def run(cat, modes, n_threads):
         ndd, nsdd = refl.normalise(True, wd, jd, None, None, n_jk, *res["dd"])
         ndr, nsdr = refl.normalise(False, wd, jd, wr, jr, n_jk, *res["dr"])
         nrr, nsrr = refl.normalise(True, wr, jr, None, None, n_jk, *res["rr"])
-        for lab, v in (("dd", (ndd, nsdd)), ("dr", (ndr, nsdr)), ("rr", (nrr, nsrr))):
-            out[f"{tag}_{lab}_norm_full"] = v[0]
-            out[f"{tag}_{lab}_norm_sub"] = v[1]
+        for lab, v in (("dd", ndd), ("dr", ndr), ("rr", nrr)):
+            out[f"{tag}_{lab}_norm_full"] = v
         with np.errstate(divide="ignore", invalid="ignore"):
             out[f"{tag}_xi_full"] = ls(ndd, ndr, nrr)
-            out[f"{tag}_xi_sub"] = ls(nsdd, nsdr, nsrr)
     return out
 
 

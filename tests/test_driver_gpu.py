@@ -123,3 +123,53 @@ def test_cli_errors(tmp_path):
     assert e.value.status == _capi.TPCF_E_UNSUPPORTED
     r = subprocess.run([CLI], capture_output=True, text=True, timeout=60)
     assert r.returncode == 1 and "usage" in r.stderr
+
+
+@pytest.mark.parametrize("case", ["box_weighted_jk", "sky_unit"])
+def test_cli_summary_reports_error_against_fp64(tmp_path, case):
+    """two_pcf --summary FILE --check-fp64: the JSON run summary gives every
+    mode's counts and, per output, the largest difference from the plain FP64
+    path.  The two paths sum the same float pair weights exactly in fixed
+    point, so every raw and normalised histogram and every xi agrees bit for
+    bit; the report must say so, and its pair counts must add up."""
+    g = _gen()
+    out_dir = tmp_path / "out"
+    out_dir.mkdir()
+    params, _ = g.write_inputs(case, str(tmp_path), str(out_dir))
+    summ = tmp_path / "summary.json"
+    _run_ours(params, "--summary", str(summ), "--check-fp64")
+    s = json.load(open(summ))
+    assert s["status"] == 0 and s["error"] is None and s["fp64_check"] is True
+    assert s["precision"] == "fp32_guard" and s["catalogues"]["data"]["kept"] > 0
+    assert len(s["modes"]) >= 1
+    pairs = 0
+    for m in s["modes"]:
+        for lab in ("DD", "DR", "RR"):
+            c = m["counts"][lab]
+            assert c["in_range_pairs"] > 0 and c["kernel_ms"] > 0 and c["pairs_per_s"] > 0
+            pairs += c["in_range_pairs"]
+            for key in (lab, lab + "_raw"):
+                e = m["fp64_check"][key]
+                assert e["bit_identical"] and e["max_rel_err"] == 0.0 and e["nonfinite_mismatch"] == 0
+                assert e["values"] == (1 + m["n_jk_regions"]) * m["bins"]
+        assert m["fp64_check"]["xi"]["max_rel_err"] == 0.0
+    assert s["in_range_pairs"] == pairs
+    # the same through the Python wrapper, which returns the summary
+    s2 = ingest.run_param_file(params, check_fp64=True, summary=str(tmp_path / "s2.json"))
+    assert [m["mode"] for m in s2["modes"]] == [m["mode"] for m in s["modes"]]
+    assert [m["counts"]["RR"]["in_range_pairs"] for m in s2["modes"]] == \
+        [m["counts"]["RR"]["in_range_pairs"] for m in s["modes"]]
+    assert all(m["fp64_check"]["xi"]["bit_identical"] for m in s2["modes"])
+
+
+def test_cli_summary_of_a_failed_run(tmp_path):
+    g = _gen()
+    params, _ = g.write_inputs("sky_unit", str(tmp_path), str(tmp_path))
+    bad = tmp_path / "hdf5.ini"
+    bad.write_text(open(params).read().replace("data_file_type = ascii", "data_file_type = hdf5"))
+    summ = tmp_path / "summary.json"
+    r = subprocess.run([CLI, str(bad), "--quiet", "--summary", str(summ)], capture_output=True, text=True,
+                       timeout=120)
+    assert r.returncode == 2
+    s = json.load(open(summ))
+    assert s["status"] == _capi.TPCF_E_UNSUPPORTED and "HDF5" in s["error"] and s["modes"] == []

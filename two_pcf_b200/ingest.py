@@ -211,9 +211,25 @@ def write_xi_ascii(filename: str, binning, dd, dr, rr, dd_sub=None, dr_sub=None,
     _check(_capi.lib().tpcf_write_xi_ascii(str(filename).encode(), binning._h, *[_ptr(a) for a in arrs]))
 
 
-def run_param_file(path: str, device: int = 0, precision: int = FP32_GUARD, log: bool = False):
-    """The reference's program on a parameter file, counts on the GPU."""
-    _check(_capi.lib().tpcf_run_param_file(str(path).encode(), int(device), int(precision), int(bool(log))))
+def run_param_file(path: str, device: int = 0, precision: int = FP32_GUARD, log: bool = False,
+                   check_fp64: bool = False, summary: str | None = None):
+    """The reference's program on a parameter file, counts on the GPU.
+    summary: path of a JSON run summary (tpcf_run_param_file_report);
+    check_fp64: also count on the plain FP64 path and report every output's
+    difference from it in the summary.  Returns the summary as a dict when
+    one was written, else None."""
+    L = _capi.lib()
+    if summary is None and not check_fp64:
+        _check(L.tpcf_run_param_file(str(path).encode(), int(device), int(precision), int(bool(log))))
+        return None
+    rc = L.tpcf_run_param_file_report(str(path).encode(), int(device), int(precision), int(bool(log)),
+                                      int(bool(check_fp64)), None if summary is None else str(summary).encode())
+    _check(rc)
+    if summary is None:
+        return None
+    import json
+    with open(summary) as f:
+        return json.load(f)
 
 
 def run_invp(ctx, params: Params, data, randoms, precision: int = FP32_GUARD, dither: bool = False,
