@@ -107,8 +107,16 @@ def other_workload(args):
                angular DD, DD-inverse-p, DR, DR-inverse-p (40 log bins, base
                1.6, theta < 0.175 rad), then the 3-D s-mu inverse-p DD and DR
                with the up-weights from those histograms;
-    adjoint -- the survey slab at scale: s-mu DD, DR, RR forward, and the
-               adjoint (per-point dL/dw) of the same counts."""
+    adjoint -- the weight-gradient workload on the survey slab at scale:
+               weights w = exp(theta . f) with 8 standardised smooth random
+               Fourier fields f over ra/dec and theta ~ N(0, 0.05); loss =
+               sum over s-mu bins of (xi - xi_target)^2, xi_target from an
+               independent clustered catalogue of the same footprint with unit
+               weights.  Forward: s-mu DD, DR, RR; backward: dL/d(histogram)
+               from the normalisation and Landy-Szalay chain, then the adjoint
+               (per-point dL/dw) of the three counts and dL/dtheta.
+
+    Every line carries the clock record of its timed region."""
     import two_pcf_b200 as tp
     from two_pcf_b200 import synthetic
     ctx = tp.Context(0)
@@ -125,6 +133,8 @@ def other_workload(args):
         return statistics.median(ms), out
 
     line = {"workload": args.workload, "scale": scale, "unit": UNIT, "dtype": "f32", "data": "synthetic"}
+    clk = ClockSampler(0)
+    clk.__enter__()
     if args.workload == "mocks":
         box, n_mocks = 1000.0, 64
 
@@ -192,26 +202,70 @@ def other_workload(args):
     else:
         w = make_workload(2, scale)
         d, r = w["data"], w["rand"]
-        D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], w["n_jk"])
-        R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
-        b = tp.Binning(ctx, tp.S_MU, *S_MU_AXES, w["n_jk"])
+        b = tp.Binning(ctx, tp.S_MU, *S_MU_AXES, 1)
+
+        def feats(c, seed):
+            rs = np.random.default_rng(seed)
+            f = np.empty((c["ra"].size, 8))
+            for j in range(8):
+                a1, a2 = rs.normal(0, 0.3, 2)
+                f[:, j] = np.cos(a1 * c["ra"] + a2 * c["dec"] + rs.uniform(0, 2 * np.pi))
+            return (f - f.mean(0)) / f.std(0)
+        fd, fr = feats(d, 21), feats(r, 22)
+        theta = rng.normal(0, 0.05, 8)
+        wd = np.exp(fd @ theta).astype(np.float32)
+        wr = np.exp(fr @ theta).astype(np.float32)
+        D = tp.Catalog(ctx, d["xyz"], d["x_norm"], d["d_comov"], wd)
+        R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], wr)
+        # target: an independent clustered catalogue, unit weights, same randoms
+        wt = synthetic.survey_catalogue(seed=31, n_data=d["xyz"].shape[0], n_rand=1000)["data"]
+        T = tp.Catalog(ctx, wt["xyz"], wt["x_norm"], wt["d_comov"])
+        R1 = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"])
+        nt, nr_ = wt["xyz"].shape[0], r["xyz"].shape[0]
+        tdd, tdr, trr = (tp.count(ctx, a, bb, b, with_regions=False)[0] for a, bb in ((T, None), (T, R1), (R1, None)))
+        tn_dd = 2 * tdd / (nt * nt * (1 - 1 / nt))
+        tn_rr = 2 * trr / (nr_ * nr_ * (1 - 1 / nr_))
+        with np.errstate(divide="ignore", invalid="ignore"):
+            xi_t = np.where(tn_rr > 0, (tn_dd - 2 * tdr / (nt * nr_)) / np.where(tn_rr > 0, tn_rr, 1) + 1, 0.0)
         jobs = [(D, None), (D, R), (R, None)]
-        G = rng.standard_normal(b.nb)
+        sd, sr = float(wd.astype(np.float64).sum()), float(wr.astype(np.float64).sum())
+        nd_ = d["xyz"].shape[0]
+        kd, kr = sd * sd * (1 - 1 / nd_), sr * sr * (1 - 1 / nr_)
 
         def fwd():
-            out = [tp.count(ctx, a, bb, b) for a, bb in jobs]
+            out = [tp.count(ctx, a, bb, b, with_regions=False) for a, bb in jobs]
             return sum(o[2]["ms_kernel"] for o in out), out
         ms_f, (_, fo) = median_ms(fwd)
+        # dL/d(raw histograms) from the normalisation (JKHists::normalise of
+        # the doubled auto counts) and the Landy-Szalay chain
+        f_dd, f_dr, f_rr = (o[0] for o in fo)
+        ndd, ndr, nrr = 2 * f_dd / kd, f_dr / (sd * sr), 2 * f_rr / kr
+        ok = nrr > 0
+        safe = np.where(ok, nrr, 1)
+        xi = np.where(ok, (ndd - 2 * ndr) / safe + 1, 0.0)
+        loss = float(((xi - xi_t) ** 2).sum())
+        gx = np.where(ok, 2 * (xi - xi_t), 0.0)
+        g_ndd, g_ndr, g_nrr = gx / safe, -2 * gx / safe, -gx * (ndd - 2 * ndr) / safe ** 2
+        Gs = [2 * g_ndd / kd, g_ndr / (sd * sr), 2 * g_nrr / kr]
 
         def bwd():
-            out = [tp.count_backward(ctx, a, bb, b, G) for a, bb in jobs]
+            out = [tp.count_backward(ctx, a, bb, b, G) for (a, bb), G in zip(jobs, Gs)]
             return sum(o[2]["ms_kernel"] for o in out), out
-        ms_b, _ = median_ms(bwd)
+        ms_b, (_, bo) = median_ms(bwd)
+        # per-object dL/dw: adjoint of the pair sums plus the weight-sum terms
+        # of the normalisation; dL/dtheta = sum_i dL/dw_i w_i f_i
+        gd = bo[0][0] + bo[1][0] - 2 * (g_ndd * ndd).sum() / sd - (g_ndr * ndr).sum() / sd
+        gr = bo[1][1] + bo[2][0] - 2 * (g_nrr * nrr).sum() / sr - (g_ndr * ndr).sum() / sr
+        dtheta = (gd * wd) @ fd + (gr * wr) @ fr
         pairs = sum(o[2]["in_range"] for o in fo)
-        line.update({"metric": "in-range pairs/sec of forward + backward (s-mu DD, DR, RR)",
+        line.update({"metric": "in-range pairs/sec of forward + backward (s-mu DD, DR, RR, loss on xi)",
                      "value": pairs / ((ms_f + ms_b) * 1e-3), "ms": ms_f + ms_b, "forward_ms": ms_f,
                      "backward_ms": ms_b, "forward_plus_backward_over_forward": (ms_f + ms_b) / ms_f,
-                     "pairs": pairs, "n_data": int(d["xyz"].shape[0]), "n_rand": int(r["xyz"].shape[0])})
+                     "pairs": pairs, "n_data": int(nd_), "n_rand": int(nr_), "loss": loss,
+                     "dL_dtheta": [float(x) for x in dtheta], "dL_dw_data_rms": float(np.sqrt((gd ** 2).mean())),
+                     "dL_dw_rand_rms": float(np.sqrt((gr ** 2).mean()))})
+    clk.__exit__()
+    line["clocks"] = clk.summary()
     line["steps"], line["warmup"] = args.steps, args.warmup
     print(json.dumps(line))
     ctx.close()

@@ -233,3 +233,32 @@ def test_weight_gradient_vs_fp64_cpu_and_finite_differences(ctx, setup):
             d.append((loss_theta(th0 + e) - loss_theta(th0 - e)) / (2 * h))
         fd = (4 * d[1] - d[0]) / 3
         assert abs(fd - gth[k]) <= 3e-6 * np.abs(gth).max(), (k, fd, gth[k], d)
+
+
+def test_theta_chain_rule_at_fixed_float_weights(ctx, setup):
+    """dL/dtheta at the spec's tolerance, apart from the float rounding of
+    the weights: the weights are held at their float values, dL/dw comes from
+    the FP64 CPU gradient (oracle pair sums and adjoint), dw/dtheta from
+    central differences with step 1e-6 of w = exp(theta . f) in double, and
+    sum_i dL/dw_i dw_i/dtheta must equal the GPU's dL/dtheta (autograd through
+    the adjoint kernel) to 1e-6 relative."""
+    s = setup
+    rng = np.random.default_rng(6)
+    theta = torch.tensor(rng.normal(0, 0.05, 8), dtype=torch.float64, requires_grad=True)
+    Fd, Fr = torch.from_numpy(s["fd"]), torch.from_numpy(s["fr"])
+    wd = torch.exp(Fd @ theta)
+    wr = torch.exp(Fr @ theta)
+    torch_loss(ctx, s, wd, wr).backward()
+    g_gpu = theta.grad.numpy().copy()
+    w32d = wd.detach().numpy().astype(np.float32).astype(np.float64)
+    w32r = wr.detach().numpy().astype(np.float32).astype(np.float64)
+    _, gdc, grc = cpu_loss_and_grad(s, w32d, w32r)
+    th0, h = theta.detach().numpy(), 1e-6
+    chain = np.empty(8)
+    for k in range(8):
+        e = np.zeros(8)
+        e[k] = h
+        dwd = (np.exp(s["fd"] @ (th0 + e)) - np.exp(s["fd"] @ (th0 - e))) / (2 * h)
+        dwr = (np.exp(s["fr"] @ (th0 + e)) - np.exp(s["fr"] @ (th0 - e))) / (2 * h)
+        chain[k] = gdc @ dwd + grc @ dwr
+    np.testing.assert_allclose(g_gpu, chain, rtol=1e-6, atol=1e-6 * np.abs(chain).max())
