@@ -85,3 +85,36 @@ def test_batch_fp64_path(ctx):
             f1, r1, _ = tp.count(ctx, m, other, b, tp.FP32_GUARD)
             assert np.array_equal(full[2 * i + k], f1)
             assert np.array_equal(reg[2 * i + k], r1)
+
+
+@pytest.mark.parametrize("weighted", [False, True])
+def test_batch_matches_oracle(ctx, weighted):
+    """The batch's job table straight against the oracle: mocks of uneven
+    size, 27 sub-cube regions, every mock's DD and DR in one launch.  The
+    oracle returns the reference's convention (delete-one slices, auto counts
+    doubled); the batch returns raw sums and the sums touching each region,
+    so the oracle's slices are turned back: touching = full - slice."""
+    from oracle import port
+    ms = mocks(7, [1800, 5200, 3100], weighted)
+    rng = np.random.default_rng(8)
+    xr = rng.uniform(0, BOX, (9000, 3))
+    R = catalog(ctx, xr, None)
+    M = [catalog(ctx, x, w) for x, w in ms]
+    b = tp.Binning(ctx, tp.S_MU, AX1, AX2, 27)
+    full, reg, _ = tp.Batch(ctx, M, R, b, what=tp.BATCH_DD | tp.BATCH_DR).run()
+    pr = port.Cat(xr, jk=subcube_jk(xr).astype(np.int32))
+    for i, (x, w) in enumerate(ms):
+        pm = port.Cat(x, w=w, jk=subcube_jk(x).astype(np.int32))
+        for k, other in ((0, None), (1, pr)):
+            auto = other is None
+            of, osub, _ = port.count_3d(port.S_MU, pm, other, is_auto=auto, n_jk=27, axes=AX1 + AX2)
+            scale = 0.5 if auto else 1.0
+            want_full = of * scale
+            want_reg = (of[None, :] - osub) * scale
+            if weighted:
+                np.testing.assert_allclose(full[2 * i + k], want_full, rtol=1e-12, atol=1e-9)
+                np.testing.assert_allclose(reg[2 * i + k], want_reg, rtol=1e-12, atol=1e-9)
+            else:
+                assert np.array_equal(full[2 * i + k], want_full)
+                assert np.array_equal(reg[2 * i + k], want_reg)
+            assert want_full.sum() > 0
