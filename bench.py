@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--replicas", action="store_true",
                    help="with --gpus N > 1: one seeded workload replica per rank, no exchange (weak scaling)")
     p.add_argument("--gloo", action="store_true", help="exchange over gloo on the host even with a GPU per rank")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="the refinement rule and default kernel configuration instead of the count autotuner "
+                        "(the warm-up steps absorb the autotuner's probes)")
     p.add_argument("--save-hists", default=None,
                    help="rank 0 writes the last FP32+guard step's histograms (full, regions per count) to this .npz")
     p.add_argument("--exchange-selftest", action="store_true",
@@ -611,6 +614,7 @@ def main():
     ctx = tp.Context(local)
     stream = torch.cuda.Stream(device=local)
     ctx.set_stream(stream.cuda_stream)
+    ctx.set_autotune(not args.no_autotune)
 
     sharded = ws > 1 and not args.replicas
     w = make_workload(2 if sharded else 2 + rank, args.scale)
@@ -756,6 +760,7 @@ def main():
                      "kernel_ms_per_step": tot_kms / args.steps,
                      "smem_atomic_peak_per_s": atom_rate},
         "fp64_path": fp64, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
+        "autotune": ctx.autotune_table() if not args.no_autotune else None,
     }
     if rank == 0:
         print(json.dumps(line))

@@ -79,6 +79,31 @@ const char *tpcf_last_error(const tpcf_ctx *ctx);
 int tpcf_set_stream(tpcf_ctx *ctx, void *cuda_stream);
 /* Cells per maximum separation (1..3; 0 = automatic). */
 int tpcf_set_refinement(tpcf_ctx *ctx, int cells_per_rmax);
+/* Autotuning of counts (no counterpart in the reference, whose cell side is
+ * always the maximum separation, src/boxes.cpp:56-59).  on != 0: the first
+ * count of each class (mode, regions, weights, precision, bins, auto or
+ * cross, and the catalogues' points per cell of side r_max to within a
+ * factor of two) probes cells of 1, 2 and 3 per maximum separation and, for
+ * the plain-weight FP32+guard kernels, both kernel configurations, each on a
+ * strided sample of its work items, and keeps the one that counted the most
+ * in-range pairs per second for every later count of the class in this
+ * context.  Results do not depend on the choice.  A fixed refinement or
+ * kernel configuration (here or per call) turns the tuning off; sharded
+ * counts are never tuned. */
+int tpcf_set_autotune(tpcf_ctx *ctx, int on);
+/* Kernel configuration of the plain-weight FP32+guard kernels: 0 the default
+ * per kind (jackknife kernels: three tile buffers of 256 points, ballots of
+ * four A slots between queue checks; kernels without regions: two buffers,
+ * two slots), 1 the alternative (jackknife: two buffers of 512 points, two
+ * slots; without regions: three buffers, four slots), -1 automatic (the
+ * autotuner's choice when it runs, else 0).  Same results either way. */
+int tpcf_set_kernel_config(tpcf_ctx *ctx, int cfg);
+/* The autotuner's choices so far as JSON text: a list of {"class", "refinement",
+ * "kernel_config", "pairs_per_s": [m = 1, 2, 3 with configuration 0, then with
+ * configuration 1; 0 where not probed]}.  Writes at most len bytes including
+ * the terminating NUL; returns the length the full text needs (without the
+ * NUL), or a negative status. */
+int64_t tpcf_autotune_describe(const tpcf_ctx *ctx, char *buf, int64_t len);
 int tpcf_synchronize(tpcf_ctx *ctx);
 
 /* A catalogue resident on the device: the Galaxy fields of src/galaxy.h:16-35.

@@ -73,6 +73,28 @@ class Context:
     def set_refinement(self, m: int):
         _check(_capi.lib().tpcf_set_refinement(self._h, int(m)), self)
 
+    def set_autotune(self, on: bool = True):
+        """Autotuning of counts (tpcf_set_autotune): the first count of each
+        class probes the refinement and kernel configuration; later counts of
+        the class use the fastest."""
+        _check(_capi.lib().tpcf_set_autotune(self._h, int(bool(on))), self)
+
+    def set_kernel_config(self, cfg: int):
+        """Kernel configuration of the plain-weight FP32+guard kernels (0, 1;
+        -1 automatic)."""
+        _check(_capi.lib().tpcf_set_kernel_config(self._h, int(cfg)), self)
+
+    def autotune_table(self) -> list:
+        """The autotuner's choices so far (tpcf_autotune_describe)."""
+        import json
+        L = _capi.lib()
+        n = L.tpcf_autotune_describe(self._h, None, 0)
+        if n < 0:
+            _check(int(-n), self)
+        buf = C.create_string_buffer(int(n) + 1)
+        L.tpcf_autotune_describe(self._h, buf, int(n) + 1)
+        return json.loads(buf.value.decode())
+
     def set_stream(self, stream_handle: int | None):
         _check(_capi.lib().tpcf_set_stream(self._h, C.c_void_p(stream_handle or 0)), self)
 

@@ -125,6 +125,9 @@ _PROTOTYPES = {
     "tpcf_sub_filename": (C.c_int, [C.c_char_p, C.c_int64, C.c_char_p, C.c_int32]),
     "tpcf_write_xi_ascii": (C.c_int, [C.c_char_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "tpcf_run_param_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int]),
+    "tpcf_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "tpcf_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
+    "tpcf_autotune_describe": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int64]),
     "tpcf_run_param_file_report": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p]),
     "tpcf_run_invp": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, C.c_int]),
 }

@@ -4,11 +4,14 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <new>
+#include <string>
 #include <vector>
 
 #include "capi_types.h"
@@ -136,6 +139,43 @@ int tpcf_set_refinement(tpcf_ctx *ctx, int m) {
     if (!ctx || m < 0 || m > 3) return TPCF_E_INVALID_ARG;
     ctx->c.refinement = m;
     return TPCF_OK;
+}
+
+int tpcf_set_autotune(tpcf_ctx *ctx, int on) {
+    if (!ctx) return TPCF_E_INVALID_ARG;
+    ctx->c.autotune = on != 0;
+    return TPCF_OK;
+}
+
+int tpcf_set_kernel_config(tpcf_ctx *ctx, int cfg) {
+    if (!ctx || cfg < -1 || cfg > 1) return TPCF_E_INVALID_ARG;
+    ctx->c.kernel_cfg = cfg;
+    return TPCF_OK;
+}
+
+int64_t tpcf_autotune_describe(const tpcf_ctx *ctx, char *buf, int64_t len) {
+    if (!ctx || len < 0 || (len > 0 && !buf)) return -TPCF_E_INVALID_ARG;
+    std::string j = "[";
+    bool first = true;
+    for (const auto &kv : ctx->c.tuned) {
+        j += first ? "" : ", ";
+        first = false;
+        j += "{\"class\": \"" + kv.first + "\", \"refinement\": " + std::to_string(kv.second.m) +
+             ", \"kernel_config\": " + std::to_string(kv.second.cfg) + ", \"pairs_per_s\": [";
+        for (size_t k = 0; k < kv.second.rate.size(); ++k) {
+            char b[32];
+            std::snprintf(b, sizeof b, "%s%.6g", k ? ", " : "", kv.second.rate[k]);
+            j += b;
+        }
+        j += "]}";
+    }
+    j += "]";
+    if (len > 0) {
+        const size_t n = std::min<size_t>(j.size(), (size_t)len - 1);
+        std::memcpy(buf, j.data(), n);
+        buf[n] = '\0';
+    }
+    return (int64_t)j.size();
 }
 
 int tpcf_synchronize(tpcf_ctx *ctx) {

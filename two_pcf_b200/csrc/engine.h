@@ -76,6 +76,15 @@ struct Ctx {
     bool own_stream = false;
     std::string last_error;
     int refinement = 0;  // 0 = automatic
+    int kernel_cfg = -1;  // -1 = automatic (the autotuner's choice when it runs, else 0)
+    // autotuning of counts: the (refinement, kernel configuration) chosen per
+    // count class by timed probes, kept for the context's lifetime
+    bool autotune = false;
+    struct Tuned {
+        int m = 0, cfg = 0;
+        std::vector<double> rate;  // in-range pairs/s of each candidate probed (m 1-3 x cfg 0-1; 0 = not probed)
+    };
+    std::map<std::string, Tuned> tuned;
     unsigned long long launches = 0;  // kernels launched by this context
     cudaMemPool_t pool = nullptr;     // stream-ordered pool for the scratch of each call
     // pinned staging of the counts in flight in count_many (two slots, grown
@@ -316,6 +325,9 @@ struct CountRequest {
     long long *raw_out = nullptr;
     int *scale_exp_out = nullptr;
     int refinement = 0;
+    // kernel configuration of the plain-weight FP32+guard kernels (0 or 1;
+    // -1: the context's setting, else the autotuner's choice, else 0)
+    int kernel_cfg = -1;
     // adjoint of a plain-weight 3-D count: with adj_G = dL/d(raw full
     // histogram) set, the count writes per-point dL/dw into grad_a (n_all of
     // a) and grad_b (n_all of b; unused for auto counts) instead of histograms

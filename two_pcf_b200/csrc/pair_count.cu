@@ -48,7 +48,8 @@ constexpr int R = 4;           // A points per thread
 constexpr int TA = NT * R;     // A chunk
 constexpr int TB = 256;        // B points per staged tile (FP32 path)
 constexpr int TB_EXACT = 256;  // B points per staged tile (FP64 path)
-constexpr int kTileMax = TB > TB_EXACT ? TB : TB_EXACT;
+constexpr int TB_ALT = 512;    // the alternative configuration of the FP32 jackknife kernels
+constexpr int kTileMax = TB_ALT > TB_EXACT ? TB_ALT : TB_EXACT;
 // Staged tile buffers (warps may run up to NBUF - 1 tiles apart): FP32 path,
 // FP64 path (whose per-pair loads of the double arrays lose L1 to a third
 // buffer; measured on the survey benchmark, each path at its faster depth)
@@ -58,10 +59,22 @@ constexpr int kNbufMax = NBUF > NBUF_EXACT ? NBUF : NBUF_EXACT;
 // Count kernels without jackknife regions keep the lighter settings (two
 // buffers, a push width of 2) so that their shared memory allows three CTAs
 // per SM (the adjoint runs two CTAs per SM either way and keeps the others).
+//
+// Kernel configuration `cfg` (plain-weight FP32+guard kernels; the autotuner
+// picks it per count class): 0 is the setting above for each kind; 1 swaps
+// the kinds' settings -- the jackknife kernels take the light ring (two
+// buffers, push width 2) with tiles of TB_ALT points, the kernels without
+// regions the heavy one (three buffers, push width 4).
 constexpr int NBUF_NOJK = 2;
-__host__ __device__ constexpr bool light_fast(bool exact, bool jk, bool adj) { return !exact && !jk && !adj; }
-__host__ __device__ constexpr int n_buffers(bool exact, bool jk, bool adj) {
-    return exact ? NBUF_EXACT : (light_fast(exact, jk, adj) ? NBUF_NOJK : NBUF);
+__host__ __device__ constexpr bool light_fast(bool exact, bool jk, bool adj, int cfg = 0) {
+    return !exact && !adj && (cfg == 0 ? !jk : jk);
+}
+__host__ __device__ constexpr int n_buffers(bool exact, bool jk, bool adj, int cfg = 0) {
+    return exact ? NBUF_EXACT : (light_fast(exact, jk, adj, cfg) ? NBUF_NOJK : NBUF);
+}
+// B points per staged tile
+__host__ __device__ constexpr int tile_points(bool exact, bool jk, bool adj, int cfg = 0) {
+    return exact ? TB_EXACT : ((cfg == 1 && jk && !adj) ? TB_ALT : TB);
 }
 // queue entries pack (A chunk index << kTileShift | tile index)
 constexpr int kTileShift = kTileMax <= 256 ? 8 : (kTileMax <= 512 ? 9 : 10);
@@ -73,8 +86,8 @@ static_assert(16 + 12 * kNbufMax <= 64 && kTileMax <= 1024 && (size_t)TA << kTil
 constexpr int QPUSH = 4;
 constexpr int QPUSH_NOJK = 2;
 __host__ __device__ constexpr int qpush_exact(int mode) { return mode == MODE_S_MU ? 4 : 2; }
-__host__ __device__ constexpr int queue_cap(bool exact, bool jk, bool adj) {
-    return 32 + 32 * (light_fast(exact, jk, adj) ? QPUSH_NOJK : 4);
+__host__ __device__ constexpr int queue_cap(bool exact, bool jk, bool adj, int cfg = 0) {
+    return 32 + 32 * (light_fast(exact, jk, adj, cfg) ? QPUSH_NOJK : 4);
 }
 static_assert(R % QPUSH == 0 && R % QPUSH_NOJK == 0 && R % 2 == 0 && QPUSH <= 4 && QPUSH_NOJK <= 4,
               "the push loops consume after every QPUSH A slots");
@@ -178,11 +191,14 @@ struct SmemLayout {
 constexpr int kSlowCap = 64;
 
 // FP32 path: pos and aux float4 per point; FP64 path: one double4 per point
-__host__ __device__ inline size_t tile_bytes(bool exact) { return exact ? (size_t)TB_EXACT * 32 : (size_t)TB * 32; }
+__host__ __device__ inline size_t tile_bytes(bool exact, bool jk, bool adj, int cfg) {
+    return (size_t)tile_points(exact, jk, adj, cfg) * 32;
+}
 
 // lo/hi: the histogram pairs are added to (per segment region when there
 // are jackknife regions); alo/ahi: the item's A-side total (jackknife only).
-__host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk, bool adj = false) {
+__host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk, bool adj = false,
+                                                  int cfg = 0) {
     SmemLayout L;
     size_t o = 0;
     L.lo = o;
@@ -203,7 +219,7 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     o += LUT2_N;
     o = (o + 15) / 16 * 16;
     L.queue = o;
-    o += (size_t)NWARP * queue_cap(exact, jk, adj) * 16;
+    o += (size_t)NWARP * queue_cap(exact, jk, adj, cfg) * 16;
     L.slow = o;
     if (!exact) o += (size_t)NWARP * kSlowCap * 4;
     L.achunk = o;  // FP32 path: (x_norm, weight) of the item's A chunk
@@ -214,9 +230,9 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     if (adj) o += (size_t)TB * 8;
     o = (o + 127) / 128 * 128;
     L.tile0 = o;
-    o += tile_bytes(exact);
+    o += tile_bytes(exact, jk, adj, cfg);
     L.tile1 = o;
-    o += (size_t)(n_buffers(exact, jk, adj) - 1) * tile_bytes(exact);
+    o += (size_t)(n_buffers(exact, jk, adj, cfg) - 1) * tile_bytes(exact, jk, adj, cfg);
     o = (o + 15) / 16 * 16;
     L.misc = o;  // item index, mbarriers, tile-done counters, the item's job
     o += 64 + sizeof(JobK);
@@ -712,15 +728,15 @@ __device__ __forceinline__ void add64_owned(uint32_t *lo, uint32_t *hi, int i, u
     hi[i] = hi[i] + vh + ((old + vl) < old ? 1u : 0u);
 }
 
-template <int MODE, bool UNITW, bool JK, bool EXACT, int WK>
-__global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParams P) {
+template <int MODE, bool UNITW, bool JK, bool EXACT, int WK, int CFG = 0>
+__global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kernel(const KParams P) {
     extern __shared__ __align__(128) unsigned char smem[];
     constexpr bool kNeedAux = (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU);
     constexpr bool ADJ = (WK == W_ADJ);
-    constexpr int TBK = EXACT ? TB_EXACT : TB;  // B points per tile
-    constexpr int NB = n_buffers(EXACT, JK, ADJ);                        // tile buffers
-    constexpr int QPF = light_fast(EXACT, JK, ADJ) ? QPUSH_NOJK : QPUSH;  // FP32 path push width
-    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ);
+    constexpr int TBK = tile_points(EXACT, JK, ADJ, CFG);                     // B points per tile
+    constexpr int NB = n_buffers(EXACT, JK, ADJ, CFG);                        // tile buffers
+    constexpr int QPF = light_fast(EXACT, JK, ADJ, CFG) ? QPUSH_NOJK : QPUSH;  // FP32 path push width
+    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ, CFG);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
     uint32_t *s_alo = (uint32_t *)(smem + L.alo);
@@ -737,7 +753,7 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
     unsigned *s_done = (unsigned *)(smem + L.misc + 16 + 8 * kNbufMax);  // warps done with each buffer (running count)
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float4 *s_q = (float4 *)(smem + L.queue) + warp * queue_cap(EXACT, JK, ADJ);
+    float4 *s_q = (float4 *)(smem + L.queue) + warp * queue_cap(EXACT, JK, ADJ, CFG);
     int *s_slow = (int *)(smem + L.slow) + warp * kSlowCap;
     const unsigned lt_mask = (1u << lane) - 1u;
     const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo),
@@ -1196,11 +1212,19 @@ __global__ void __launch_bounds__(NT, JK ? 2 : 3) pair_count_kernel(const KParam
 typedef void (*KernelFn)(const KParams);
 
 template <int MODE, int WK>
-KernelFn pick_kernel(bool unitw, bool jk, bool exact) {
+KernelFn pick_kernel(bool unitw, bool jk, bool exact, int cfg = 0) {
     if constexpr (WK == W_ADJ) {  // no regions, per-point weights
         return exact ? pair_count_kernel<MODE, false, false, true, WK> : pair_count_kernel<MODE, false, false, false, WK>;
     } else {
         if constexpr (WK == W_PLAIN) {
+            // the alternative configuration (plain-weight FP32+guard kernels)
+            if (cfg == 1 && !exact) {
+                if (unitw)
+                    return jk ? pair_count_kernel<MODE, true, true, false, WK, 1>
+                              : pair_count_kernel<MODE, true, false, false, WK, 1>;
+                return jk ? pair_count_kernel<MODE, false, true, false, WK, 1>
+                          : pair_count_kernel<MODE, false, false, false, WK, 1>;
+            }
             if (unitw) {
                 if (exact)
                     return jk ? pair_count_kernel<MODE, true, true, true, WK>
@@ -1216,25 +1240,25 @@ KernelFn pick_kernel(bool unitw, bool jk, bool exact) {
 }
 
 template <int MODE>
-KernelFn pick_3d(int wk, bool unitw, bool jk, bool exact) {
+KernelFn pick_3d(int wk, bool unitw, bool jk, bool exact, int cfg) {
     switch (wk) {
     case W_INVP_DD: return pick_kernel<MODE, W_INVP_DD>(unitw, jk, exact);
     case W_INVP_DR: return pick_kernel<MODE, W_INVP_DR>(unitw, jk, exact);
     case W_ADJ: return pick_kernel<MODE, W_ADJ>(unitw, jk, exact);
-    default: return pick_kernel<MODE, W_PLAIN>(unitw, jk, exact);
+    default: return pick_kernel<MODE, W_PLAIN>(unitw, jk, exact, cfg);
     }
 }
 
 // Kernel for a mode, weight kind (W_PLAIN, W_INVP_DD, W_INVP_DR for 3-D;
 // W_PLAIN, W_ANG_INVP for angular), unit weights, jackknife and precision.
-KernelFn pick(int mode, int wk, bool unitw, bool jk, bool exact) {
+KernelFn pick(int mode, int wk, bool unitw, bool jk, bool exact, int cfg = 0) {
     switch (mode) {
-    case MODE_MONOPOLE: return pick_3d<MODE_MONOPOLE>(wk, unitw, jk, exact);
-    case MODE_SIGMA_PI: return pick_3d<MODE_SIGMA_PI>(wk, unitw, jk, exact);
-    case MODE_S_MU: return pick_3d<MODE_S_MU>(wk, unitw, jk, exact);
+    case MODE_MONOPOLE: return pick_3d<MODE_MONOPOLE>(wk, unitw, jk, exact, cfg);
+    case MODE_SIGMA_PI: return pick_3d<MODE_SIGMA_PI>(wk, unitw, jk, exact, cfg);
+    case MODE_S_MU: return pick_3d<MODE_S_MU>(wk, unitw, jk, exact, cfg);
     default:
         return wk == W_ANG_INVP ? pick_kernel<MODE_ANGULAR, W_ANG_INVP>(unitw, jk, exact)
-                                : pick_kernel<MODE_ANGULAR, W_PLAIN>(unitw, jk, exact);
+                                : pick_kernel<MODE_ANGULAR, W_PLAIN>(unitw, jk, exact, cfg);
     }
 }
 
@@ -1461,6 +1485,10 @@ struct CountPlan {
     Luts luts;
     KParams P;
     KernelFn fn = nullptr;
+    int m = 0;              // cells per maximum separation
+    int cfg = 0;            // kernel configuration
+    bool cfg_tunable = false;  // plain-weight FP32+guard count: both configurations exist
+    double dens_a = 0, dens_b = 0;  // points per cell of side rb (the autotuner's density class)
     size_t n_flags() const { return wk == W_PLAIN ? 0 : (size_t)(1 + n_jk) * nb; }
     size_t n_up() const { return up ? up->thr.size() : 0; }
 };
@@ -1595,6 +1623,19 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         norm_dev = std::max(A->norm_dev, B->norm_dev);
         rb = std::sqrt(2.0 * tn + 4e-15 + 2.0 * norm_dev) * (1.0 + 1e-6) + 1e-12;
     }
+    auto per_cell = [&](const Catalog *X, int k) {
+        const double *lo = C.angular ? (subset ? X->ulo_kept : X->ulo_all) : X->lo_kept;
+        const double *hi = C.angular ? (subset ? X->uhi_kept : X->uhi_all) : X->hi_kept;
+        const double n = subset ? (double)X->n_kept : (double)X->n_all;
+        double vol = 1;
+        for (int d = 0; d < 3; ++d) vol *= std::max(hi[d] - lo[d], rb);
+        const double c = rb / k;
+        return n * c * c * c / vol;
+    };
+    C.dens_a = per_cell(A, 1);
+    C.dens_b = per_cell(B, 1);
+    C.cfg_tunable = C.wk == W_PLAIN && !req.exact_fp64 && !C.adj;
+    C.cfg = C.cfg_tunable ? (req.kernel_cfg >= 0 ? req.kernel_cfg : std::max(ctx->kernel_cfg, 0)) : 0;
     int m = req.refinement > 0 ? req.refinement : ctx->refinement;
     if (m <= 0) {
         // Automatic: refine to side rb/2 when cells of that size would still
@@ -1606,18 +1647,10 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         // to side rb/3 once the A catalogue holds ~50 points per such cell
         // (measured on the survey benchmark: 3-8 % faster on each count that
         // meets it; the FP32 path gains under 1 % there and keeps rb/2).
-        auto per_cell = [&](const Catalog *X, int k) {
-            const double *lo = C.angular ? (subset ? X->ulo_kept : X->ulo_all) : X->lo_kept;
-            const double *hi = C.angular ? (subset ? X->uhi_kept : X->uhi_all) : X->hi_kept;
-            const double n = subset ? (double)X->n_kept : (double)X->n_all;
-            double vol = 1;
-            for (int d = 0; d < 3; ++d) vol *= std::max(hi[d] - lo[d], rb);
-            const double c = rb / k;
-            return n * c * c * c / vol;
-        };
         m = std::max(per_cell(A, 2), per_cell(B, 2)) >= 256 ? 2 : 1;
         if (req.exact_fp64 && per_cell(A, 3) >= 50) m = 3;
     }
+    C.m = m;
     const double side = rb / m * (1.0 + 1e-9);
     GridSpec gs;
     gs.side = side;
@@ -1693,7 +1726,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         C.items.swap(mine);
     }
     C.raw_out = req.raw_out;
-    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk, C.adj);
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk, C.adj, C.cfg);
     if (C.L.total + 1024 > ctx->smem_optin) {
         err->status = 6;
         err->msg = "histogram does not fit in shared memory";
@@ -1726,7 +1759,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         return (q & (a - 1)) == 0;
     };
     P.mask_vec = (P.n_mask % 4 == 0 && aligned(32)) ? 4 : ((P.n_mask % 2 == 0 && aligned(16)) ? 2 : 1);
-    C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64);
+    C.fn = pick(bin->mode, C.wk, C.unitw, C.jk, req.exact_fp64, C.cfg);
     return 0;
 }
 
@@ -2087,9 +2120,95 @@ int pinned_slot(Ctx *ctx, int k, size_t bytes, unsigned char **out, size_t *cap,
     return 0;
 }
 
+// ---- autotuning of counts (Ctx::autotune)
+//
+// A count class -- mode, regions, unit or plain weights, precision, weight
+// kind, auto or cross, number of bins, and the two catalogues' points per
+// cell of side r_max to within a factor of two -- gets the refinement (1-3
+// cells per r_max) and kernel configuration whose timed probe counted the
+// most in-range pairs per second.  A probe runs one candidate on a strided
+// sample of its own work list (every k-th item, at least 32 per SM, so the
+// ramp-down of the last wave weighs little); its histograms are discarded.
+// Every candidate gives the same histograms: any complete cell scheme visits
+// the same pairs, and the configurations differ only in staging.  The
+// choice is kept in the context; sharded counts are not tuned (every rank
+// must plan the same work list).
+std::string tune_key(const CountPlan &C, const CountRequest &req) {
+    auto lg = [](double v) { return (int)std::floor(std::log2(std::max(v, 1e-9))); };
+    char b[160];
+    std::snprintf(b, sizeof b, "mode %d, regions %d, unit weights %d, fp64 %d, weight kind %d, auto %d, bins %d, "
+                  "density 2^%d / 2^%d", C.bin->mode, C.jk ? 1 : 0, C.unitw ? 1 : 0, req.exact_fp64 ? 1 : 0, C.wk,
+                  C.is_auto ? 1 : 0, C.nb, lg(C.dens_a), lg(C.dens_b));
+    return b;
+}
+
+int tune_probe(Ctx *ctx, const CountRequest &req, int m, int cfg, double *rate, Error *err) {
+    CountRequest r = req;
+    r.refinement = m;
+    r.kernel_cfg = cfg;
+    CountPlan C;
+    if (plan_count(ctx, r, true, C, err)) return err->status;
+    const size_t want = std::max<size_t>((size_t)32 * ctx->num_sms, C.items.size() / 16);
+    if (C.items.size() > want) {
+        const size_t stride = C.items.size() / want;
+        std::vector<WorkItem> sample;
+        sample.reserve(C.items.size() / stride + 1);
+        for (size_t k = 0; k < C.items.size(); k += stride) sample.push_back(C.items[k]);
+        C.items.swap(sample);
+        C.P.n_items = (int)C.items.size();
+    }
+    CountScratch S;
+    if (alloc_scratch(ctx, C, S, err)) return err->status;
+    std::vector<double> full(C.nb), reg((size_t)C.nb * std::max(C.n_jk, 1));
+    Stats st;
+    if (execute(ctx, C, S.D, full.data(), reg.data(), &st, err, true)) return err->status;
+    *rate = st.ms_kernel > 0 ? (double)st.in_range / (st.ms_kernel * 1e-3) : 0.0;
+    return 0;
+}
+
+// The tuned refinement and kernel configuration into `req` (probing the
+// count's class the first time it is met).  Leaves `req` as it is when
+// autotuning is off or the caller fixed either choice.
+int autotune(Ctx *ctx, CountRequest &req, Error *err) {
+    if (!ctx->autotune || req.adj_G || req.n_shards > 1 || req.refinement > 0 || ctx->refinement > 0 ||
+        req.kernel_cfg >= 0 || ctx->kernel_cfg >= 0)
+        return 0;
+    CountPlan C0;
+    if (plan_count(ctx, req, true, C0, err, true)) return err->status;
+    const std::string key = tune_key(C0, req);
+    auto it = ctx->tuned.find(key);
+    if (it == ctx->tuned.end()) {
+        Ctx::Tuned t;
+        t.rate.assign(6, 0.0);
+        double best = -1.0;
+        for (int cfg = 0; cfg < (C0.cfg_tunable ? 2 : 1); ++cfg)
+            for (int m = 1; m <= 3; ++m) {
+                double r = 0.0;
+                if (tune_probe(ctx, req, m, cfg, &r, err)) return err->status;
+                t.rate[(size_t)(m - 1) + 3 * (size_t)cfg] = r;
+                if (r > best) {
+                    best = r;
+                    t.m = m;
+                    t.cfg = cfg;
+                }
+            }
+        if (trace_enabled()) {
+            std::fprintf(stderr, "[tpcf trace] autotune %s: pairs/s", key.c_str());
+            for (double r : t.rate) std::fprintf(stderr, " %.3g", r);
+            std::fprintf(stderr, " -> refinement %d, configuration %d\n", t.m, t.cfg);
+        }
+        it = ctx->tuned.emplace(key, t).first;
+    }
+    req.refinement = it->second.m;
+    req.kernel_cfg = it->second.cfg;
+    return 0;
+}
+
 }  // namespace
 
-int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *region_out, Stats *st, Error *err) {
+int run_count(Ctx *ctx, const CountRequest &req_in, double *full_out, double *region_out, Stats *st, Error *err) {
+    CountRequest req = req_in;
+    if (autotune(ctx, req, err)) return err->status;
     CountPlan C;
     if (plan_count(ctx, req, true, C, err)) return err->status;
     if (req.scale_exp_out) *req.scale_exp_out = C.scale_exp;
@@ -2098,7 +2217,11 @@ int run_count(Ctx *ctx, const CountRequest &req, double *full_out, double *regio
     return execute(ctx, C, S.D, full_out, region_out, st, err, true);
 }
 
-int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs, const std::vector<CountOut> &outs, Error *err) {
+int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs_in, const std::vector<CountOut> &outs,
+                   Error *err) {
+    std::vector<CountRequest> reqs(reqs_in);
+    for (CountRequest &r : reqs)
+        if (autotune(ctx, r, err)) return err->status;
     // TPCF_TRACE=1: one stderr line per count with its host planning time
     // and where its kernel ran on the device, in ms from the call's start
     // (diagnostics of the pipelining; the counts are unchanged)
