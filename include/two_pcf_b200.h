@@ -29,7 +29,8 @@ typedef enum {
     TPCF_E_CUDA = 3,            /* any other CUDA runtime error */
     TPCF_E_DEVICE_TIMEOUT = 4,  /* a bounded device wait gave up; results discarded */
     TPCF_E_OVERFLOW = 5,        /* a fixed-point histogram bin would overflow */
-    TPCF_E_UNSUPPORTED = 6      /* configuration outside the engine's limits */
+    TPCF_E_UNSUPPORTED = 6,     /* configuration outside the engine's limits */
+    TPCF_E_DEVICE_CHECK = 7     /* a device bounds check failed (checked build only); results discarded */
 } tpcf_status;
 
 typedef enum {
@@ -400,6 +401,21 @@ int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit);
  * one fails as out of memory until this is called with after < 0.  The
  * failing call returns an error status and releases what it had allocated. */
 int tpcf_debug_fail_allocations(int64_t after);
+
+/* Device bounds checks (no counterpart in the reference).  The checked build
+ * of this library (TPCF_DEVICE_CHECKS=1 python two_pcf_b200/build.py, written
+ * to two_pcf_b200/lib/checked/) tests, in every count kernel, every index a
+ * work item and its segments carry (segment range, A chunk, cells, regions,
+ * B runs, job), every bin index and every queue fill against its bounds
+ * before use; the first failure stops the count, which returns
+ * TPCF_E_DEVICE_CHECK naming the check, the value and the limit, and no
+ * access leaves its buffer.  tpcf_device_checks() is 1 in that build, 0 in
+ * the release build.  tpcf_debug_corrupt_work_list(1), checked build only
+ * (process-wide, for tests): the next count's first segment gets a region
+ * past the histogram rows after planning, on the host; the release build
+ * returns TPCF_E_UNSUPPORTED. */
+int tpcf_device_checks(void);
+int tpcf_debug_corrupt_work_list(int what);
 
 /* ---------------------------------------------------------------------------
  * The command-line flow around the counts (src/main.cpp:11-84): parameter

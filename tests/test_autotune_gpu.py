@@ -27,6 +27,8 @@ def cats():
     bx = synthetic.box_catalogue(seed=3, n_data=30_000, n_rand=60_000, box=300.0, n_centres=600)
     BD, BR = tp.Catalog(c, bx["data"]["xyz"]), tp.Catalog(c, bx["rand"]["xyz"])
     yield {"ctx": c, "D": D, "R": R, "n_jk": w["n_jk"], "BD": BD, "BR": BR}
+    for cat in (D, R, BD, BR):
+        cat.close()
     c.close()
 
 

@@ -130,3 +130,26 @@ def test_reference_binning_monotone_exhaustive(spec, sq, hi):
     L.orc_axis_check_monotone.restype = C.c_uint
     ax = port.axis(*spec)
     assert L.orc_axis_check_monotone(C.byref(ax), sq, 0.0, hi) == 0xFFFFFFFF
+
+
+def test_release_build_has_no_device_checks():
+    """The release library reports no device checks and refuses the test hook
+    that would plant a bad index (nothing there would catch it)."""
+    L = _capi.lib()
+    assert L.tpcf_device_checks() == 0
+    assert L.tpcf_debug_corrupt_work_list(1) == _capi.TPCF_E_UNSUPPORTED
+    assert L.tpcf_status_string(_capi.TPCF_E_DEVICE_CHECK).decode() == "device bounds check failed"
+
+
+def test_checked_build_exports_the_same_symbols():
+    import ctypes
+    import os
+    import subprocess
+    path = _capi.CHECKED_LIB_PATH
+    if not os.path.exists(path):
+        pytest.skip("checked build absent (TPCF_DEVICE_CHECKS=1 python two_pcf_b200/build.py)")
+    out = subprocess.run(["nm", "-D", "--defined-only", path], capture_output=True, text=True, check=True).stdout
+    exported = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    assert set(_capi._PROTOTYPES) <= exported
+    L = ctypes.CDLL(path)
+    assert L.tpcf_device_checks() == 1

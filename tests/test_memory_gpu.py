@@ -64,9 +64,10 @@ def test_catalogue_outlives_its_context():
     st = tp.Stats()
     assert L.tpcf_count(h, cat, None, b, tp.FP32_GUARD, full.ctypes.data_as(C.c_void_p), None, C.byref(st)) == 0
     assert full.sum() > 0
-    assert L.tpcf_destroy(h) == 0          # context first: its pool goes, the catalogue's memory stays valid
-    assert L.tpcf_catalog_destroy(cat) == 0
+    assert L.tpcf_destroy(h) == 0          # context first: its pool stays while the catalogue holds memory from it
+    assert L.tpcf_catalog_destroy(cat) == 0   # frees into that pool, which then goes
     assert L.tpcf_binning_destroy(b) == 0
+    _free_bytes()                          # a device-wide synchronisation completes the frees
     # the device is still healthy
     ctx = tp.Context(0)
     c2 = tp.Catalog(ctx, x)

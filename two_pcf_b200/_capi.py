@@ -10,6 +10,10 @@ import ctypes as C
 import os
 
 LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "libtpcf_b200.so")
+# the checked build (device bounds checks) of the same library
+CHECKED_LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "lib", "checked", "libtpcf_b200.so")
+if os.environ.get("TPCF_CHECKED") == "1":
+    LIB_PATH = CHECKED_LIB_PATH
 
 TPCF_OK = 0
 TPCF_E_INVALID_ARG = 1
@@ -18,6 +22,7 @@ TPCF_E_CUDA = 3
 TPCF_E_DEVICE_TIMEOUT = 4
 TPCF_E_OVERFLOW = 5
 TPCF_E_UNSUPPORTED = 6
+TPCF_E_DEVICE_CHECK = 7
 
 MONOPOLE, SIGMA_PI, S_MU, ANGULAR = 0, 1, 2, 3
 FP32_GUARD, FP64 = 0, 1
@@ -126,6 +131,8 @@ _PROTOTYPES = {
     "tpcf_write_xi_ascii": (C.c_int, [C.c_char_p, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "tpcf_run_param_file": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int]),
     "tpcf_set_autotune": (C.c_int, [C.c_void_p, C.c_int]),
+    "tpcf_device_checks": (C.c_int, []),
+    "tpcf_debug_corrupt_work_list": (C.c_int, [C.c_int]),
     "tpcf_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
     "tpcf_autotune_describe": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int64]),
     "tpcf_run_param_file_report": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p]),

@@ -62,6 +62,7 @@ const char *tpcf_status_string(int status) {
     case TPCF_E_DEVICE_TIMEOUT: return "device wait timed out";
     case TPCF_E_OVERFLOW: return "histogram overflow";
     case TPCF_E_UNSUPPORTED: return "unsupported configuration";
+    case TPCF_E_DEVICE_CHECK: return "device bounds check failed";
     default: return "unknown status";
     }
 }
@@ -93,12 +94,15 @@ int tpcf_create(int device, tpcf_ctx **out) {
         props.location.id = device;
         e = cudaMemPoolCreate(&ctx->c.pool, &props);
         if (e == cudaSuccess) {
+            ctx->c.pool_ref = std::make_shared<tpcf::PoolRef>();
+            ctx->c.pool_ref->pool = ctx->c.pool;
             uint64_t keep = UINT64_MAX;
             e = cudaMemPoolSetAttribute(ctx->c.pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
     if (e != cudaSuccess) {
-        if (ctx->c.pool) cudaMemPoolDestroy(ctx->c.pool);
+        if (ctx->c.pool && !ctx->c.pool_ref) cudaMemPoolDestroy(ctx->c.pool);
+        ctx->c.pool_ref.reset();
         if (ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
         delete ctx;
         return TPCF_E_CUDA;
@@ -114,7 +118,9 @@ int tpcf_destroy(tpcf_ctx *ctx) {
     if (ctx->c.stream) cudaStreamSynchronize(ctx->c.stream);
     for (unsigned char *p : ctx->c.pinned)
         if (p) cudaFreeHost(p);
-    if (ctx->c.pool) cudaMemPoolDestroy(ctx->c.pool);
+    // the pool goes with the last array allocated from it (PoolRef): arrays of
+    // catalogues that outlive the context still free into it
+    ctx->c.pool_ref.reset();
     if (ctx->c.own_stream && ctx->c.stream) cudaStreamDestroy(ctx->c.stream);
     delete ctx;
     return TPCF_OK;
@@ -964,6 +970,25 @@ int tpcf_measure_peaks(tpcf_ctx *ctx, double *fp32_tflops, double *smem_atomics_
 int tpcf_debug_fail_allocations(int64_t after) {
     tpcf::alloc_fail_budget().store(after < 0 ? -1 : (long long)after);
     return TPCF_OK;
+}
+
+int tpcf_debug_corrupt_work_list(int what) {
+#ifdef TPCF_DEVICE_CHECKS
+    if (what != 0 && what != 1) return TPCF_E_INVALID_ARG;
+    tpcf::debug_corrupt_work_list().store(what);
+    return TPCF_OK;
+#else
+    (void)what;
+    return TPCF_E_UNSUPPORTED;  // the release build has no device checks to catch it
+#endif
+}
+
+int tpcf_device_checks(void) {
+#ifdef TPCF_DEVICE_CHECKS
+    return 1;
+#else
+    return 0;
+#endif
 }
 
 int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit) {

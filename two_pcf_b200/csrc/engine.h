@@ -46,6 +46,14 @@ inline std::atomic<long long> &alloc_fail_budget() {
     static std::atomic<long long> budget{-1};
     return budget;
 }
+// Checked build only (tpcf_debug_corrupt_work_list): 1 = give the next
+// count's first segment a region past the histogram rows, on the host after
+// planning, so the device bounds checks have something to find.
+inline std::atomic<int> &debug_corrupt_work_list() {
+    static std::atomic<int> v{0};
+    return v;
+}
+
 inline bool alloc_injected_failure() {
     auto &b = alloc_fail_budget();
     long long v = b.load(std::memory_order_relaxed);
@@ -68,6 +76,20 @@ struct Error {
     std::string msg;
 };
 
+// A context's stream-ordered memory pool, shared by the context and by every
+// catalogue and grid array allocated from it: the pool is destroyed when the
+// last of them goes, so an array that outlives its context (a catalogue
+// destroyed after tpcf_destroy) frees into a pool that still exists.
+struct PoolRef {
+    cudaMemPool_t pool = nullptr;
+    PoolRef() = default;
+    PoolRef(const PoolRef &) = delete;
+    PoolRef &operator=(const PoolRef &) = delete;
+    ~PoolRef() {
+        if (pool) cudaMemPoolDestroy(pool);  // returns at once; reclaimed once pending frees complete
+    }
+};
+
 struct Ctx {
     int device = 0;
     int num_sms = 148;
@@ -86,7 +108,8 @@ struct Ctx {
     };
     std::map<std::string, Tuned> tuned;
     unsigned long long launches = 0;  // kernels launched by this context
-    cudaMemPool_t pool = nullptr;     // stream-ordered pool for the scratch of each call
+    cudaMemPool_t pool = nullptr;     // stream-ordered pool for the scratch of each call (owned by pool_ref)
+    std::shared_ptr<PoolRef> pool_ref;
     // pinned staging of the counts in flight in count_many (two slots, grown
     // on demand, freed with the context)
     unsigned char *pinned[2] = {nullptr, nullptr};
@@ -141,6 +164,7 @@ struct PoolBuf {
     T *p = nullptr;
     size_t n = 0;
     int device = 0;
+    std::shared_ptr<PoolRef> pool_ref;  // the pool p came from, kept until p is freed
     PoolBuf() = default;
     PoolBuf(const PoolBuf &) = delete;
     PoolBuf &operator=(const PoolBuf &) = delete;
@@ -159,6 +183,7 @@ struct PoolBuf {
         }
         p = nullptr;
         n = 0;
+        pool_ref.reset();  // after the free is queued: the last reference destroys the pool
     }
     cudaError_t alloc(const Ctx &ctx, size_t count) {
         release();
@@ -167,8 +192,12 @@ struct PoolBuf {
         if (alloc_injected_failure()) return cudaErrorMemoryAllocation;
         cudaError_t e = ctx.pool ? cudaMallocFromPoolAsync((void **)&p, count * sizeof(T), ctx.pool, ctx.stream)
                                  : cudaMallocAsync((void **)&p, count * sizeof(T), ctx.stream);
-        if (e == cudaSuccess) n = count;
-        else p = nullptr;
+        if (e == cudaSuccess) {
+            n = count;
+            pool_ref = ctx.pool_ref;
+        } else {
+            p = nullptr;
+        }
         return e;
     }
 };

@@ -104,6 +104,29 @@ constexpr unsigned char LUT_AMB = 255;  // bucket within the guard of an edge
 constexpr unsigned char LUT_EDGE = 128;
 constexpr int kLutEdgeMaxBins = 126;
 constexpr uint32_t kWaitLimit = 1u << 22;
+
+// A count's error record on the device: [0] the flag (0 none, kErrTimeout: a
+// bounded wait gave up, kErrCheck: a device bounds check failed), then for a
+// failed check its id, the value and the limit it broke.  Any flag stops the
+// CTAs from taking further work items and the host discards the results.
+constexpr int kErrWords = 4;
+constexpr int kErrTimeout = 4;
+constexpr int kErrCheck = 8;
+// Device bounds checks of the checked build (TPCF_DEVICE_CHECKS)
+enum DeviceCheck {
+    DC_BIN = 1,       // bin index < bins
+    DC_JOB,           // work item's job < jobs of the launch
+    DC_SEGMENTS,      // work item's segments within the segment list
+    DC_A_CHUNK,       // A chunk length within 0..kChunkA
+    DC_A_POINTS,      // A chunk within grid A's points
+    DC_A_CELL,        // A cell < cells of grid A
+    DC_A_REGION,      // A region < regions
+    DC_B_POINTS,      // segment's B run within grid B's points
+    DC_B_CELL,        // B cell < cells of grid B
+    DC_B_REGION,      // segment's region < regions
+    DC_QUEUE,         // warp queue fill within its capacity
+    DC_SIDE_QUEUE,    // side queue fill within its capacity
+};
 static_assert(TA == kChunkA, "work items are built for chunks of kChunkA points");
 
 struct GridK {
@@ -114,6 +137,7 @@ struct GridK {
     const double4 *unit_s;
     const int3 *coord;
     int kmin0, kmin1, kmin2;
+    int n_pts, n_cells;  // points and dense cells of the grid
     const double *xyz;   // original catalogue arrays (exact path)
     const double *unit;
 };
@@ -132,6 +156,7 @@ struct KParams {
     const WorkItem *items;
     const Segment *segs;
     int n_items;
+    int n_segs, n_jobs;
     int *head;
     double side;
     int n1, n2, nb;
@@ -521,11 +546,56 @@ __device__ __noinline__ void flag_nonfinite(const KParams &P, int bin, int ra, i
     if (rb != ra) atomicOr(&P.flags[(size_t)(1 + rb) * P.nb + bin], f);
 }
 
+#ifdef TPCF_DEVICE_CHECKS
+// Checked build (TPCF_DEVICE_CHECKS): the first index found outside its
+// range is recorded in the count's error record (check id, value, limit)
+// with the flag kErrCheck, which stops further work items and makes the host
+// discard the results and report TPCF_E_DEVICE_CHECK.
+__device__ __noinline__ void dcheck_record(int *err, int id, long long v, long long lim) {
+    if (atomicCAS(err, 0, kErrCheck) == 0) {
+        err[1] = id;
+        err[2] = (int)max(min(v, (long long)INT_MAX), (long long)INT_MIN);
+        err[3] = (int)max(min(lim, (long long)INT_MAX), (long long)INT_MIN);
+    }
+}
+// True when lo <= v <= hi; else records the failure.
+__device__ __forceinline__ bool dcheck(int *err, int id, long long v, long long lo, long long hi) {
+    if (v >= lo && v <= hi) return true;
+    dcheck_record(err, id, v, hi);
+    return false;
+}
+// Every index a work item and its segments carry, against the bounds of the
+// arrays it selects from, before any of its tiles is staged: the item's
+// segment range, A chunk, cell and region, and each segment's B run, cell and
+// region.  Each thread checks the item and every NT-th segment.
+__device__ bool item_in_bounds(const KParams &P, const JobK &J, const WorkItem &it, int tid) {
+    int *e = P.err;
+    bool ok = dcheck(e, DC_SEGMENTS, it.seg_end, 0, P.n_segs) && dcheck(e, DC_SEGMENTS, it.seg_begin, 0, it.seg_end);
+    ok = ok && dcheck(e, DC_A_CHUNK, it.a_len, 0, kChunkA);
+    ok = ok && dcheck(e, DC_A_POINTS, it.a_start, 0, J.a.n_pts) &&
+         dcheck(e, DC_A_POINTS, (long long)it.a_start + it.a_len, 0, J.a.n_pts);
+    ok = ok && dcheck(e, DC_A_CELL, it.a_cell, 0, J.a.n_cells - 1);
+    ok = ok && dcheck(e, DC_A_REGION, it.a_region, 0, P.n_jk - 1);
+    if (!ok) return false;
+    for (int k = it.seg_begin + tid; k < it.seg_end; k += NT) {
+        const Segment sg = P.segs[k];
+        ok = ok && dcheck(e, DC_B_POINTS, sg.b_len, 0, J.b.n_pts) && dcheck(e, DC_B_POINTS, sg.b_start, 0, J.b.n_pts) &&
+             dcheck(e, DC_B_POINTS, (long long)sg.b_start + sg.b_len, 0, J.b.n_pts);
+        ok = ok && dcheck(e, DC_B_CELL, sg.b_cell, 0, J.b.n_cells - 1);
+        ok = ok && dcheck(e, DC_B_REGION, sg.meta & 0xffff, 0, P.n_jk - 1);
+    }
+    return ok;
+}
+#endif
+
 // Add one binned pair: weight from the queue (product of the grid weights)
 // or, for the inverse-p kinds, formed here; fixed-point shared add.
 template <bool UNITW, int WK>
 __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, const Shm &S, int bin, float wa, float wb,
                                            int ia, int jb, int ka, int jl, int ra, int rb) {
+#ifdef TPCF_DEVICE_CHECKS
+    if (WK == W_ADJ && !dcheck(P.err, DC_BIN, bin, 0, P.nb - 1)) return;
+#endif
     if constexpr (WK == W_ADJ) {
         // the pair adds wa * wb to its bin: dL/dwa += G wb, dL/dwb += G wa
         const double g = S.G[bin];
@@ -533,6 +603,9 @@ __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, cons
         dev::acc_add(S.gb_lo, S.gb_hi, jl, __double2ll_rn(g * (double)wa * P.adj_scale));
         return;
     }
+#ifdef TPCF_DEVICE_CHECKS
+    if (!dcheck(P.err, DC_BIN, bin, 0, P.nb - 1)) return;
+#endif
     float w = UNITW ? 1.0f : __fmul_rn(wa, wb);
     if (WK != W_PLAIN) {
         w = pair_weight<WK>(P, J, w, J.a.idx[ia], J.b.idx[jb]);
@@ -719,6 +792,7 @@ __device__ __forceinline__ void bin_exact(const KParams &P, const JobK &J, const
     add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
 }
 
+
 // Add a 64-bit value held as two 32-bit words into another such pair (the
 // caller owns the bin: no atomics).
 __device__ __forceinline__ void add64_owned(uint32_t *lo, uint32_t *hi, int i, unsigned long long v) {
@@ -753,7 +827,8 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
     unsigned *s_done = (unsigned *)(smem + L.misc + 16 + 8 * kNbufMax);  // warps done with each buffer (running count)
     JobK *s_job = (JobK *)(smem + L.misc + 64);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float4 *s_q = (float4 *)(smem + L.queue) + warp * queue_cap(EXACT, JK, ADJ, CFG);
+    constexpr int QCAP = queue_cap(EXACT, JK, ADJ, CFG);  // entries of each warp's queue
+    float4 *s_q = (float4 *)(smem + L.queue) + warp * QCAP;
     int *s_slow = (int *)(smem + L.slow) + warp * kSlowCap;
     const unsigned lt_mask = (1u << lane) - 1u;
     const Shm S{s_t1, s_t2, s_l1, s_l2, s_lo, s_hi, (const double *)(smem + L.lo),
@@ -803,6 +878,10 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
         const int item = s_item[0];
         if (item >= P.n_items) break;
         const WorkItem it = P.items[item];
+#ifdef TPCF_DEVICE_CHECKS
+        // a barrier before skipping: every thread has read the item index
+        if (__syncthreads_or(JK && !dcheck(P.err, DC_JOB, it.job, 0, P.n_jobs - 1))) continue;
+#endif
         if constexpr (JK) {
             // the item's job (grids and output slot), staged for every thread
             const int *src = (const int *)(P.jobs + it.job);
@@ -811,6 +890,9 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
             __syncthreads();
         }
         const JobK &J = JK ? *s_job : P.job0;
+#ifdef TPCF_DEVICE_CHECKS
+        if (__syncthreads_or(!item_in_bounds(P, J, it, tid))) continue;
+#endif
         const ExactArgs EA{J.a.xyz, J.a.unit, J.b.xyz, J.b.unit, P.min_r_sq, P.max_r_sq, P.n1, P.n2, P.los_mid};
     auto issue = [&](unsigned tc, int start, int len) {
         const unsigned buf = tc % NB;
@@ -934,7 +1016,7 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
                 const int tstart = t * TBK;
                 const int tlen = min(TBK, sg.b_len - tstart);
                 if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, kWaitLimit)) {
-                    atomicExch(P.err, 4);  // device timeout: results are discarded by the host
+                    atomicCAS(P.err, 0, kErrTimeout);  // device timeout: results are discarded by the host
                 }
                 const int jbase = sg.b_start + tstart;
                 const int nsteps = (tlen + Pn - 1) / Pn;
@@ -974,6 +1056,9 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
 #pragma unroll
                             for (int r = r0; r < r0 + QPX; ++r) {
                                 const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+#ifdef TPCF_DEVICE_CHECKS
+                                if (!dcheck(P.err, DC_QUEUE, qn + __popc(bal), 0, QCAP)) continue;
+#endif
                                 if (hit[r])
                                     s_q[qn + __popc(bal & lt_mask)] =
                                         make_float4(d0[r], d1[r], d2[r], __int_as_float(apack[r] | jj));
@@ -1012,6 +1097,9 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
                     // packed indices go to the side queue
                     auto park = [&](bool dfr, const float4 &e) {
                         const unsigned bd = __ballot_sync(0xffffffffu, dfr);
+#ifdef TPCF_DEVICE_CHECKS
+                        if (!dcheck(P.err, DC_SIDE_QUEUE, ns + __popc(bd), 0, kSlowCap)) return;
+#endif
                         if (dfr) s_slow[ns + __popc(bd & lt_mask)] = __float_as_int(e.w);
                         ns += __popc(bd);
                     };
@@ -1056,6 +1144,9 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
 #pragma unroll
                                 for (int r = r0; r < r0 + QPF; ++r) {
                                     const unsigned bal = __ballot_sync(0xffffffffu, hit[r]);
+#ifdef TPCF_DEVICE_CHECKS
+                                    if (!dcheck(P.err, DC_QUEUE, qn + __popc(bal), 0, QCAP)) continue;
+#endif
                                     if (hit[r])
                                         s_q[qn + __popc(bal & lt_mask)] =
                                             make_float4(dx[r], dy[r], dz[r], __int_as_float(apack[r] | jj));
@@ -1518,6 +1609,8 @@ void fill_grid(GridK &k, const Grid &gr, const Catalog &c) {
     k.kmin0 = gr.kmin[0];
     k.kmin1 = gr.kmin[1];
     k.kmin2 = gr.kmin[2];
+    k.n_pts = gr.n;
+    k.n_cells = gr.ncell;
     k.xyz = c.xyz.p;
     k.unit = c.unit.p;
 }
@@ -1529,6 +1622,8 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     KParams &P = C.P;
     std::memset(&P, 0, sizeof(P));
     P.n_items = (int)C.items.size();
+    P.n_segs = (int)C.segs.size();
+    P.n_jobs = 1;
     P.side = side;
     P.n1 = bin->nb1;
     P.n2 = (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) ? bin->nb2 : 0;
@@ -1818,6 +1913,10 @@ int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Erro
         const void *s2 = src(h, bytes);
         return bytes ? cudaMemcpyAsync(dst, s2, bytes, cudaMemcpyHostToDevice, stm) : cudaSuccess;
     };
+#ifdef TPCF_DEVICE_CHECKS
+    if (debug_corrupt_work_list().exchange(0) == 1 && !C.segs.empty())
+        C.segs[0].meta = (C.segs[0].meta & ~0xffff) | ((C.n_jk + 3) & 0xffff);
+#endif
     if (!C.items.empty()) {
         TPCF_TRY(h2d(D.items, C.items.data(), sizeof(WorkItem) * C.items.size()));
         TPCF_TRY(h2d(D.segs, C.segs.data(), sizeof(Segment) * C.segs.size()));
@@ -1838,7 +1937,7 @@ int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Erro
     TPCF_TRY(cudaMemsetAsync(D.sub, 0, sizeof(unsigned long long) * 2 * (size_t)nb * n_jk, stm));
     TPCF_TRY(cudaMemsetAsync(D.cnt, 0, sizeof(unsigned long long) * 4, stm));
     TPCF_TRY(cudaMemsetAsync(D.head, 0, sizeof(int), stm));
-    TPCF_TRY(cudaMemsetAsync(D.err, 0, sizeof(int), stm));
+    TPCF_TRY(cudaMemsetAsync(D.err, 0, sizeof(int) * kErrWords, stm));
     if (C.n_flags()) TPCF_TRY(cudaMemsetAsync(D.flags, 0, sizeof(unsigned) * C.n_flags(), stm));
     if (C.adj) {
         TPCF_TRY(h2d(D.adj_G, C.adj_G_host, sizeof(double) * nb));
@@ -1847,6 +1946,8 @@ int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Erro
     }
 
     KParams P = C.P;
+    P.n_segs = (int)C.segs.size();
+    P.n_jobs = (int)C.jobs.size();
     P.jobs = D.jobs;
     P.job0 = C.jobs[0];
     P.items = D.items;
@@ -1892,22 +1993,40 @@ int launch_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, Erro
     if (io.stage) {
         r = io.stage + off;
     } else {
-        io.own.assign(n_hf + n_hs + 4 + 1 + (n_fl + 1) / 2, 0ull);
+        io.own.assign(n_hf + n_hs + 4 + 2 + (n_fl + 1) / 2, 0ull);
         r = reinterpret_cast<unsigned char *>(io.own.data());
     }
     io.hf = reinterpret_cast<unsigned long long *>(r);
     io.hs = io.hf + n_hf;
     io.hc = io.hs + n_hs;
-    io.herr = reinterpret_cast<int *>(io.hc + 4);
-    io.hflags = reinterpret_cast<unsigned *>(io.hc + 5);
+    io.herr = reinterpret_cast<int *>(io.hc + 4);   // kErrWords ints
+    io.hflags = reinterpret_cast<unsigned *>(io.hc + 6);
     TPCF_TRY(cudaMemcpyAsync(io.hf, D.full, sizeof(unsigned long long) * n_hf, cudaMemcpyDeviceToHost, stm));
     TPCF_TRY(cudaMemcpyAsync(io.hs, D.sub, sizeof(unsigned long long) * n_hs, cudaMemcpyDeviceToHost, stm));
     TPCF_TRY(cudaMemcpyAsync(io.hc, D.cnt, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm));
-    TPCF_TRY(cudaMemcpyAsync(io.herr, D.err, sizeof(int), cudaMemcpyDeviceToHost, stm));
+    TPCF_TRY(cudaMemcpyAsync(io.herr, D.err, sizeof(int) * kErrWords, cudaMemcpyDeviceToHost, stm));
     if (n_fl) TPCF_TRY(cudaMemcpyAsync(io.hflags, D.flags, sizeof(unsigned) * n_fl, cudaMemcpyDeviceToHost, stm));
     TPCF_TRY(cudaEventCreateWithFlags(&io.done, cudaEventDisableTiming));
     TPCF_TRY(cudaEventRecord(io.done, stm));
     return 0;
+}
+
+// The status and message of a count whose device error record is set.
+int device_error(const int *e, Error *err) {
+    if (e[0] == kErrCheck) {
+        static const char *names[] = {"?", "bin index", "work item's job", "work item's segment range",
+                                      "A chunk length", "A chunk's points", "A cell", "A region",
+                                      "segment's B points", "B cell", "segment's region", "warp queue fill",
+                                      "side queue fill"};
+        const int id = e[1] >= 1 && e[1] <= DC_SIDE_QUEUE ? e[1] : 0;
+        err->status = 7;
+        err->msg = std::string("device bounds check failed: ") + names[id] + " " + std::to_string(e[2]) +
+                   " outside its range (limit " + std::to_string(e[3]) + "); results discarded";
+        return err->status;
+    }
+    err->status = 4;
+    err->msg = "device wait exceeded its iteration limit; results discarded";
+    return err->status;
 }
 
 // Wait for a launched count and convert its fixed-point sums (or hand back
@@ -1922,11 +2041,7 @@ int finish_count(Ctx *ctx, CountPlan &C, const CountBuffers &D, HostIO &io, doub
     const unsigned long long *hf = io.hf, *hs = io.hs, *hc = io.hc;
     const bool has_flags = C.n_flags() > 0;
     const unsigned *hflags = io.hflags;
-    if (*io.herr) {
-        err->status = 4;
-        err->msg = "device wait exceeded its iteration limit; results discarded";
-        return err->status;
-    }
+    if (*io.herr) return device_error(io.herr, err);
     if (C.adj) {
         TPCF_TRY(cudaMemcpy(C.grad_a_host, D.grad_a, sizeof(double) * C.n_a, cudaMemcpyDeviceToHost));
         if (!C.is_auto && C.grad_b_host)
@@ -2064,7 +2179,7 @@ int alloc_scratch(Ctx *ctx, const CountPlan &C, CountScratch &S, Error *err) {
     TPCF_TRY(S.sub.alloc(X, 2 * (size_t)C.nb * C.n_jk));
     TPCF_TRY(S.cnt.alloc(X, 4));
     TPCF_TRY(S.head.alloc(X, 1));
-    TPCF_TRY(S.err.alloc(X, 1));
+    TPCF_TRY(S.err.alloc(X, kErrWords));
     TPCF_TRY(S.t1.alloc(X, bin->t1.size()));
     TPCF_TRY(S.t2.alloc(X, std::max<size_t>(bin->t2.size(), 1)));
     TPCF_TRY(S.l1.alloc(X, LUT1_N));
@@ -2433,7 +2548,7 @@ int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *
     TPCF_TRY(B->sub.alloc(2 * nb * nj * B->n_out));
     TPCF_TRY(B->cnt.alloc(4));
     TPCF_TRY(B->head.alloc(1));
-    TPCF_TRY(B->err.alloc(1));
+    TPCF_TRY(B->err.alloc(kErrWords));
     TPCF_TRY(B->t1.alloc(bin->t1.size()));
     TPCF_TRY(B->t2.alloc(std::max<size_t>(bin->t2.size(), 1)));
     TPCF_TRY(B->l1.alloc(LUT1_N));
@@ -2441,7 +2556,7 @@ int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *
     TPCF_TRY(cudaMallocHost((void **)&B->h_full, sizeof(unsigned long long) * 2 * nb * B->n_out));
     TPCF_TRY(cudaMallocHost((void **)&B->h_sub, sizeof(unsigned long long) * 2 * nb * nj * B->n_out));
     TPCF_TRY(cudaMallocHost((void **)&B->h_cnt, sizeof(unsigned long long) * 4));
-    TPCF_TRY(cudaMallocHost((void **)&B->h_err, sizeof(int)));
+    TPCF_TRY(cudaMallocHost((void **)&B->h_err, sizeof(int) * kErrWords));
     if (!C.items.empty()) {
         TPCF_TRY(cudaMemcpyAsync(B->items.p, C.items.data(), sizeof(WorkItem) * C.items.size(),
                                  cudaMemcpyHostToDevice, stm));
@@ -2457,6 +2572,8 @@ int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *
     TPCF_TRY(cudaStreamSynchronize(stm));
 
     KParams P = C.P;
+    P.n_segs = (int)C.segs.size();
+    P.n_jobs = (int)C.jobs.size();
     P.jobs = B->jobs.p;
     P.items = B->items.p;
     P.segs = B->segs.p;
@@ -2480,13 +2597,13 @@ int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *
     cudaMemsetAsync(B->sub.p, 0, sizeof(unsigned long long) * 2 * nb * nj * B->n_out, stm);
     cudaMemsetAsync(B->cnt.p, 0, sizeof(unsigned long long) * 4, stm);
     cudaMemsetAsync(B->head.p, 0, sizeof(int), stm);
-    cudaMemsetAsync(B->err.p, 0, sizeof(int), stm);
+    cudaMemsetAsync(B->err.p, 0, sizeof(int) * kErrWords, stm);
     if (!C.items.empty()) C.fn<<<B->grid, NT, C.L.total, stm>>>(P);
     cudaMemcpyAsync(B->h_full, B->full.p, sizeof(unsigned long long) * 2 * nb * B->n_out, cudaMemcpyDeviceToHost, stm);
     cudaMemcpyAsync(B->h_sub, B->sub.p, sizeof(unsigned long long) * 2 * nb * nj * B->n_out, cudaMemcpyDeviceToHost,
                     stm);
     cudaMemcpyAsync(B->h_cnt, B->cnt.p, sizeof(unsigned long long) * 4, cudaMemcpyDeviceToHost, stm);
-    cudaMemcpyAsync(B->h_err, B->err.p, sizeof(int), cudaMemcpyDeviceToHost, stm);
+    cudaMemcpyAsync(B->h_err, B->err.p, sizeof(int) * kErrWords, cudaMemcpyDeviceToHost, stm);
     TPCF_TRY(cudaStreamEndCapture(stm, &B->graph));
     TPCF_TRY(cudaGraphInstantiate(&B->exec, B->graph, 0));
     out = std::move(B);
@@ -2511,11 +2628,7 @@ int batch_run(Batch *B, double *full_out, double *region_out, Stats *st, Error *
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (!C.items.empty()) ++ctx->launches;
-    if (*B->h_err) {
-        err->status = 4;
-        err->msg = "device wait exceeded its iteration limit; results discarded";
-        return err->status;
-    }
+    if (*B->h_err) return device_error(B->h_err, err);
     const size_t nb = C.nb, nj = C.n_jk;
     for (size_t k = 0; k < nb * B->n_out; ++k) full_out[k] = fixed_to_double(&B->h_full[2 * k], C.inv);
     if (region_out)
@@ -2673,7 +2786,7 @@ int run_count_static(Ctx *ctx, const CountRequest &req, double *full_out, double
     const size_t o_sub = sp.take(sizeof(unsigned long long) * 2 * (size_t)nb * n_jk);
     const size_t o_cnt = sp.take(sizeof(unsigned long long) * 4);
     const size_t o_head = sp.take(sizeof(int));
-    const size_t o_err = sp.take(sizeof(int));
+    const size_t o_err = sp.take(sizeof(int) * kErrWords);
     const size_t o_t1 = sp.take(sizeof(float) * bin->t1.size());
     const size_t o_t2 = sp.take(sizeof(float) * std::max<size_t>(bin->t2.size(), 1));
     const size_t o_l1 = sp.take(LUT1_N);
