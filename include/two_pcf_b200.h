@@ -84,14 +84,24 @@ int tpcf_set_refinement(tpcf_ctx *ctx, int cells_per_rmax);
  * always the maximum separation, src/boxes.cpp:56-59).  on != 0: the first
  * count of each class (mode, regions, weights, precision, bins, auto or
  * cross, and the catalogues' points per cell of side r_max to within a
- * factor of two) probes cells of 1, 2 and 3 per maximum separation and, for
- * the plain-weight FP32+guard kernels, both kernel configurations, each on a
- * strided sample of its work items, and keeps the one that counted the most
- * in-range pairs per second for every later count of the class in this
- * context.  Results do not depend on the choice.  A fixed refinement or
- * kernel configuration (here or per call) turns the tuning off; sharded
- * counts are never tuned. */
+ * factor of two) probes cells of 1, 2 and 3 per maximum separation, for the
+ * plain-weight FP32+guard kernels both kernel configurations, and for
+ * plain-weight cross counts both orders, each on a strided sample of its
+ * work items, and keeps the one that counted the most in-range pairs per
+ * second for every later count of the class in this context.  Counts do not
+ * depend on the choice, nor do weighted sums whose pair weights all lie
+ * within a factor 2^15 of the largest (the fixed-point resolution of smaller
+ * ones, 2^-(S+1) in the notes of tpcf_count, follows the chosen plan).  A
+ * fixed refinement, kernel configuration or order (here or per call) turns
+ * the tuning off; sharded counts are never tuned. */
 int tpcf_set_autotune(tpcf_ctx *ctx, int on);
+/* Order of plain-weight cross counts: 0 counts a's points against b's (a's
+ * points held in registers, b's streamed through shared memory), 1 the
+ * reverse, -1 automatic (the autotuner's choice when it runs, else 0).  Same
+ * results either way: each pair adds to the full histogram and to the rows of
+ * both its regions, the pair weight is a commutative float product, and
+ * swapping the points negates the separation exactly. */
+int tpcf_set_cross_order(tpcf_ctx *ctx, int order);
 /* Kernel configuration of the plain-weight FP32+guard kernels: 0 the default
  * per kind (jackknife kernels: three tile buffers of 256 points, ballots of
  * four A slots between queue checks; kernels without regions: two buffers,
@@ -100,8 +110,9 @@ int tpcf_set_autotune(tpcf_ctx *ctx, int on);
  * autotuner's choice when it runs, else 0).  Same results either way. */
 int tpcf_set_kernel_config(tpcf_ctx *ctx, int cfg);
 /* The autotuner's choices so far as JSON text: a list of {"class", "refinement",
- * "kernel_config", "pairs_per_s": [m = 1, 2, 3 with configuration 0, then with
- * configuration 1; 0 where not probed]}.  Writes at most len bytes including
+ * "kernel_config", "order", "pairs_per_s": [m = 1, 2, 3 with configuration 0,
+ * then with configuration 1, first in order 0, then in order 1; 0 where not
+ * probed]}.  Writes at most len bytes including
  * the terminating NUL; returns the length the full text needs (without the
  * NUL), or a negative status. */
 int64_t tpcf_autotune_describe(const tpcf_ctx *ctx, char *buf, int64_t len);

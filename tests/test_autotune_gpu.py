@@ -49,18 +49,22 @@ def test_every_choice_counts_the_same(cats, precision):
     for a, b, bn in cases(cats):
         c.set_refinement(0)
         c.set_kernel_config(-1)
+        c.set_cross_order(-1)
         full, reg, st = tp.count(c, a, b, bn, precision)
         assert st["in_range"] > 0
         for m in (1, 2, 3):
             for cfg in (0, 1):
-                c.set_refinement(m)
-                c.set_kernel_config(cfg)
-                f2, r2, st2 = tp.count(c, a, b, bn, precision)
-                assert np.array_equal(f2, full), (m, cfg)
-                assert np.array_equal(r2, reg), (m, cfg)
-                assert st2["in_range"] == st["in_range"]
+                for order in ((0, 1) if b is not None else (0,)):
+                    c.set_refinement(m)
+                    c.set_kernel_config(cfg)
+                    c.set_cross_order(order)
+                    f2, r2, st2 = tp.count(c, a, b, bn, precision)
+                    assert np.array_equal(f2, full), (m, cfg, order)
+                    assert np.array_equal(r2, reg), (m, cfg, order)
+                    assert st2["in_range"] == st["in_range"]
     c.set_refinement(0)
     c.set_kernel_config(-1)
+    c.set_cross_order(-1)
 
 
 def test_autotuned_counts_and_table(cats):
@@ -74,10 +78,12 @@ def test_autotuned_counts_and_table(cats):
         table = c.autotune_table()
         assert len(table) >= 3
         for e in table:
-            assert e["refinement"] in (1, 2, 3) and e["kernel_config"] in (0, 1)
+            assert e["refinement"] in (1, 2, 3) and e["kernel_config"] in (0, 1) and e["order"] in (0, 1)
             rates = e["pairs_per_s"]
-            assert len(rates) == 6 and all(r > 0 for r in rates)   # plain-weight FP32+guard: 3 x 2 probes
-            assert rates[(e["refinement"] - 1) + 3 * e["kernel_config"]] == max(rates)
+            cross = "auto 0" in e["class"]
+            # plain-weight FP32+guard: 3 refinements x 2 configurations, x 2 orders for a cross count
+            assert len(rates) == 12 and sum(r > 0 for r in rates) == (12 if cross else 6)
+            assert rates[(e["refinement"] - 1) + 3 * e["kernel_config"] + 6 * e["order"]] == max(rates)
         for (f, r, _), (f2, r2, _) in zip(ref, got):
             assert np.array_equal(f, f2) and np.array_equal(r, r2)
         # a second pass meets known classes: no new probes
@@ -89,7 +95,7 @@ def test_autotuned_counts_and_table(cats):
         f64, r64, _ = tp.count(c, jobs[0][0], jobs[0][1], jobs[0][2], tp.FP64)
         assert np.array_equal(f64, ref64[0]) and np.array_equal(r64, ref64[1])
         e64 = [e for e in c.autotune_table() if "fp64 1" in e["class"]]
-        assert len(e64) == 1 and e64[0]["kernel_config"] == 0 and e64[0]["pairs_per_s"][3:] == [0, 0, 0]
+        assert len(e64) == 1 and e64[0]["kernel_config"] == 0 and e64[0]["pairs_per_s"][3:6] == [0, 0, 0]
     finally:
         c.set_autotune(False)
 

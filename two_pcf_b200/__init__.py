@@ -84,6 +84,11 @@ class Context:
         -1 automatic)."""
         _check(_capi.lib().tpcf_set_kernel_config(self._h, int(cfg)), self)
 
+    def set_cross_order(self, order: int):
+        """Order of plain-weight cross counts (tpcf_set_cross_order): 0 a's
+        points against b's, 1 the reverse, -1 automatic."""
+        _check(_capi.lib().tpcf_set_cross_order(self._h, int(order)), self)
+
     def autotune_table(self) -> list:
         """The autotuner's choices so far (tpcf_autotune_describe)."""
         import json

@@ -134,6 +134,7 @@ _PROTOTYPES = {
     "tpcf_device_checks": (C.c_int, []),
     "tpcf_debug_corrupt_work_list": (C.c_int, [C.c_int]),
     "tpcf_set_kernel_config": (C.c_int, [C.c_void_p, C.c_int]),
+    "tpcf_set_cross_order": (C.c_int, [C.c_void_p, C.c_int]),
     "tpcf_autotune_describe": (C.c_int64, [C.c_void_p, C.c_char_p, C.c_int64]),
     "tpcf_run_param_file_report": (C.c_int, [C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_char_p]),
     "tpcf_run_invp": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, C.c_int, _vp, C.c_int]),

@@ -153,6 +153,12 @@ int tpcf_set_autotune(tpcf_ctx *ctx, int on) {
     return TPCF_OK;
 }
 
+int tpcf_set_cross_order(tpcf_ctx *ctx, int order) {
+    if (!ctx || order < -1 || order > 1) return TPCF_E_INVALID_ARG;
+    ctx->c.swap = order;
+    return TPCF_OK;
+}
+
 int tpcf_set_kernel_config(tpcf_ctx *ctx, int cfg) {
     if (!ctx || cfg < -1 || cfg > 1) return TPCF_E_INVALID_ARG;
     ctx->c.kernel_cfg = cfg;
@@ -167,7 +173,8 @@ int64_t tpcf_autotune_describe(const tpcf_ctx *ctx, char *buf, int64_t len) {
         j += first ? "" : ", ";
         first = false;
         j += "{\"class\": \"" + kv.first + "\", \"refinement\": " + std::to_string(kv.second.m) +
-             ", \"kernel_config\": " + std::to_string(kv.second.cfg) + ", \"pairs_per_s\": [";
+             ", \"kernel_config\": " + std::to_string(kv.second.cfg) +
+             ", \"order\": " + std::to_string(kv.second.swap) + ", \"pairs_per_s\": [";
         for (size_t k = 0; k < kv.second.rate.size(); ++k) {
             char b[32];
             std::snprintf(b, sizeof b, "%s%.6g", k ? ", " : "", kv.second.rate[k]);

@@ -99,12 +99,14 @@ struct Ctx {
     std::string last_error;
     int refinement = 0;  // 0 = automatic
     int kernel_cfg = -1;  // -1 = automatic (the autotuner's choice when it runs, else 0)
+    int swap = -1;        // order of plain-weight cross counts (CountRequest::swap); -1 = automatic
     // autotuning of counts: the (refinement, kernel configuration) chosen per
     // count class by timed probes, kept for the context's lifetime
     bool autotune = false;
     struct Tuned {
-        int m = 0, cfg = 0;
-        std::vector<double> rate;  // in-range pairs/s of each candidate probed (m 1-3 x cfg 0-1; 0 = not probed)
+        int m = 0, cfg = 0, swap = 0;
+        // in-range pairs/s of each candidate probed, index (m - 1) + 3 cfg + 6 swap; 0 = not probed
+        std::vector<double> rate;
     };
     std::map<std::string, Tuned> tuned;
     unsigned long long launches = 0;  // kernels launched by this context
@@ -357,6 +359,13 @@ struct CountRequest {
     // kernel configuration of the plain-weight FP32+guard kernels (0 or 1;
     // -1: the context's setting, else the autotuner's choice, else 0)
     int kernel_cfg = -1;
+    // order of a plain-weight cross count: 1 counts b's points against a's
+    // (b in registers, a streamed in tiles), 0 a's against b's; -1 the
+    // context's setting, else the autotuner's choice, else 0.  The histograms
+    // are the same either way: each pair adds once to the full histogram and
+    // to the rows of both its regions, the pair weight is a commutative float
+    // product, and swapping the points negates the separation exactly.
+    int swap = -1;
     // adjoint of a plain-weight 3-D count: with adj_G = dL/d(raw full
     // histogram) set, the count writes per-point dL/dw into grad_a (n_all of
     // a) and grad_b (n_all of b; unused for auto counts) instead of histograms

@@ -2257,10 +2257,26 @@ std::string tune_key(const CountPlan &C, const CountRequest &req) {
     return b;
 }
 
-int tune_probe(Ctx *ctx, const CountRequest &req, int m, int cfg, double *rate, Error *err) {
+// A cross count whose two catalogues may play either role: plain weights,
+// not an adjoint.
+bool swappable(const CountRequest &req) {
+    return req.b != nullptr && req.b != req.a && req.weighting == WEIGHTS_PLAIN && !req.adj_G;
+}
+
+// The request with its catalogues in the order it asks for (swap = 1: b's
+// points in registers, a's streamed in tiles).
+void apply_order(const Ctx *ctx, CountRequest &req) {
+    const int s = req.swap >= 0 ? req.swap : std::max(ctx->swap, 0);
+    req.swap = s;
+    if (s == 1 && swappable(req)) std::swap(req.a, req.b);
+}
+
+int tune_probe(Ctx *ctx, const CountRequest &req, int m, int cfg, int swap, double *rate, Error *err) {
     CountRequest r = req;
     r.refinement = m;
     r.kernel_cfg = cfg;
+    r.swap = swap;
+    apply_order(ctx, r);
     CountPlan C;
     if (plan_count(ctx, r, true, C, err)) return err->status;
     const size_t want = std::max<size_t>((size_t)32 * ctx->num_sms, C.items.size() / 16);
@@ -2286,7 +2302,7 @@ int tune_probe(Ctx *ctx, const CountRequest &req, int m, int cfg, double *rate, 
 // autotuning is off or the caller fixed either choice.
 int autotune(Ctx *ctx, CountRequest &req, Error *err) {
     if (!ctx->autotune || req.adj_G || req.n_shards > 1 || req.refinement > 0 || ctx->refinement > 0 ||
-        req.kernel_cfg >= 0 || ctx->kernel_cfg >= 0)
+        req.kernel_cfg >= 0 || ctx->kernel_cfg >= 0 || req.swap >= 0 || ctx->swap >= 0)
         return 0;
     CountPlan C0;
     if (plan_count(ctx, req, true, C0, err, true)) return err->status;
@@ -2294,28 +2310,31 @@ int autotune(Ctx *ctx, CountRequest &req, Error *err) {
     auto it = ctx->tuned.find(key);
     if (it == ctx->tuned.end()) {
         Ctx::Tuned t;
-        t.rate.assign(6, 0.0);
+        t.rate.assign(12, 0.0);
         double best = -1.0;
-        for (int cfg = 0; cfg < (C0.cfg_tunable ? 2 : 1); ++cfg)
-            for (int m = 1; m <= 3; ++m) {
-                double r = 0.0;
-                if (tune_probe(ctx, req, m, cfg, &r, err)) return err->status;
-                t.rate[(size_t)(m - 1) + 3 * (size_t)cfg] = r;
-                if (r > best) {
-                    best = r;
-                    t.m = m;
-                    t.cfg = cfg;
+        for (int swap = 0; swap < (swappable(req) ? 2 : 1); ++swap)
+            for (int cfg = 0; cfg < (C0.cfg_tunable ? 2 : 1); ++cfg)
+                for (int m = 1; m <= 3; ++m) {
+                    double r = 0.0;
+                    if (tune_probe(ctx, req, m, cfg, swap, &r, err)) return err->status;
+                    t.rate[(size_t)(m - 1) + 3 * (size_t)cfg + 6 * (size_t)swap] = r;
+                    if (r > best) {
+                        best = r;
+                        t.m = m;
+                        t.cfg = cfg;
+                        t.swap = swap;
+                    }
                 }
-            }
         if (trace_enabled()) {
             std::fprintf(stderr, "[tpcf trace] autotune %s: pairs/s", key.c_str());
             for (double r : t.rate) std::fprintf(stderr, " %.3g", r);
-            std::fprintf(stderr, " -> refinement %d, configuration %d\n", t.m, t.cfg);
+            std::fprintf(stderr, " -> refinement %d, configuration %d, order %d\n", t.m, t.cfg, t.swap);
         }
         it = ctx->tuned.emplace(key, t).first;
     }
     req.refinement = it->second.m;
     req.kernel_cfg = it->second.cfg;
+    req.swap = it->second.swap;
     return 0;
 }
 
@@ -2324,6 +2343,7 @@ int autotune(Ctx *ctx, CountRequest &req, Error *err) {
 int run_count(Ctx *ctx, const CountRequest &req_in, double *full_out, double *region_out, Stats *st, Error *err) {
     CountRequest req = req_in;
     if (autotune(ctx, req, err)) return err->status;
+    apply_order(ctx, req);
     CountPlan C;
     if (plan_count(ctx, req, true, C, err)) return err->status;
     if (req.scale_exp_out) *req.scale_exp_out = C.scale_exp;
@@ -2335,8 +2355,10 @@ int run_count(Ctx *ctx, const CountRequest &req_in, double *full_out, double *re
 int run_count_many(Ctx *ctx, const std::vector<CountRequest> &reqs_in, const std::vector<CountOut> &outs,
                    Error *err) {
     std::vector<CountRequest> reqs(reqs_in);
-    for (CountRequest &r : reqs)
+    for (CountRequest &r : reqs) {
         if (autotune(ctx, r, err)) return err->status;
+        apply_order(ctx, r);
+    }
     // TPCF_TRACE=1: one stderr line per count with its host planning time
     // and where its kernel ran on the device, in ms from the call's start
     // (diagnostics of the pipelining; the counts are unchanged)
