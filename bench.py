@@ -383,6 +383,29 @@ def make_workload(seed: int, scale: float):
     return w
 
 
+def reference_grid_candidates(xa, xb, rmax, auto, lo, hi):
+    """Candidate pairs the reference's own cell scheme enumerates for one
+    count: cells of side rmax on the joint bounding box of the driver's two
+    catalogues (cell index (int)((x - min) / rmax), src/boxes.cpp:29-80), every
+    cell against its 27 neighbours (src/correlators.cpp:11-125; an auto count
+    pairs a cell with itself once, k < l, and with each other neighbour once).
+    The FP32 flop model counted on this fixed set of pairs does not depend on
+    this engine's refinement or order."""
+    from scipy.ndimage import convolve
+    dims = (np.floor((hi - lo) / rmax).astype(int) + 1)
+
+    def hist(x):
+        c = np.minimum(((x - lo) / rmax).astype(np.int64), dims - 1)
+        return np.bincount((c[:, 0] * dims[1] + c[:, 1]) * dims[2] + c[:, 2],
+                           minlength=int(np.prod(dims))).reshape(dims).astype(np.float64)
+    na = hist(xa)
+    nb = na if auto else hist(xb)
+    nbr = convolve(nb, np.ones((3, 3, 3)), mode="constant", cval=0.0)
+    if auto:
+        return int(round((float((na * nbr).sum()) - float(na.sum())) / 2))
+    return int(round(float((na * nbr).sum())))
+
+
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
@@ -730,6 +753,17 @@ def main():
             cpu = {"value": None, "error": str(ex)}
 
     achieved = tot_flops / (tot_kms * 1e-3) / 1e12 if tot_kms > 0 else 0.0
+    # the same flop model on the reference's own candidate set (cells of side
+    # r_max, 27 neighbours): a fixed amount of work per step
+    lo = np.minimum(d["xyz"].min(0), r["xyz"].min(0))
+    hi = np.maximum(d["xyz"].max(0), r["xyz"].max(0))
+    ref_cand, ref_flops = 0, 0.0
+    in_per_step = tot_in / args.steps
+    for mode, rmax in ((1, float(np.hypot(SIGMA_PI_AXES[0][1], SIGMA_PI_AXES[1][1]))), (2, S_MU_AXES[0][1])):
+        for xa, xb, auto in ((d["xyz"], None, True), (d["xyz"], r["xyz"], False), (r["xyz"], None, True)):
+            ref_cand += reference_grid_candidates(xa, xb, rmax, auto, lo, hi)
+    ref_flops = 8.0 * ref_cand + (tot_flops - 8.0 * tot_cand) / args.steps  # in-range part as measured
+    ref_achieved = ref_flops / (tot_kms / args.steps * 1e-3) / 1e12 if tot_kms > 0 else 0.0
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "strong" if sharded else "weak",
@@ -758,7 +792,14 @@ def main():
                                     "MEASURED_PEAKS.json has no FP32 figure",
                      "flops_model": "8 per candidate pair + 16 (sigma-pi) / 13 (s-mu) per in-range pair",
                      "kernel_ms_per_step": tot_kms / args.steps,
-                     "smem_atomic_peak_per_s": atom_rate},
+                     "smem_atomic_peak_per_s": atom_rate,
+                     "reference_grid": {
+                         "candidates_per_step": ref_cand, "achieved": ref_achieved,
+                         "frac": ref_achieved / fp32_tflops if fp32_tflops else None,
+                         "note": "the same flop model with the candidates the reference's own cell scheme "
+                                 "enumerates (cells of side r_max, 27 neighbours): a fixed workload; `achieved` "
+                                 "above counts the candidates this engine enumerated, fewer when its refinement "
+                                 "is finer"}},
         "fp64_path": fp64, "e2e": e2e, "cpu_baseline": cpu, "gpu_launches": int(launches), "clocks": clocks,
         "autotune": ctx.autotune_table() if not args.no_autotune else None,
     }

@@ -55,3 +55,23 @@ def test_gpus_2_launches_two_ranks_and_reduces_exactly():
     assert r.returncode == 0, r.stderr[-2000:]
     line = json.loads([ln for ln in r.stdout.splitlines() if ln.startswith("{")][-1])
     assert line == {"exchange_selftest": True, "n_ranks": 2, "backend": "gloo"}
+
+
+def test_reference_grid_candidates_brute_force():
+    """The reference's candidate set (cells of side r_max on the joint bounding
+    box, 27 neighbours; auto counts each unordered pair once) counted by the
+    bench's histogram convolution equals a pair-by-pair enumeration."""
+    rng = np.random.default_rng(1)
+    a = rng.uniform(0, 30, (300, 3))
+    b = rng.uniform(0, 30, (500, 3))
+    lo, hi = np.minimum(a.min(0), b.min(0)), np.maximum(a.max(0), b.max(0))
+    r = 7.0
+    top = np.floor((hi - lo) / r).astype(int)
+
+    def cells(x):
+        return np.minimum(((x - lo) / r).astype(int), top)
+    ca, cb = cells(a), cells(b)
+    near_ab = np.all(np.abs(ca[:, None, :] - cb[None, :, :]) <= 1, axis=2)
+    near_aa = np.all(np.abs(ca[:, None, :] - ca[None, :, :]) <= 1, axis=2)
+    assert bench.reference_grid_candidates(a, b, r, False, lo, hi) == int(near_ab.sum())
+    assert bench.reference_grid_candidates(a, None, r, True, lo, hi) == int(np.triu(near_aa, 1).sum())
