@@ -166,6 +166,7 @@ def other_workload(args):
                      "value": pairs / ((ms_b + ms_r) * 1e-3), "ms": ms_b + ms_r, "batch_ms": ms_b, "rr_ms": ms_r,
                      "batch_pairs": st_b["in_range"], "rr_pairs": st_r["in_range"], "mock_points": int(sizes.sum()),
                      "random_points": int(10_000_000 * scale), "refinement": batch.refinement,
+                     "dr_order": batch.order,
                      "batch_work_items": st_b["work_items"]})
     elif args.workload == "invp":
         w = synthetic.survey_catalogue(seed=4, n_data=int(500_000 * scale), n_rand=int(2_000_000 * scale))

@@ -275,8 +275,12 @@ int tpcf_iip_weights(int64_t n, int32_t n_mask_ints, const int64_t *bitmask, con
  *   what: TPCF_BATCH_DD | TPCF_BATCH_DR; outputs are ordered mock by mock,
  *         DD then DR, each as tpcf_count returns it (raw, not doubled).
  *   refinement: cells per maximum separation 1..3, 0 automatic, or
- *         TPCF_BATCH_AUTOTUNE: each of 1, 2, 3 is planned and timed once and
- *         the fastest is kept (tpcf_batch_refinement reports it).
+ *         TPCF_BATCH_AUTOTUNE: each of 1, 2, 3, and for DR jobs each order
+ *         (the mock's points against the randoms', or the reverse), is
+ *         planned on a strided sample of its work items and timed once; the
+ *         one that counted the most in-range pairs per second is built in
+ *         full (tpcf_batch_refinement and tpcf_batch_order report it).  The
+ *         histograms do not depend on the choice.
  * The catalogues must outlive the batch, keep their weights, and keep their
  * cached grids (no tpcf_catalog_release_cache) while it exists. */
 typedef struct tpcf_batch tpcf_batch;
@@ -289,6 +293,8 @@ int tpcf_batch_create(tpcf_ctx *ctx, const tpcf_catalog *const *mocks, int32_t n
 int tpcf_batch_run(tpcf_batch *batch, double *full_out, double *region_out, tpcf_stats *stats);
 int tpcf_batch_n_outputs(const tpcf_batch *batch);
 int tpcf_batch_refinement(const tpcf_batch *batch);
+/* 1 when the batch counts its DR jobs the randoms' points against each mock's. */
+int tpcf_batch_order(const tpcf_batch *batch);
 int tpcf_batch_destroy(tpcf_batch *batch);
 
 /* Host-side evaluation of the up-weight of a 3-D inverse-p spec at values of

@@ -118,3 +118,22 @@ def test_batch_matches_oracle(ctx, weighted):
                 assert np.array_equal(full[2 * i + k], want_full)
                 assert np.array_equal(reg[2 * i + k], want_reg)
             assert want_full.sum() > 0
+
+
+def test_batch_autotune_with_dr_orders(ctx):
+    """The batch autotuner probes refinements 1-3 and both orders of the DR
+    jobs on sampled work items and builds the fastest in full; whatever it
+    picks, every output equals one tp.count."""
+    ms = mocks(9, [2600, 4800], True)
+    rng = np.random.default_rng(10)
+    R = catalog(ctx, rng.uniform(0, BOX, (12000, 3)), None)
+    M = [catalog(ctx, x, w) for x, w in ms]
+    b = tp.Binning(ctx, tp.S_MU, AX1, AX2, 27)
+    batch = tp.Batch(ctx, M, R, b, what=tp.BATCH_DD | tp.BATCH_DR, refinement=tp.BATCH_AUTOTUNE)
+    assert batch.refinement in (1, 2, 3) and batch.order in (0, 1)
+    full, reg, _ = batch.run()
+    for i, m in enumerate(M):
+        for k, other in ((0, None), (1, R)):
+            f1, r1, _ = tp.count(ctx, m, other, b)
+            np.testing.assert_allclose(full[2 * i + k], f1, rtol=1e-12, atol=1e-9)
+            np.testing.assert_allclose(reg[2 * i + k], r1, rtol=1e-12, atol=1e-9)

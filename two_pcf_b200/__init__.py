@@ -447,8 +447,9 @@ def count_backward(ctx: Context, a: Catalog, b: Catalog | None, binning: Binning
 class Batch:
     """DD and/or DR counts of many mock catalogues (DR against one shared random
     catalogue) in one persistent launch, planned once and replayed as a CUDA
-    graph by run().  refinement: 1..3, 0 automatic, BATCH_AUTOTUNE to time
-    1, 2 and 3 and keep the fastest."""
+    graph by run().  refinement: 1..3, 0 automatic, BATCH_AUTOTUNE to probe
+    refinements 1, 2, 3 and both orders of the DR jobs and keep the fastest
+    (.refinement, .order)."""
 
     def __init__(self, ctx: Context, mocks, randoms: Catalog | None, binning: Binning, precision: int = FP32_GUARD,
                  what: int = BATCH_DD | BATCH_DR, refinement: int = 0):
@@ -461,6 +462,7 @@ class Batch:
         self._keep = (list(mocks), randoms)
         self.n_outputs = int(_capi.lib().tpcf_batch_n_outputs(h))
         self.refinement = int(_capi.lib().tpcf_batch_refinement(h))
+        self.order = int(_capi.lib().tpcf_batch_order(h))
 
     def run(self, with_regions: bool = True):
         """(full[n_outputs, nb], regions[n_outputs, n_jk, nb] or None, stats)."""

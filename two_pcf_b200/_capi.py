@@ -98,6 +98,7 @@ _PROTOTYPES = {
     "tpcf_batch_run": (C.c_int, [_vp, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_batch_n_outputs": (C.c_int, [_vp]),
     "tpcf_batch_refinement": (C.c_int, [_vp]),
+    "tpcf_batch_order": (C.c_int, [C.c_void_p]),
     "tpcf_batch_destroy": (C.c_int, [_vp]),
     "tpcf_auto_pair_count": (C.c_int, [_vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),
     "tpcf_cross_pair_count": (C.c_int, [_vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.POINTER(Stats)]),

@@ -873,6 +873,7 @@ int tpcf_batch_run(tpcf_batch *batch, double *full_out, double *region_out, tpcf
 }
 
 int tpcf_batch_n_outputs(const tpcf_batch *batch) { return batch ? tpcf::batch_jobs(batch->b) : -TPCF_E_INVALID_ARG; }
+int tpcf_batch_order(const tpcf_batch *batch) { return batch ? tpcf::batch_order(batch->b) : -TPCF_E_INVALID_ARG; }
 int tpcf_batch_refinement(const tpcf_batch *batch) {
     return batch ? tpcf::batch_refinement(batch->b) : -TPCF_E_INVALID_ARG;
 }

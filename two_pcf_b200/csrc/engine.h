@@ -409,6 +409,7 @@ int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning 
 // sums as tpcf_count returns them, job after job.
 int batch_run(Batch *b, double *full_out, double *region_out, Stats *st, Error *err);
 int batch_refinement(const Batch *b);
+int batch_order(const Batch *b);
 int batch_jobs(const Batch *b);
 void batch_destroy(Batch *b);
 

@@ -2527,6 +2527,7 @@ struct Batch {
     Ctx *ctx = nullptr;
     CountPlan C;
     int m = 0, grid = 0;
+    int order = 0;  // 1: the DR jobs count the shared catalogue's points against each mock's
     size_t n_out = 0;
     DevBuf<WorkItem> items;
     DevBuf<Segment> segs;
@@ -2553,13 +2554,25 @@ namespace {
 
 // Plan, allocate and upload a batch for one refinement, then capture its
 // run (clears, the launch, the read-backs) as a CUDA graph.
+// sample: keep every k-th work item only (at least 32 per SM), for the
+// autotuner's timed probes.
 int batch_build(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *bin, bool exact, int m,
-                std::unique_ptr<Batch> &out, Error *err) {
+                std::unique_ptr<Batch> &out, Error *err, bool sample = false) {
     std::unique_ptr<Batch> B(new Batch());
     B->ctx = ctx;
     B->m = m;
     CountPlan &C = B->C;
     if (plan_batch(ctx, jobs, bin, exact, m, C, err)) return err->status;
+    if (sample) {
+        const size_t want = std::max<size_t>((size_t)32 * ctx->num_sms, C.items.size() / 16);
+        if (C.items.size() > want) {
+            const size_t stride = C.items.size() / want;
+            std::vector<WorkItem> kept;
+            for (size_t k = 0; k < C.items.size(); k += stride) kept.push_back(C.items[k]);
+            C.items.swap(kept);
+            C.P.n_items = (int)C.items.size();
+        }
+    }
     B->n_out = C.jobs.size();
     const size_t nb = C.nb, nj = C.n_jk;
     cudaStream_t stm = ctx->stream;
@@ -2674,10 +2687,51 @@ int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning 
         err->msg = "empty batch";
         return err->status;
     }
+    if (refinement < 0) {
+        // autotune: every (refinement 1-3, order) candidate planned on a
+        // strided sample of its work items and timed once; the one that
+        // counted the most in-range pairs per second is built in full.  Order
+        // 1 swaps the catalogues of the DR jobs (the shared catalogue's points
+        // in registers, the mock's streamed); the histograms are the same.
+        bool any_cross = false;
+        for (const BatchJobSpec &j : jobs) any_cross = any_cross || (j.b && j.b != j.a);
+        std::vector<BatchJobSpec> swapped(jobs);
+        for (BatchJobSpec &j : swapped)
+            if (j.b && j.b != j.a) std::swap(j.a, j.b);
+        int best_m = 0, best_order = 0;
+        double best_rate = -1.0;
+        for (int order = 0; order < (any_cross ? 2 : 1); ++order)
+            for (int m = 1; m <= 3; ++m) {
+                std::unique_ptr<Batch> b;
+                if (batch_build(ctx, order ? swapped : jobs, bin, exact_fp64, m, b, err, true)) {
+                    if (err->status == 6) continue;  // e.g. a grid too fine for this refinement
+                    return err->status;
+                }
+                std::vector<double> f(b->C.nb * b->n_out);
+                Stats st;
+                if (batch_run(b.get(), f.data(), nullptr, &st, err)) return err->status;
+                const double rate = st.ms_kernel > 0 ? (double)st.in_range / st.ms_kernel : 0.0;
+                if (rate > best_rate) {
+                    best_rate = rate;
+                    best_m = m;
+                    best_order = order;
+                }
+            }
+        if (best_m == 0) {
+            err->status = 6;
+            err->msg = "no refinement could be planned";
+            return err->status;
+        }
+        std::unique_ptr<Batch> b;
+        if (batch_build(ctx, best_order ? swapped : jobs, bin, exact_fp64, best_m, b, err)) return err->status;
+        b->order = best_order;
+        *out = b.release();
+        return 0;
+    }
     std::vector<int> choices;
     if (refinement > 0) {
         choices.push_back(refinement);
-    } else if (refinement == 0) {
+    } else {
         // as run_count: from the largest catalogue's mean density
         const Catalog *big = jobs[0].a;
         for (const BatchJobSpec &j : jobs) {
@@ -2688,8 +2742,6 @@ int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning 
         double vol = 1;
         for (int k = 0; k < 3; ++k) vol *= std::max(big->hi_kept[k] - big->lo_kept[k], rb);
         choices.push_back(big->n_kept * (rb / 2) * (rb / 2) * (rb / 2) / vol >= 256 ? 2 : 1);
-    } else {
-        choices = {1, 2, 3};
     }
     std::unique_ptr<Batch> best;
     double best_ms = 0;
@@ -2722,6 +2774,7 @@ int batch_create(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning 
 }
 
 int batch_refinement(const Batch *b) { return b->m; }
+int batch_order(const Batch *b) { return b->order; }
 int batch_jobs(const Batch *b) { return (int)b->n_out; }
 void batch_destroy(Batch *b) { delete b; }
 
