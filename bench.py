@@ -123,6 +123,7 @@ def other_workload(args):
     import two_pcf_b200 as tp
     from two_pcf_b200 import synthetic
     ctx = tp.Context(0)
+    ctx.set_autotune(not args.no_autotune)   # the warm-up steps absorb the probes
     scale = args.scale
     rng = np.random.default_rng(11)
 

@@ -85,8 +85,9 @@ int tpcf_set_refinement(tpcf_ctx *ctx, int cells_per_rmax);
  * count of each class (mode, regions, weights, precision, bins, auto or
  * cross, and the catalogues' points per cell of side r_max to within a
  * factor of two) probes cells of 1, 2 and 3 per maximum separation, for the
- * plain-weight FP32+guard kernels both kernel configurations, and for
- * plain-weight cross counts both orders, each on a strided sample of its
+ * plain-weight FP32+guard kernels both kernel configurations, and for cross
+ * counts with plain or inverse-p DR weights both orders (the adjoint tunes
+ * its refinement only), each on a strided sample of its
  * work items, and keeps the one that counted the most in-range pairs per
  * second for every later count of the class in this context.  Counts do not
  * depend on the choice, nor do weighted sums whose pair weights all lie
@@ -95,7 +96,7 @@ int tpcf_set_refinement(tpcf_ctx *ctx, int cells_per_rmax);
  * fixed refinement, kernel configuration or order (here or per call) turns
  * the tuning off; sharded counts are never tuned. */
 int tpcf_set_autotune(tpcf_ctx *ctx, int on);
-/* Order of plain-weight cross counts: 0 counts a's points against b's (a's
+/* Order of cross counts with plain or inverse-p DR weights: 0 counts a's points against b's (a's
  * points held in registers, b's streamed through shared memory), 1 the
  * reverse, -1 automatic (the autotuner's choice when it runs, else 0).  Same
  * results either way: each pair adds to the full histogram and to the rows of

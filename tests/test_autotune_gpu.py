@@ -24,6 +24,8 @@ def cats():
     d, r = w["data"], w["rand"]
     D = tp.Catalog(c, d["xyz"], d["x_norm"], d["d_comov"], d["weight"], None, d["jk"], w["n_jk"])
     R = tp.Catalog(c, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
+    _SRC[id(D)] = (d["xyz"], d["x_norm"], d["d_comov"], d["weight"])
+    _SRC[id(R)] = (r["xyz"], r["x_norm"], r["d_comov"], r["weight"])
     bx = synthetic.box_catalogue(seed=3, n_data=30_000, n_rand=60_000, box=300.0, n_centres=600)
     BD, BR = tp.Catalog(c, bx["data"]["xyz"]), tp.Catalog(c, bx["rand"]["xyz"])
     yield {"ctx": c, "D": D, "R": R, "n_jk": w["n_jk"], "BD": BD, "BR": BR}
@@ -112,3 +114,62 @@ def test_fixed_choice_turns_tuning_off(cats):
     finally:
         c.set_autotune(False)
         c.set_refinement(0)
+
+
+def test_autotuned_adjoint(cats):
+    """The adjoint tunes its refinement only (its gradients are per catalogue,
+    so the order stays): gradients equal the untuned ones to the adjoint's
+    fixed-point resolution."""
+    c = cats["ctx"]
+    D, R = cats["D"], cats["R"]
+    b = tp.Binning(c, *SMU, 1)
+    D1 = tp.Catalog(c, *[np.asarray(x) for x in _xyz_of(D)])
+    R1 = tp.Catalog(c, *[np.asarray(x) for x in _xyz_of(R)])
+    G = np.random.default_rng(3).standard_normal(b.nb)
+    ga, gb, _ = tp.count_backward(c, D1, R1, b, G)
+    c.set_autotune(True)
+    try:
+        ga2, gb2, _ = tp.count_backward(c, D1, R1, b, G)
+        e = [x for x in c.autotune_table() if "weight kind 6" in x["class"]]
+        assert len(e) == 1 and e[0]["order"] == 0 and sum(r > 0 for r in e[0]["pairs_per_s"]) == 3
+    finally:
+        c.set_autotune(False)
+    scale = np.abs(ga).max()
+    np.testing.assert_allclose(ga2, ga, rtol=1e-11, atol=1e-12 * scale)
+    np.testing.assert_allclose(gb2, gb, rtol=1e-11, atol=1e-12 * np.abs(gb).max())
+    D1.close()
+    R1.close()
+
+
+@pytest.mark.parametrize("precision", [tp.FP32_GUARD, tp.FP64], ids=["fp32_guard", "fp64"])
+def test_invp_dr_counts_the_same_in_either_order(cats, precision):
+    """Inverse-p DR weights are symmetric in the two points (the product of
+    the two weights, and for 3-D counts times the angular up-weight of
+    1 - cos(theta)): both orders give the same histograms."""
+    c = cats["ctx"]
+    D, R, n_jk = cats["D"], cats["R"], cats["n_jk"]
+    nt = 20
+    theta_axis = (0.0, 1.0 - np.cos(0.05), 1.6, nt)
+    rng = np.random.default_rng(8)
+    num = rng.uniform(1.0, 2.0, (1 + n_jk) * nt)
+    den = rng.uniform(0.5, 1.0, (1 + n_jk) * nt)
+    cases_ = [(tp.Binning(c, tp.ANGULAR, theta_axis, None, n_jk), tp.Weights(tp.WEIGHTS_INVP_DR)),
+              (tp.Binning(c, *SMU, n_jk), tp.Weights(tp.WEIGHTS_INVP_DR, 64, theta_axis, num, den))]
+    try:
+        for b, wts in cases_:
+            out = []
+            for order in (0, 1):
+                c.set_cross_order(order)
+                f, r, st = tp.count_weighted(c, D, R, b, wts, precision)
+                assert st["in_range"] > 0
+                out.append((f, r))
+            assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    finally:
+        c.set_cross_order(-1)
+
+
+_SRC = {}
+
+
+def _xyz_of(cat):
+    return _SRC[id(cat)]

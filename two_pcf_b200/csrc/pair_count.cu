@@ -2257,10 +2257,13 @@ std::string tune_key(const CountPlan &C, const CountRequest &req) {
     return b;
 }
 
-// A cross count whose two catalogues may play either role: plain weights,
-// not an adjoint.
+// A cross count whose two catalogues may play either role: plain weights or
+// inverse-p DR weights (the weight product and the angular up-weight of
+// 1 - cos(theta) are symmetric in the two points, and DR reads no masks);
+// not an adjoint, whose gradients are per catalogue.
 bool swappable(const CountRequest &req) {
-    return req.b != nullptr && req.b != req.a && req.weighting == WEIGHTS_PLAIN && !req.adj_G;
+    return req.b != nullptr && req.b != req.a && !req.adj_G &&
+           (req.weighting == WEIGHTS_PLAIN || req.weighting == WEIGHTS_INVP_DR);
 }
 
 // The request with its catalogues in the order it asks for (swap = 1: b's
@@ -2301,7 +2304,7 @@ int tune_probe(Ctx *ctx, const CountRequest &req, int m, int cfg, int swap, doub
 // count's class the first time it is met).  Leaves `req` as it is when
 // autotuning is off or the caller fixed either choice.
 int autotune(Ctx *ctx, CountRequest &req, Error *err) {
-    if (!ctx->autotune || req.adj_G || req.n_shards > 1 || req.refinement > 0 || ctx->refinement > 0 ||
+    if (!ctx->autotune || req.n_shards > 1 || req.refinement > 0 || ctx->refinement > 0 ||
         req.kernel_cfg >= 0 || ctx->kernel_cfg >= 0 || req.swap >= 0 || ctx->swap >= 0)
         return 0;
     CountPlan C0;
