@@ -420,6 +420,15 @@ int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit);
  * failing call returns an error status and releases what it had allocated. */
 int tpcf_debug_fail_allocations(int64_t after);
 
+/* Give-up path of the count kernels themselves (no counterpart in the
+ * reference; process-wide, for tests): counts planned after this call wait at
+ * most `limit` iterations for each staged tile of catalogue B (limit 0: the
+ * wait gives up at once) before the kernel flags a device timeout, stops
+ * taking work items and the call returns TPCF_E_DEVICE_TIMEOUT with its
+ * results discarded.  The wait before a CTA exits keeps the built-in limit,
+ * so no copy is left in flight.  limit < 0 restores the built-in limit. */
+int tpcf_debug_tile_wait_limit(int64_t limit);
+
 /* Device bounds checks (no counterpart in the reference).  The checked build
  * of this library (TPCF_DEVICE_CHECKS=1 python two_pcf_b200/build.py, written
  * to two_pcf_b200/lib/checked/) tests, in every count kernel, every index a

@@ -980,6 +980,11 @@ int tpcf_debug_fail_allocations(int64_t after) {
     return TPCF_OK;
 }
 
+int tpcf_debug_tile_wait_limit(int64_t limit) {
+    tpcf::debug_tile_wait_limit().store(limit < 0 ? -1 : (long long)limit);
+    return TPCF_OK;
+}
+
 int tpcf_debug_corrupt_work_list(int what) {
 #ifdef TPCF_DEVICE_CHECKS
     if (what != 0 && what != 1) return TPCF_E_INVALID_ARG;

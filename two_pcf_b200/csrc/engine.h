@@ -54,6 +54,14 @@ inline std::atomic<int> &debug_corrupt_work_list() {
     return v;
 }
 
+// Tile-wait limit of the count kernels (tpcf_debug_tile_wait_limit): the
+// iterations each wait for a staged tile may take before the kernel gives up
+// and reports a device timeout; -1 = the built-in limit.
+inline std::atomic<long long> &debug_tile_wait_limit() {
+    static std::atomic<long long> v{-1};
+    return v;
+}
+
 inline bool alloc_injected_failure() {
     auto &b = alloc_fail_budget();
     long long v = b.load(std::memory_order_relaxed);

@@ -169,6 +169,8 @@ struct KParams {
     const unsigned char *lut1g, *lut2g;
     unsigned lut1_base;  // (bits of the lowest bucket) >> (23 - LUT1_BITS)
     float lut2_scale;    // bucket = (int)(value * lut2_scale)
+    int direct2;         // axis 2 binned directly (linear, from 0): bin = floor(value * inv2)
+    float inv2, k2;      // the axis's float 1 / step and the constant part of its guard (in bins)
     unsigned long long *g_full, *g_sub;  // 128-bit fixed-point sums (low, high word pairs)
     int n_jk;
     float wscale;
@@ -194,6 +196,7 @@ struct KParams {
     const double *adj_G;
     double *grad_a, *grad_b;
     double adj_scale, adj_inv;  // gradient terms are summed as round(term * adj_scale) in 64-bit fixed point
+    uint32_t wait_limit;        // iterations of each wait for a staged tile before the kernel gives up
 };
 
 // Shared-memory views the binning steps use.
@@ -452,6 +455,21 @@ __device__ __forceinline__ unsigned lut_decode(unsigned c, float x, const float 
     return c;
 }
 
+// Direct binning of a linear axis starting at 0 from y = value * (1 / step),
+// the reference's own float product (Axis::bin_num, src/hist.cpp:46-53):
+// the nearest integer r of y and its distance d come from the 2^23 shift
+// (exact for 0 <= y < 2^22), the bin is floor(y), and *amb is set unless y is
+// farther than gy (bins) from r, the only threshold it can be near; NaN and
+// infinite y are ambiguous.  Bins at or above n are returned as LUT_INV.
+__device__ __forceinline__ unsigned direct_bin(float y, float gy, int n, bool *amb) {
+    const float t = y + 8388608.0f;
+    const int r = __float_as_int(t) - 0x4B000000;
+    const float d = y - (t - 8388608.0f);
+    *amb = !(fabsf(d) > gy);
+    const int b = r - (d < 0.0f ? 1 : 0);
+    return b < n ? (unsigned)b : (unsigned)LUT_INV;
+}
+
 // JKHists::interp (src/hist.cpp:369-391) of the angular up-weight at
 // v = 1 - cos(theta): the interval comes from the host-built thresholds on
 // (float)v (the reference's bin_num runs on glibc log1pf), the
@@ -697,7 +715,9 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
                 c1 = LUT_INV;  // sqrtf(negative) is NaN: never binned
                 amb1 = false;
             }
-            const unsigned c2 = lut_decode(S.l2[lut2_index(P.lut2_scale, api)], api, S.t2, P.g_pi, P.lut_edge2, &amb2);
+            const unsigned c2 = P.direct2 ? direct_bin(api * P.inv2, P.k2, P.n2, &amb2)
+                                          : lut_decode(S.l2[lut2_index(P.lut2_scale, api)], api, S.t2, P.g_pi,
+                                                       P.lut_edge2, &amb2);
             if (!amb && ((c1 == LUT_INV && !amb1) || (c2 == LUT_INV && !amb2))) {
                 cnt.in_range += 1;
                 return false;
@@ -714,12 +734,14 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
                 const float inv_s = rsqrtf(s2);
                 mu = fabsf(pi) * inv_s;
                 gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
-                raw2 = S.l2[lut2_index(P.lut2_scale, mu)];
+                if (!P.direct2) raw2 = S.l2[lut2_index(P.lut2_scale, mu)];
             }
             const unsigned c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
             bool amb2 = false;
             unsigned c2 = 0;
-            if (MODE == MODE_S_MU) c2 = lut_decode(raw2, mu, S.t2, gmu, P.lut_edge2, &amb2);
+            if (MODE == MODE_S_MU)
+                c2 = P.direct2 ? direct_bin(mu * P.inv2, fmaf(gmu, P.inv2, P.k2), P.n2, &amb2)
+                               : lut_decode(raw2, mu, S.t2, gmu, P.lut_edge2, &amb2);
             if (c1 == LUT_INV) {
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
@@ -1015,7 +1037,7 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
             for (int t = 0; t < ntiles; ++t) {
                 const int tstart = t * TBK;
                 const int tlen = min(TBK, sg.b_len - tstart);
-                if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, kWaitLimit)) {
+                if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, P.wait_limit)) {
                     atomicCAS(P.err, 0, kErrTimeout);  // device timeout: results are discarded by the host
                 }
                 const int jbase = sg.b_start + tstart;
@@ -1456,6 +1478,8 @@ struct Luts {
     unsigned base1 = 0;
     float scale2 = 0;
     float s2_lut_min = 0;
+    bool direct2 = false;  // axis 2 binned directly (direct_bin) instead of by table 2
+    float inv2 = 0, k2 = 0;
 };
 
 Luts build_luts(const Binning &bin, const Guards &g) {
@@ -1517,6 +1541,30 @@ Luts build_luts(const Binning &bin, const Guards &g) {
         }
         const double vlast = (LUT2_N - 1) * w;
         if (c2(vlast - g2) < 0 && vlast - g2 > bin.t2[bin.nb2]) L.l2[LUT2_N - 1] = LUT_INV;
+        // Direct binning of a linear axis 2 from 0 (mu, |pi|): the kernel
+        // bins y = value * c with the reference's own float c = 1 / step, so
+        // threshold k sits at t2[k] c, within dev of k (exact in double: a
+        // product of two floats).  y is within 2^-24 y of value * c, the
+        // value within its guard gx of the reference's; so a y farther than
+        // dev + gx c + 2^-24 y_max from its nearest integer lies in the
+        // reference's bin floor(y).  k2 is that bound (gx c added per pair
+        // for mu), each term at least doubled.
+        const double c = (double)bin.ax2.inv_step;
+        bool ok = !bin.ax2.log_binning && bin.ax2.min == 0.0f && bin.vs2 == ValueSpace::Direct && c > 0 &&
+                  std::isfinite(c);
+        double dev = 0;
+        for (int k = 0; ok && k <= bin.nb2; ++k) {
+            ok = std::isfinite(bin.t2[k]);
+            if (ok) dev = std::max(dev, std::fabs((double)bin.t2[k] * c - k));
+        }
+        const double ymax = xmax2 * c;
+        const double k2 = 2.0 * dev + std::ldexp(ymax, -22) + (bin.mode == MODE_SIGMA_PI ? 2.0 * g.g_pi * c : 0.0);
+        if (ok && dev < 1e-3 && k2 < 0.05 && ymax < 1e6) {
+            L.direct2 = true;
+            L.inv2 = (float)c;
+            L.k2 = (float)k2;
+            L.s2_lut_min = 0.0f;  // the per-pair guard of mu holds at every s
+        }
     }
     return L;
 }
@@ -1655,11 +1703,16 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     P.lut_edge1 = C.luts.edge1 ? 1 : 0;
     P.lut_edge2 = C.luts.edge2 ? 1 : 0;
     P.lut2_scale = C.luts.scale2;
+    P.direct2 = C.luts.direct2 ? 1 : 0;
+    P.inv2 = C.luts.inv2;
+    P.k2 = C.luts.k2;
     P.n_jk = C.n_jk;
     P.wscale = wscale;
     P.n_runs_f = (float)n_runs;
     P.n_runs_d = (double)n_runs;
     P.los_mid = bin->los_midpoint ? 1 : 0;
+    const long long wl = debug_tile_wait_limit().load();
+    P.wait_limit = wl < 0 ? kWaitLimit : (uint32_t)std::min<long long>(wl, kWaitLimit);
     if (C.up) {
         P.n_up = C.up->ax.n_bins;
         P.up_min = (double)C.up->ax.min;
