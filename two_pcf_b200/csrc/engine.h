@@ -226,7 +226,7 @@ struct Grid {
     int n = 0;            // points in the grid
     bool subset_kept = true;
     PoolBuf<float4> pos;   // (x - kx*side, y - ky*side, z - kz*side, weight), float
-    PoolBuf<float4> aux;   // (x_norm as float, weight): the pi step reads both with one load
+    PoolBuf<float4> aux;   // (x_norm / 2 as float, weight): the pi step reads both with one load
     PoolBuf<int> idx;      // original catalogue index
     PoolBuf<double4> xyz_s;   // sorted double coordinates (exact path, FP64 path)
     PoolBuf<double4> unit_s;  // sorted double unit vectors

@@ -176,7 +176,7 @@ __global__ void scatter_kernel(GeomDev g, const double *__restrict__ xyz, const 
     float wi = w ? w[i] : 1.0f;
     pos[dst] = make_float4(__double2float_rn(x - ox), __double2float_rn(y - oy), __double2float_rn(z - oz), wi);
     const int r = jk ? jk[i] : 0;
-    aux[dst] = make_float4(__double2float_rn(nx), __double2float_rn(ny), __double2float_rn(nz), wi);
+    aux[dst] = make_float4(__double2float_rn(0.5 * nx), __double2float_rn(0.5 * ny), __double2float_rn(0.5 * nz), wi);
     idx[dst] = i;
     if (xyz_s) {
         xyz_s[dst] = make_double4(x, y, z, (double)wi);

@@ -161,7 +161,8 @@ struct KParams {
     double side;
     int n1, n2, nb;
     float min_r_sq, max_r_sq, lo_cut, hi_cut;
-    float cut_mid, cut_half;  // candidate test |s^2 - cut_mid| < cut_half covers [lo_cut, hi_cut]
+    float cut_mid, cut_half;  // |s^2 - cut_mid| < cut_half covers [lo_cut, hi_cut]
+    float s2_test;            // FP32 candidate test s^2 < s2_test (the upper side of the one above)
     float g_s2, g_pi, g_a, c1_mu, c2_mu, g_mu0;
     float s2_lut_min;   // below this s^2 the mu table's guard does not hold
     int lut_edge1, lut_edge2;  // tables carry LUT_EDGE codes
@@ -171,6 +172,7 @@ struct KParams {
     float lut2_scale;    // bucket = (int)(value * lut2_scale)
     int direct2;         // axis 2 binned directly (linear, from 0): bin = floor(value * inv2)
     float inv2, k2;      // the axis's float 1 / step and the constant part of its guard (in bins)
+    float c1y, c2y, g0y;  // mu guard in bins: c2y / s^2 + c1y / s + g0y (k2 included)
     unsigned long long *g_full, *g_sub;  // 128-bit fixed-point sums (low, high word pairs)
     int n_jk;
     float wscale;
@@ -608,7 +610,7 @@ __device__ bool item_in_bounds(const KParams &P, const JobK &J, const WorkItem &
 
 // Add one binned pair: weight from the queue (product of the grid weights)
 // or, for the inverse-p kinds, formed here; fixed-point shared add.
-template <bool UNITW, int WK>
+template <bool UNITW, int WK, bool WA_SCALED = false>
 __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, const Shm &S, int bin, float wa, float wb,
                                            int ia, int jb, int ka, int jl, int ra, int rb) {
 #ifdef TPCF_DEVICE_CHECKS
@@ -632,7 +634,8 @@ __device__ __forceinline__ void add_binned(const KParams &P, const JobK &J, cons
             return;
         }
     }
-    const long long q = (UNITW && WK == W_PLAIN) ? 1LL : __float2ll_rn(__fmul_rn(w, P.wscale));
+    const long long q = (UNITW && WK == W_PLAIN) ? 1LL
+                        : __float2ll_rn(WA_SCALED ? w : __fmul_rn(w, P.wscale));
     dev::acc_add(S.lo, S.hi, bin, q);
 }
 
@@ -665,9 +668,9 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
     const float wa = qa.w;
     float wb, pi = 0.f;
     if constexpr (MODE == MODE_SIGMA_PI || MODE == MODE_S_MU) {
-        const float4 ab = s_aux[jl];  // unit vector and weight of the B point
+        const float4 ab = s_aux[jl];  // half the unit vector and the weight of the B point
         wb = ab.w;
-        pi = 0.5f * fmaf(dz, qa.z + ab.z, fmaf(dy, qa.y + ab.y, dx * (qa.x + ab.x)));
+        pi = fmaf(dz, qa.z + ab.z, fmaf(dy, qa.y + ab.y, dx * (qa.x + ab.x)));  // halved unit vectors
     } else {
         wb = s_pos[jl].w;
     }
@@ -697,7 +700,7 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             if (!inr) return false;
             bin = b;
         }
-        add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+        add_binned<UNITW, WK, WK == W_PLAIN>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
         return false;
     } else {
         if (MODE == MODE_SIGMA_PI) {
@@ -727,21 +730,40 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             bin = (int)(c1 * P.n2 + c2);
         } else {
             // both table lookups first: the two load chains overlap
-            const unsigned raw1 = S.l1[lut1_index(P.lut1_base, s2)];
+            // s^2 passed the candidate test, so it lies below the table's top
+            const unsigned raw1 = S.l1[max((int)((__float_as_uint(s2) >> (23 - LUT1_BITS)) - P.lut1_base), 0)];
             unsigned raw2 = 0;
             float mu = 0.f, gmu = 0.f;
+            if (MODE == MODE_S_MU && P.direct2) {
+                // mu binned directly, its guard taken in bins
+                const float inv_s = rsqrtf(s2);
+                bool amb2;
+                const unsigned c2 = direct_bin(fabsf(pi) * inv_s * P.inv2,
+                                               fmaf(P.c2y * inv_s, inv_s, fmaf(P.c1y, inv_s, P.g0y)), P.n2, &amb2);
+                const unsigned c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
+                if (c1 == LUT_INV) {
+                    cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
+                    return false;
+                }
+                if (c2 == LUT_INV && !amb2 && !amb) {
+                    cnt.in_range += 1;
+                    return false;
+                }
+                amb = amb || amb2;
+                if (!amb) cnt.in_range += 1;
+                bin = (int)(c1 * P.n2 + c2);
+                goto binned;
+            }
             if (MODE == MODE_S_MU) {
                 const float inv_s = rsqrtf(s2);
                 mu = fabsf(pi) * inv_s;
                 gmu = fmaf(P.c2_mu * inv_s, inv_s, fmaf(P.c1_mu, inv_s, P.g_mu0));
-                if (!P.direct2) raw2 = S.l2[lut2_index(P.lut2_scale, mu)];
+                raw2 = S.l2[lut2_index(P.lut2_scale, mu)];
             }
             const unsigned c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
             bool amb2 = false;
             unsigned c2 = 0;
-            if (MODE == MODE_S_MU)
-                c2 = P.direct2 ? direct_bin(mu * P.inv2, fmaf(gmu, P.inv2, P.k2), P.n2, &amb2)
-                               : lut_decode(raw2, mu, S.t2, gmu, P.lut_edge2, &amb2);
+            if (MODE == MODE_S_MU) c2 = lut_decode(raw2, mu, S.t2, gmu, P.lut_edge2, &amb2);
             if (c1 == LUT_INV) {
                 // certainly outside the range or the bins; the range status is
                 // the same for every value of the widened bucket
@@ -758,6 +780,7 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             if (!amb) cnt.in_range += 1;
             bin = (int)(MODE == MODE_S_MU ? c1 * P.n2 + c2 : c1);
         }
+    binned:
         if (amb) {
             if constexpr (!SLOW) return true;
             bool inr, guarded;
@@ -766,7 +789,7 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             cnt.guard += guarded ? 1 : 0;
             if (bin < 0) return false;
         }
-        add_binned<UNITW, WK>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
+        add_binned<UNITW, WK, WK == W_PLAIN>(P, J, S, bin, wa, wb, ia, jb, ka, jl, ra, rb);
         return false;
     }
 }
@@ -967,11 +990,14 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
         }
 
         if (!EXACT) {
-            // unit vector and weight of every A point of the chunk, read by the
-            // consume step (pi, pair weight) at full warp occupancy
+            // half the unit vector and the weight of every A point of the
+            // chunk, read by the consume step (pi, pair weight) at full warp
+            // occupancy
             for (int k = tid; k < it.a_len; k += NT) {
                 const int gi = it.a_start + k;
-                const float wk = J.a.pos[gi].w;
+                // plain weights: the A weight times the fixed-point scale 2^S
+                // (exact), so the pair's fixed-point value is one product
+                const float wk = (WK == W_PLAIN && !UNITW) ? J.a.pos[gi].w * P.wscale : J.a.pos[gi].w;
                 if (kNeedAux) {
                     const float4 q = J.a.aux[gi];
                     s_achunk[k] = make_float4(q.x, q.y, q.z, wk);
@@ -1122,8 +1148,10 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
 #ifdef TPCF_DEVICE_CHECKS
                         if (!dcheck(P.err, DC_SIDE_QUEUE, ns + __popc(bd), 0, kSlowCap)) return;
 #endif
-                        if (dfr) s_slow[ns + __popc(bd & lt_mask)] = __float_as_int(e.w);
-                        ns += __popc(bd);
+                        if (bd) {
+                            if (dfr) s_slow[ns + __popc(bd & lt_mask)] = __float_as_int(e.w);
+                            ns += __popc(bd);
+                        }
                     };
                     // second pass over a parked pair: its separation again,
                     // from the A point (global) in this segment's frame and
@@ -1143,12 +1171,13 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
                     // into the warp's queue with a ballot, and each time 32 are
                     // queued the whole warp bins them (pi, weight, tables) at
                     // full occupancy.  Self segments (auto counts) keep j > i.
-                    auto run = [&](auto self_c) {
+                    auto run = [&](auto self_c, auto one_c) {
                         constexpr bool SELF = decltype(self_c)::value;
+                        constexpr bool ONE = decltype(one_c)::value;  // one group: B point m at step m
                         for (int m = 0; m < nsteps; ++m) {
-                            const int jj = grp + m * Pn;
-                            const float4 pb = s_pos[min(jj, tlen - 1)];
-                            const bool jv = jj < tlen;
+                            const int jj = ONE ? m : grp + m * Pn;
+                            const float4 pb = s_pos[ONE ? jj : min(jj, tlen - 1)];
+                            const bool jv = ONE || jj < tlen;
                             const int jg = jbase + jj;
                             float dx[R], dy[R], dz[R];
                             bool hit[R];
@@ -1158,7 +1187,7 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
                                 dy[r] = ay[r] - pb.y;
                                 dz[r] = az[r] - pb.z;
                                 const float s2 = fmaf(dz[r], dz[r], fmaf(dy[r], dy[r], dx[r] * dx[r]));
-                                hit[r] = jv && fabsf(s2 - P.cut_mid) < P.cut_half;
+                                hit[r] = jv && s2 < P.s2_test;
                                 if (SELF) hit[r] = hit[r] && jg > ai[r];
                             }
 #pragma unroll
@@ -1191,8 +1220,13 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
                             }
                         }
                     };
-                    if (self) run(std::true_type{});
-                    else run(std::false_type{});
+                    if (Pn == 1) {
+                        if (self) run(std::true_type{}, std::true_type{});
+                        else run(std::false_type{}, std::true_type{});
+                    } else {
+                        if (self) run(std::true_type{}, std::false_type{});
+                        else run(std::false_type{}, std::false_type{});
+                    }
                     // drain: the queued and parked entries refer to this
                     // tile's positions
                     if (qn > 0) {
@@ -1589,9 +1623,13 @@ long long max_item_pairs(const std::vector<WorkItem> &items, const std::vector<S
 // shared-memory sums and 128-bit global sums.  S keeps the largest flush
 // (pmax pairs of weight at most wmax) below 2^62; every float weight of at
 // least 2^(23-S) is then represented exactly, and smaller ones to 2^-(S+1).
-int fixed_point_shift(double wmax, long long pmax) {
+// The plain-weight kernels stage each A weight times 2^S, so S also keeps
+// wa_max 2^S (wa_max: the largest weight of either catalogue) far below the
+// float range.
+int fixed_point_shift(double wmax, long long pmax, double wa_max = 0) {
     const double lg = std::log2(std::max(wmax * (1.0 + 1e-6), 1e-30)) + std::log2((double)std::max(pmax, 1LL));
-    const int S = (int)std::floor(62.0 - lg);
+    int S = (int)std::floor(62.0 - lg);
+    if (wa_max > 0) S = std::min(S, (int)std::floor(120.0 - std::log2(wa_max)));
     return std::max(-100, std::min(S, 100));
 }
 
@@ -1699,6 +1737,21 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     P.cut_mid = (float)(0.5 * ((double)P.lo_cut + (double)P.hi_cut));
     P.cut_half = (float)(0.5 * ((double)P.hi_cut - (double)P.lo_cut) * (1.0 + 1e-5) +
                          1e-6 * std::fabs((double)P.cut_mid));
+    // The FP32 candidate test keeps the upper side only: s^2 < h, h the
+    // smallest float with fl(h - cut_mid) >= cut_half (rounding is monotone,
+    // so s^2 < h exactly when fl(s^2 - cut_mid) < cut_half).  Pairs below
+    // lo_cut (a minimum separation above 0) then reach the binning step,
+    // whose tables and range test drop them.
+    {
+        volatile float h = (float)((double)P.cut_mid + (double)P.cut_half);
+        while (!((float)(h - P.cut_mid) >= P.cut_half)) h = std::nextafter((float)h, INFINITY);
+        for (;;) {
+            const float lower = std::nextafter((float)h, -INFINITY);
+            if (!((float)(lower - P.cut_mid) >= P.cut_half)) break;
+            h = lower;
+        }
+        P.s2_test = h;
+    }
     P.lut1_base = C.luts.base1;
     P.lut_edge1 = C.luts.edge1 ? 1 : 0;
     P.lut_edge2 = C.luts.edge2 ? 1 : 0;
@@ -1706,6 +1759,11 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     P.direct2 = C.luts.direct2 ? 1 : 0;
     P.inv2 = C.luts.inv2;
     P.k2 = C.luts.k2;
+    // the mu guard scaled to bins, rounded up
+    const double up = 1.0 + std::ldexp(1.0, -20);
+    P.c1y = (float)((double)g.c1_mu * C.luts.inv2 * up);
+    P.c2y = (float)((double)g.c2_mu * C.luts.inv2 * up);
+    P.g0y = (float)(((double)g.g_mu0 * C.luts.inv2 + C.luts.k2) * up);
     P.n_jk = C.n_jk;
     P.wscale = wscale;
     P.n_runs_f = (float)n_runs;
@@ -1859,7 +1917,7 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
         if (C.wk == W_INVP_DD) wmax *= up_max * num;
         else if (C.wk == W_INVP_DR) wmax *= up_max;
         else if (C.wk == W_ANG_INVP) wmax *= num;
-        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
+        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs), std::max(wmax_of(A), wmax_of(B)));
         wscale = std::ldexp(1.0f, S);
         C.inv = std::ldexp(1.0, -S);
         C.scale_exp = S;
@@ -2507,11 +2565,12 @@ int plan_batch(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *b
     C.jk = true;  // per-item flushes to each job's own histograms
     C.wk = W_PLAIN;
     bool unitw = true;
-    double wmax = 0;
+    double wmax = 0, wa_max = 0;
     for (const BatchJobSpec &j : jobs) {
         const Catalog *A = j.a, *B = j.b ? j.b : j.a;
         unitw = unitw && A->unit_weights && B->unit_weights;
         wmax = std::max(wmax, (double)A->w_max * (double)B->w_max);
+        wa_max = std::max(wa_max, (double)std::max(A->w_max, B->w_max));
     }
     C.unitw = unitw;
     const double rb = bin->rmax_bound;
@@ -2559,7 +2618,7 @@ int plan_batch(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *b
 
     float wscale = 1.0f;
     if (!unitw) {
-        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs));
+        const int S = fixed_point_shift(wmax, max_item_pairs(C.items, C.segs), wa_max);
         wscale = std::ldexp(1.0f, S);
         C.inv = std::ldexp(1.0, -S);
     }
