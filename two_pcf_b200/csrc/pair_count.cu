@@ -472,6 +472,15 @@ __device__ __forceinline__ unsigned direct_bin(float y, float gy, int n, bool *a
     return b < n ? (unsigned)b : (unsigned)LUT_INV;
 }
 
+// Approximate 1 / sqrt(x) (the MUFU reciprocal square root rsqrtf also
+// uses, same error bound) with a subnormal x flushed to zero (+inf out): a
+// pair that close has an infinite mu guard and goes to the exact path.
+__device__ __forceinline__ float rsqrt_ftz(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // JKHists::interp (src/hist.cpp:369-391) of the angular up-weight at
 // v = 1 - cos(theta): the interval comes from the host-built thresholds on
 // (float)v (the reference's bin_num runs on glibc log1pf), the
@@ -736,21 +745,30 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             float mu = 0.f, gmu = 0.f;
             if (MODE == MODE_S_MU && P.direct2) {
                 // mu binned directly, its guard taken in bins
-                const float inv_s = rsqrtf(s2);
+                const float inv_s = rsqrt_ftz(s2);
                 bool amb2;
                 const unsigned c2 = direct_bin(fabsf(pi) * inv_s * P.inv2,
                                                fmaf(P.c2y * inv_s, inv_s, fmaf(P.c1y, inv_s, P.g0y)), P.n2, &amb2);
-                const unsigned c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
-                if (c1 == LUT_INV) {
-                    cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
-                    return false;
+                // a plain bin (the common case) needs no decoding
+                unsigned c1 = raw1;
+                amb = false;
+                if (raw1 >= LUT_EDGE) {
+                    c1 = lut_decode(raw1, s2, S.t1, P.g_s2, P.lut_edge1, &amb);
+                    if (c1 == LUT_INV) {
+                        cnt.in_range += (s2 < P.max_r_sq && s2 > P.min_r_sq) ? 1 : 0;
+                        return false;
+                    }
                 }
-                if (c2 == LUT_INV && !amb2 && !amb) {
+                if (amb || amb2 || c2 == LUT_INV) {
+                    // rare: ambiguous, or mu certainly beyond the last bin
+                    if (!amb && !amb2) {
+                        cnt.in_range += 1;
+                        return false;
+                    }
+                    amb = true;
+                } else {
                     cnt.in_range += 1;
-                    return false;
                 }
-                amb = amb || amb2;
-                if (!amb) cnt.in_range += 1;
                 bin = (int)(c1 * P.n2 + c2);
                 goto binned;
             }
