@@ -48,7 +48,7 @@ UNIT = "pairs/s"
 SIGMA_PI_AXES = ((0.0, 50.0, 1.0, 50), (0.0, 50.0, 1.0, 50))
 S_MU_AXES = ((0.0, 100.0, 1.3, 40), (0.0, 1.0, 0.0, 50))
 F_MODE = {1: 16, 2: 13, 0: 0}   # FP32 flops per in-range pair beyond the 8 of s^2
-TRAFFIC_SMU_RR_5PCT = 26.36e6   # DRAM bytes of one s-mu RR launch at --scale 0.05 (ncu, see profiles/)
+TRAFFIC_SMU_RR = 21.254e9   # DRAM bytes (read + write) of one full-size s-mu RR launch (ncu, see profiles/)
 
 
 def parse():
@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--exchange-selftest", action="store_true",
                    help="launcher check without a GPU: the ranks reduce known partial sums through the sharded "
                         "count's exchange and rank 0 prints whether every rank combined them exactly")
+    p.add_argument("--refinement", type=int, default=0,
+                   help="--one-count: cells per maximum separation (1-3; 0 = the engine's rule)")
     p.add_argument("--one-count", choices=["s_mu", "sigma_pi"], default=None,
                    help="profiling case: one RR count of the workload's randoms at --scale, then exit")
     p.add_argument("--workload", choices=["survey", "mocks", "invp", "adjoint"], default="survey",
@@ -89,6 +91,8 @@ def one_count(args):
     w = make_workload(2, args.scale)
     r = w["rand"]
     ctx = tp.Context(0)
+    if args.refinement:
+        ctx.set_refinement(args.refinement)
     R = tp.Catalog(ctx, r["xyz"], r["x_norm"], r["d_comov"], r["weight"], None, r["jk"], w["n_jk"])
     axes = S_MU_AXES if args.one_count == "s_mu" else SIGMA_PI_AXES
     b = tp.Binning(ctx, tp.S_MU if args.one_count == "s_mu" else tp.SIGMA_PI, *axes, w["n_jk"])
@@ -782,11 +786,12 @@ def main():
         "in_range_pairs_per_step": tot_in // args.steps, "candidates_per_step": tot_cand // args.steps,
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops, "unit": "TFLOP/s",
                      "frac": achieved / fp32_tflops if fp32_tflops else None,
-                     "traffic": TRAFFIC_SMU_RR_5PCT * 20,
-                     "traffic_note": "DRAM bytes (read + write) of one s-mu RR launch: ncu capture at 5 % of the "
-                                     "catalogue (profiles/pair_count_smu_jk_weighted_ncu.md, 26.4 MB) scaled by the "
-                                     "points (x20); the catalogue is read about once per launch, tiles and A chunks "
-                                     "are reused from shared memory and L2",
+                     "traffic": TRAFFIC_SMU_RR,
+                     "traffic_note": "DRAM bytes (read + write) of one full-size s-mu RR launch (5M randoms, 3 cells "
+                                     "per maximum separation; one-pass ncu capture, profiles/"
+                                     "pair_count_smu_jk_weighted_ncu.md): 21.3 GB against 0.16 GB of catalogue, as "
+                                     "every work item streams its B tiles (and re-reads its A chunk per segment) "
+                                     "through L2; 12 GB/s over the launch, 0.2 % of HBM bandwidth",
                      "smem_atomics_per_s": 2.0 * tot_in / (tot_kms * 1e-3) if tot_kms > 0 else None,
                      "smem_atomic_frac": (2.0 * tot_in / (tot_kms * 1e-3) / atom_rate) if (tot_kms > 0 and atom_rate)
                      else None,

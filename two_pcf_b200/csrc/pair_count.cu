@@ -2626,10 +2626,14 @@ int plan_batch(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *b
         }
         C.segs.insert(C.segs.end(), sg.begin(), sg.end());
     }
-    // one longest-first order over every job's items
+    // one order over every job's items: larger first by power-of-two cost
+    // class (a balanced end of the queue), each job's items in cell order
+    // inside a class (neighbouring cells in flight together share their B
+    // tiles in L2)
+    auto cls = [](long long c) { return c > 0 ? 63 - __builtin_clzll((unsigned long long)c) : -1; };
     std::vector<int> order(C.items.size());
     for (size_t k = 0; k < order.size(); ++k) order[k] = (int)k;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cost[x] > cost[y]; });
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return cls(cost[x]) > cls(cost[y]); });
     std::vector<WorkItem> sorted(C.items.size());
     for (size_t k = 0; k < order.size(); ++k) sorted[k] = C.items[order[k]];
     C.items.swap(sorted);

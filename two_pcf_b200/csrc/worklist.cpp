@@ -182,10 +182,15 @@ void build_work_items(const Grid &ga, const Grid &gb, bool is_auto, int m, doubl
         if (!pt.segs.empty()) std::memcpy(segs.data() + so[k], pt.segs.data(), sizeof(Segment) * pt.segs.size());
         std::vector<Segment>().swap(pt.segs);
     }
-    // Largest items first, so the dynamic queue ends balanced.
+    // Larger items first (by power-of-two cost class), so the dynamic queue
+    // ends balanced; inside a class the items keep the cell order, so the
+    // items in flight at once belong to neighbouring cells and share their B
+    // tiles in L2 (a full-size s-mu RR count read 104 GB from DRAM in plain
+    // longest-first order, 21 GB in this one).
+    auto cls = [](long long c) { return c > 0 ? 63 - __builtin_clzll((unsigned long long)c) : -1; };
     std::stable_sort(cost.begin(), cost.end(),
-                     [](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
-                         return x.first > y.first;
+                     [&](const std::pair<long long, int> &x, const std::pair<long long, int> &y) {
+                         return cls(x.first) > cls(y.first);
                      });
     items.resize(ni);
 #pragma omp parallel for schedule(static)
