@@ -421,13 +421,13 @@ int tpcf_wait_selftest(tpcf_ctx *ctx, int32_t arrive, uint32_t limit);
 int tpcf_debug_fail_allocations(int64_t after);
 
 /* Give-up path of the count kernels themselves (no counterpart in the
- * reference; process-wide, for tests): counts planned after this call wait at
- * most `limit` iterations for each staged tile of catalogue B (limit 0: the
- * wait gives up at once) before the kernel flags a device timeout, stops
- * taking work items and the call returns TPCF_E_DEVICE_TIMEOUT with its
- * results discarded.  The wait before a CTA exits keeps the built-in limit,
- * so no copy is left in flight.  limit < 0 restores the built-in limit. */
-int tpcf_debug_tile_wait_limit(int64_t limit);
+ * reference; process-wide, for tests): with on != 0, counts planned after
+ * this call take the branch of a tile wait that gave up (the device-timeout
+ * flag is raised, the CTAs stop taking work items and the call returns
+ * TPCF_E_DEVICE_TIMEOUT with its results discarded), after each wait has
+ * still seen its copy complete, so no copy is left in flight.  on == 0
+ * restores normal counts. */
+int tpcf_debug_force_tile_timeout(int32_t on);
 
 /* Device bounds checks (no counterpart in the reference).  The checked build
  * of this library (TPCF_DEVICE_CHECKS=1 python two_pcf_b200/build.py, written

@@ -31,13 +31,13 @@ def test_bounded_wait_gives_up_and_the_context_stays_usable(ctx):
 
 @pytest.mark.parametrize("precision", [tp.FP32_GUARD, tp.FP64])
 def test_count_kernel_gives_up_on_its_own_tile_wait(ctx, precision):
-    """The count kernels' own give-up path: with the tile-wait limit at 0
-    (tpcf_debug_tile_wait_limit) every wait for a staged tile of B gives up at
-    once, so the kernel flags a device timeout, the other CTAs stop taking
-    work items and the call returns TPCF_E_DEVICE_TIMEOUT with its results
-    discarded.  The wait before a CTA exits keeps the built-in limit, so no
-    copy outlives the launch; with the limit restored the same counts come out
-    bit for bit as before, with and without jackknife regions."""
+    """The count kernels' own give-up path: with tpcf_debug_force_tile_timeout
+    every wait for a staged tile of B, once its copy has completed, takes the
+    branch of a wait that gave up, so the kernel raises the device-timeout
+    flag, the other CTAs stop taking work items and the call returns
+    TPCF_E_DEVICE_TIMEOUT with its results discarded.  No copy is ever left in
+    flight.  With the switch off the same counts come out bit for bit as
+    before, with and without jackknife regions."""
     lib = _capi.lib()
     w, D, R = _survey_pair(ctx, 37, 3000, 9000)
     b_jk = tp.Binning(ctx, tp.S_MU, (0.0, 100.0, 1.3, 40), (0.0, 1.0, 0.0, 50), w["n_jk"])
@@ -47,14 +47,14 @@ def test_count_kernel_gives_up_on_its_own_tile_wait(ctx, precision):
     cases = [(D, R, b_jk), (box, None, b_mono)]
     before = [tp.count(ctx, a, bb, b, precision) for a, bb, b in cases]
     try:
-        assert lib.tpcf_debug_tile_wait_limit(0) == _capi.TPCF_OK
+        assert lib.tpcf_debug_force_tile_timeout(1) == _capi.TPCF_OK
         for a, bb, b in cases:
             with pytest.raises(tp.TpcfError) as exc:
                 tp.count(ctx, a, bb, b, precision)
             assert exc.value.status == _capi.TPCF_E_DEVICE_TIMEOUT
             assert "iteration limit" in str(exc.value)
     finally:
-        lib.tpcf_debug_tile_wait_limit(-1)
+        lib.tpcf_debug_force_tile_timeout(0)
     for (a, bb, b), (f0, r0, s0) in zip(cases, before):
         f1, r1, s1 = tp.count(ctx, a, bb, b, precision)
         assert np.array_equal(f0, f1) and np.array_equal(r0, r1) and f0.sum() > 0

@@ -20,6 +20,10 @@ AXES = {
     "s_mu_lin_min": (tp.S_MU, (3.0, 60.0, 1.0, 19), (0.0, 1.0, 0.0, 7)),
     "sigma_pi_lin": (tp.SIGMA_PI, (0.0, 50.0, 1.0, 50), (0.0, 50.0, 1.0, 50)),
     "sigma_pi_log": (tp.SIGMA_PI, (0.5, 40.0, 1.4, 12), (0.0, 30.0, 1.0, 10)),
+    # second axes the kernel cannot bin directly (a mu axis from above 0, a log pi axis): table 2 and its
+    # edge-coded buckets
+    "s_mu_mu_min": (tp.S_MU, (0.0, 80.0, 1.3, 20), (0.1, 1.0, 0.0, 9)),
+    "sigma_pi_log_pi": (tp.SIGMA_PI, (0.0, 40.0, 1.0, 20), (0.5, 30.0, 1.4, 10)),
 }
 
 

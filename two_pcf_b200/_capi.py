@@ -109,7 +109,7 @@ _PROTOTYPES = {
     "tpcf_measure_peaks": (C.c_int, [_vp, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "tpcf_wait_selftest": (C.c_int, [_vp, C.c_int32, C.c_uint32]),
     "tpcf_debug_fail_allocations": (C.c_int, [C.c_int64]),
-    "tpcf_debug_tile_wait_limit": (C.c_int, [C.c_int64]),
+    "tpcf_debug_force_tile_timeout": (C.c_int, [C.c_int32]),
     # command-line flow (host only)
     "tpcf_host_last_error": (C.c_char_p, []),
     "tpcf_params_load": (C.c_int, [C.c_char_p, C.POINTER(_vp)]),

@@ -980,8 +980,8 @@ int tpcf_debug_fail_allocations(int64_t after) {
     return TPCF_OK;
 }
 
-int tpcf_debug_tile_wait_limit(int64_t limit) {
-    tpcf::debug_tile_wait_limit().store(limit < 0 ? -1 : (long long)limit);
+int tpcf_debug_force_tile_timeout(int32_t on) {
+    tpcf::debug_force_tile_timeout().store(on ? 1 : 0);
     return TPCF_OK;
 }
 

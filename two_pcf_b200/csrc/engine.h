@@ -54,11 +54,11 @@ inline std::atomic<int> &debug_corrupt_work_list() {
     return v;
 }
 
-// Tile-wait limit of the count kernels (tpcf_debug_tile_wait_limit): the
-// iterations each wait for a staged tile may take before the kernel gives up
-// and reports a device timeout; -1 = the built-in limit.
-inline std::atomic<long long> &debug_tile_wait_limit() {
-    static std::atomic<long long> v{-1};
+// Forced tile timeout of the count kernels (tpcf_debug_force_tile_timeout):
+// every wait for a staged tile still waits for its copy, then raises the
+// device-timeout flag as a wait that gave up does.
+inline std::atomic<int> &debug_force_tile_timeout() {
+    static std::atomic<int> v{0};
     return v;
 }
 

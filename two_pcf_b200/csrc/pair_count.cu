@@ -91,9 +91,11 @@ __host__ __device__ constexpr int queue_cap(bool exact, bool jk, bool adj, int c
 }
 static_assert(R % QPUSH == 0 && R % QPUSH_NOJK == 0 && R % 2 == 0 && QPUSH <= 4 && QPUSH_NOJK <= 4,
               "the push loops consume after every QPUSH A slots");
-constexpr int LUT1_BITS = 8;   // buckets per octave of the float-indexed table
-constexpr int LUT1_OCTAVES = 24;
-constexpr int LUT1_N = LUT1_OCTAVES << LUT1_BITS;
+// Table 1 over the float bits of its value: 2^bits buckets per octave (8,
+// over 32 octaves; 9 over 16 for the linear sigma axis, whose edges crowd
+// less toward 0 but sit closer together in sigma^2 at large sigma)
+constexpr int LUT1_N = 8192;
+constexpr int LUT1_N_T2 = 6144;  // when table 2 is staged too (the shared-memory footprint of both stays 10 KB)
 constexpr int LUT2_N = 4096;
 constexpr unsigned char LUT_INV = 254;  // every value of the bucket is dropped
 constexpr unsigned char LUT_AMB = 255;  // bucket within the guard of an edge
@@ -168,7 +170,9 @@ struct KParams {
     int lut_edge1, lut_edge2;  // tables carry LUT_EDGE codes
     const float *t1g, *t2g;
     const unsigned char *lut1g, *lut2g;
-    unsigned lut1_base;  // (bits of the lowest bucket) >> (23 - LUT1_BITS)
+    unsigned lut1_base;  // (bits of the lowest bucket) >> lut1_shift
+    unsigned lut1_shift;  // 23 - bits per octave
+    int lut1_n;           // buckets of table 1 (LUT1_N, or LUT1_N_T2 beside table 2)
     float lut2_scale;    // bucket = (int)(value * lut2_scale)
     int direct2;         // axis 2 binned directly (linear, from 0): bin = floor(value * inv2)
     float inv2, k2;      // the axis's float 1 / step and the constant part of its guard (in bins)
@@ -198,7 +202,7 @@ struct KParams {
     const double *adj_G;
     double *grad_a, *grad_b;
     double adj_scale, adj_inv;  // gradient terms are summed as round(term * adj_scale) in 64-bit fixed point
-    uint32_t wait_limit;        // iterations of each wait for a staged tile before the kernel gives up
+    int force_timeout;          // tests: raise the timeout flag after a (completed) wait for a tile
 };
 
 // Shared-memory views the binning steps use.
@@ -228,7 +232,7 @@ __host__ __device__ inline size_t tile_bytes(bool exact, bool jk, bool adj, int 
 // lo/hi: the histogram pairs are added to (per segment region when there
 // are jackknife regions); alo/ahi: the item's A-side total (jackknife only).
 __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool exact, bool jk, bool adj = false,
-                                                  int cfg = 0) {
+                                                  int cfg = 0, bool lut2 = true) {
     SmemLayout L;
     size_t o = 0;
     L.lo = o;
@@ -244,9 +248,9 @@ __host__ __device__ inline SmemLayout smem_layout(int nb, int n1, int n2, bool e
     L.t2 = o;
     o += 4 * (size_t)(n2 + 1);
     L.lut1 = o;
-    o += LUT1_N;
-    L.lut2 = o;
-    o += LUT2_N;
+    o += lut2 ? LUT1_N_T2 : LUT1_N;
+    L.lut2 = o;  // table 2 only where an axis 2 is binned by table
+    if (lut2) o += LUT2_N;
     o = (o + 15) / 16 * 16;
     L.queue = o;
     o += (size_t)NWARP * queue_cap(exact, jk, adj, cfg) * 16;
@@ -429,9 +433,9 @@ __device__ __forceinline__ int precise_bin(const PreciseArgs P, const ExactArgs 
     return bin;
 }
 
-__device__ __forceinline__ int lut1_index(unsigned base, float x) {
-    const int i = (int)((__float_as_uint(x) >> (23 - LUT1_BITS)) - base);
-    return min(max(i, 0), LUT1_N - 1);
+__device__ __forceinline__ int lut1_index(unsigned base, unsigned shift, int n, float x) {
+    const int i = (int)((__float_as_uint(x) >> shift) - base);
+    return min(max(i, 0), n - 1);
 }
 
 __device__ __forceinline__ int lut2_index(float scale, float x) {
@@ -689,7 +693,8 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
         // v = |n1 - n2|^2 / 2 approximates 1 - cos(theta) within g_ang
         const float v = 0.5f * s2;
         bool amb1;
-        const unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, v)], v, S.t1, P.g_ang, P.lut_edge1, &amb1);
+        const unsigned c1 =
+            lut_decode(S.l1[lut1_index(P.lut1_base, P.lut1_shift, P.lut1_n, v)], v, S.t1, P.g_ang, P.lut_edge1, &amb1);
         if (c1 == LUT_INV) return false;
         if (!amb1) {
             cnt.in_range += 1;
@@ -718,7 +723,8 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
             const float a = fmaf(-pi, pi, s2);
             const float api = fabsf(pi);
             bool amb1, amb2;
-            unsigned c1 = lut_decode(S.l1[lut1_index(P.lut1_base, a)], a, S.t1, P.g_a, P.lut_edge1, &amb1);
+            unsigned c1 =
+                lut_decode(S.l1[lut1_index(P.lut1_base, P.lut1_shift, P.lut1_n, a)], a, S.t1, P.g_a, P.lut_edge1, &amb1);
             if (a <= P.g_a) {
                 c1 = LUT_AMB;
                 amb1 = true;
@@ -740,7 +746,7 @@ __device__ __forceinline__ bool bin_fast(const KParams &P, const JobK &J, const 
         } else {
             // both table lookups first: the two load chains overlap
             // s^2 passed the candidate test, so it lies below the table's top
-            const unsigned raw1 = S.l1[max((int)((__float_as_uint(s2) >> (23 - LUT1_BITS)) - P.lut1_base), 0)];
+            const unsigned raw1 = S.l1[max((int)((__float_as_uint(s2) >> P.lut1_shift) - P.lut1_base), 0)];
             unsigned raw2 = 0;
             float mu = 0.f, gmu = 0.f;
             if (MODE == MODE_S_MU && P.direct2) {
@@ -873,7 +879,8 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
     constexpr int TBK = tile_points(EXACT, JK, ADJ, CFG);                     // B points per tile
     constexpr int NB = n_buffers(EXACT, JK, ADJ, CFG);                        // tile buffers
     constexpr int QPF = light_fast(EXACT, JK, ADJ, CFG) ? QPUSH_NOJK : QPUSH;  // FP32 path push width
-    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ, CFG);
+    const bool need_lut2 = kNeedAux && !P.direct2;
+    const SmemLayout L = smem_layout(P.nb, P.n1, P.n2, EXACT, JK, ADJ, CFG, need_lut2);
     uint32_t *s_lo = (uint32_t *)(smem + L.lo);
     uint32_t *s_hi = (uint32_t *)(smem + L.hi);
     uint32_t *s_alo = (uint32_t *)(smem + L.alo);
@@ -915,8 +922,9 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
     }
     for (int i = tid; i <= P.n1; i += NT) s_t1[i] = P.t1g[i];
     for (int i = tid; i <= P.n2; i += NT) s_t2[i] = P.t2g[i];
-    for (int i = tid; i < LUT1_N; i += NT) s_l1[i] = P.lut1g[i];
-    for (int i = tid; i < LUT2_N; i += NT) s_l2[i] = P.lut2g[i];
+    for (int i = tid; i < P.lut1_n; i += NT) s_l1[i] = P.lut1g[i];
+    if (need_lut2)
+        for (int i = tid; i < LUT2_N; i += NT) s_l2[i] = P.lut2g[i];
     if (tid == 0) {
         for (int b = 0; b < NB; ++b) {
             dev::mbar_init(&bar[b], 1);
@@ -1081,7 +1089,7 @@ __global__ void __launch_bounds__(NT, (JK || CFG == 1) ? 2 : 3) pair_count_kerne
             for (int t = 0; t < ntiles; ++t) {
                 const int tstart = t * TBK;
                 const int tlen = min(TBK, sg.b_len - tstart);
-                if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, P.wait_limit)) {
+                if (!dev::mbar_wait_bounded(&bar[tcount % NB], (tcount / NB) & 1u, kWaitLimit) || P.force_timeout) {
                     atomicCAS(P.err, 0, kErrTimeout);  // device timeout: results are discarded by the host
                 }
                 const int jbase = sg.b_start + tstart;
@@ -1527,16 +1535,48 @@ Guards compute_guards(double side, int m, double rb) {
 struct Luts {
     std::vector<unsigned char> l1, l2;
     bool edge1 = false, edge2 = false;  // edge-coded tables (LUT_EDGE)
-    unsigned base1 = 0;
+    unsigned base1 = 0, shift1 = 23 - 8;
+    int n1 = LUT1_N;  // buckets of table 1 in use
     float scale2 = 0;
     float s2_lut_min = 0;
     bool direct2 = false;  // axis 2 binned directly (direct_bin) instead of by table 2
     float inv2 = 0, k2 = 0;
 };
 
+// Direct binning of a linear axis 2 from 0 (mu, |pi|): the kernel bins
+// y = value * c with the reference's own float c = 1 / step, so threshold k
+// sits at t2[k] c, within dev of k (exact in double: a product of two
+// floats).  y is within 2^-24 y of value * c, the value within its guard gx
+// of the reference's; so a y farther than dev + gx c + 2^-24 y_max from its
+// nearest integer lies in the reference's bin floor(y).  k2 is that bound (gx
+// c added per pair for mu), each term at least doubled.  False when the axis
+// needs table 2.
+bool direct2_params(const Binning &bin, const Guards &g, float *inv2, float *k2_out) {
+    if (bin.mode != MODE_SIGMA_PI && bin.mode != MODE_S_MU) return false;
+    const double xmax2 = bin.mode == MODE_S_MU ? 1.25 : 1.25 * std::sqrt((double)bin.max_r_sq);
+    const double c = (double)bin.ax2.inv_step;
+    bool ok = !bin.ax2.log_binning && bin.ax2.min == 0.0f && bin.vs2 == ValueSpace::Direct && c > 0 &&
+              std::isfinite(c);
+    double dev = 0;
+    for (int k = 0; ok && k <= bin.nb2; ++k) {
+        ok = std::isfinite(bin.t2[k]);
+        if (ok) dev = std::max(dev, std::fabs((double)bin.t2[k] * c - k));
+    }
+    const double ymax = xmax2 * c;
+    const double k2 = 2.0 * dev + std::ldexp(ymax, -22) + (bin.mode == MODE_SIGMA_PI ? 2.0 * g.g_pi * c : 0.0);
+    if (!(ok && dev < 1e-3 && k2 < 0.05 && ymax < 1e6)) return false;
+    *inv2 = (float)c;
+    *k2_out = (float)k2;
+    return true;
+}
+
 Luts build_luts(const Binning &bin, const Guards &g) {
     Luts L;
     L.l1.assign(LUT1_N, LUT_AMB);
+    float inv2 = 0, k2 = 0;
+    const bool d2 = direct2_params(bin, g, &inv2, &k2);
+    const bool table2 = (bin.mode == MODE_SIGMA_PI || bin.mode == MODE_S_MU) && !d2;
+    L.n1 = table2 ? LUT1_N_T2 : LUT1_N;
     L.l2.assign(LUT2_N, LUT_AMB);
     // Table 1 over the float bits of s^2 (monopole, s-mu; the range test is
     // folded in), of sigma^2 (sigma-pi) or of 1 - cos(theta) (angular).
@@ -1550,12 +1590,14 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     }
     const double xmax1 = std::max((double)bin.max_r_sq, 1e-30) * 2.0;
     const int ehi = (int)std::ceil(std::log2(xmax1)) + 1;
-    const int elo = ehi - LUT1_OCTAVES;
-    const uint32_t sh = 23 - LUT1_BITS;
+    const int bits1 = (bin.mode == MODE_SIGMA_PI && !bin.ax1.log_binning && !table2) ? 9 : 8;
+    const int elo = ehi - (L.n1 >> bits1);
+    const uint32_t sh = 23 - bits1;
+    L.shift1 = sh;
     L.base1 = bits_of(std::ldexp(1.0f, elo)) >> sh;
     const double g1 = s_axis ? g.g_s2 : (bin.mode == MODE_ANGULAR ? g.g_ang : g.g_a);
     L.edge1 = bin.nb1 <= kLutEdgeMaxBins;
-    for (int i = 1; i < LUT1_N - 1; ++i) {
+    for (int i = 1; i < L.n1 - 1; ++i) {
         const double v0 = f_from_bits((L.base1 + i) << sh);
         const double v1 = f_from_bits((L.base1 + i + 1) << sh);
         L.l1[i] = lut_entry(c1, e1, v0, v1, g1, L.edge1);
@@ -1563,9 +1605,9 @@ Luts build_luts(const Binning &bin, const Guards &g) {
     // Bucket 0 holds everything below the table (ambiguous); the last bucket
     // holds everything above it.
     {
-        const double v0 = f_from_bits((L.base1 + LUT1_N - 1) << sh);
-        if (s_axis && v0 - g1 > bin.max_r_sq) L.l1[LUT1_N - 1] = LUT_INV;
-        if (!s_axis && std::isfinite(bin.t1[bin.nb1]) && v0 - g1 > bin.t1[bin.nb1]) L.l1[LUT1_N - 1] = LUT_INV;
+        const double v0 = f_from_bits((L.base1 + L.n1 - 1) << sh);
+        if (s_axis && v0 - g1 > bin.max_r_sq) L.l1[L.n1 - 1] = LUT_INV;
+        if (!s_axis && std::isfinite(bin.t1[bin.nb1]) && v0 - g1 > bin.t1[bin.nb1]) L.l1[L.n1 - 1] = LUT_INV;
     }
     if (bin.mode == MODE_SIGMA_PI || bin.mode == MODE_S_MU) {
         // Table 2, linear buckets: mu on [0, 1.25) or |pi| on [0, 1.25 rmax).
@@ -1593,28 +1635,10 @@ Luts build_luts(const Binning &bin, const Guards &g) {
         }
         const double vlast = (LUT2_N - 1) * w;
         if (c2(vlast - g2) < 0 && vlast - g2 > bin.t2[bin.nb2]) L.l2[LUT2_N - 1] = LUT_INV;
-        // Direct binning of a linear axis 2 from 0 (mu, |pi|): the kernel
-        // bins y = value * c with the reference's own float c = 1 / step, so
-        // threshold k sits at t2[k] c, within dev of k (exact in double: a
-        // product of two floats).  y is within 2^-24 y of value * c, the
-        // value within its guard gx of the reference's; so a y farther than
-        // dev + gx c + 2^-24 y_max from its nearest integer lies in the
-        // reference's bin floor(y).  k2 is that bound (gx c added per pair
-        // for mu), each term at least doubled.
-        const double c = (double)bin.ax2.inv_step;
-        bool ok = !bin.ax2.log_binning && bin.ax2.min == 0.0f && bin.vs2 == ValueSpace::Direct && c > 0 &&
-                  std::isfinite(c);
-        double dev = 0;
-        for (int k = 0; ok && k <= bin.nb2; ++k) {
-            ok = std::isfinite(bin.t2[k]);
-            if (ok) dev = std::max(dev, std::fabs((double)bin.t2[k] * c - k));
-        }
-        const double ymax = xmax2 * c;
-        const double k2 = 2.0 * dev + std::ldexp(ymax, -22) + (bin.mode == MODE_SIGMA_PI ? 2.0 * g.g_pi * c : 0.0);
-        if (ok && dev < 1e-3 && k2 < 0.05 && ymax < 1e6) {
+        if (d2) {
             L.direct2 = true;
-            L.inv2 = (float)c;
-            L.k2 = (float)k2;
+            L.inv2 = inv2;
+            L.k2 = k2;
             L.s2_lut_min = 0.0f;  // the per-pair guard of mu holds at every s
         }
     }
@@ -1771,6 +1795,8 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
         P.s2_test = h;
     }
     P.lut1_base = C.luts.base1;
+    P.lut1_shift = C.luts.shift1;
+    P.lut1_n = C.luts.n1;
     P.lut_edge1 = C.luts.edge1 ? 1 : 0;
     P.lut_edge2 = C.luts.edge2 ? 1 : 0;
     P.lut2_scale = C.luts.scale2;
@@ -1787,8 +1813,7 @@ void fill_params(CountPlan &C, const Binning *bin, const Guards &g, double side,
     P.n_runs_f = (float)n_runs;
     P.n_runs_d = (double)n_runs;
     P.los_mid = bin->los_midpoint ? 1 : 0;
-    const long long wl = debug_tile_wait_limit().load();
-    P.wait_limit = wl < 0 ? kWaitLimit : (uint32_t)std::min<long long>(wl, kWaitLimit);
+    P.force_timeout = debug_force_tile_timeout().load() ? 1 : 0;
     if (C.up) {
         P.n_up = C.up->ax.n_bins;
         P.up_min = (double)C.up->ax.min;
@@ -1959,6 +1984,9 @@ int plan_count(Ctx *ctx, const CountRequest &req, bool build, CountPlan &C, Erro
     Guards g = compute_guards(side, m, rb);
     if (C.angular) g.g_ang = (float)((0.5 * g.g_s2 + 2.0 * norm_dev + 2e-15) * (1.0 + 1e-6));
     C.luts = build_luts(*bin, g);
+    // without table 2 (axis 2 binned directly) the kernel's layout is smaller
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, req.exact_fp64, C.jk, C.adj, C.cfg,
+                      (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) && !C.luts.direct2);
 
     fill_params(C, bin, g, side, tn, wscale, req.n_runs);
     KParams &P = C.P;
@@ -2652,6 +2680,8 @@ int plan_batch(Ctx *ctx, const std::vector<BatchJobSpec> &jobs, const Binning *b
     }
     const Guards g = compute_guards(side, m, rb);
     C.luts = build_luts(*bin, g);
+    C.L = smem_layout(C.nb, bin->nb1, bin->nb2, exact, true, false, 0,
+                      (bin->mode == MODE_SIGMA_PI || bin->mode == MODE_S_MU) && !C.luts.direct2);
     fill_params(C, bin, g, side, 2.0, wscale, 0);
     C.P.job0 = C.jobs[0];
     C.fn = pick(bin->mode, W_PLAIN, unitw, true, exact);
