@@ -789,9 +789,11 @@ def main():
                      "traffic": TRAFFIC_SMU_RR,
                      "traffic_note": "DRAM bytes (read + write) of one full-size s-mu RR launch (5M randoms, 3 cells "
                                      "per maximum separation; one-pass ncu capture, profiles/"
-                                     "pair_count_smu_jk_weighted_ncu.md): 21.3 GB against 0.16 GB of catalogue, as "
-                                     "every work item streams its B tiles (and re-reads its A chunk per segment) "
-                                     "through L2; 12 GB/s over the launch, 0.2 % of HBM bandwidth",
+                                     "pair_count_smu_jk_weighted_ncu.md): 21.3 GB, about 1.1x the algorithmic tile "
+                                     "loads (each work item streams the B points of its segments once per A chunk "
+                                     "of at most 1024 points: at least 32 B x 6.09e11 candidates / 1024 = 19.0 GB; "
+                                     "the catalogue itself is 0.16 GB); 12 GB/s over the launch, 0.2 % of HBM "
+                                     "bandwidth",
                      "smem_atomics_per_s": 2.0 * tot_in / (tot_kms * 1e-3) if tot_kms > 0 else None,
                      "smem_atomic_frac": (2.0 * tot_in / (tot_kms * 1e-3) / atom_rate) if (tot_kms > 0 and atom_rate)
                      else None,
